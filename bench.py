@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pressure projection (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--mode fp64|mixed] [--no-cpu-baseline]
+
+Workload: one projection step of the channel case 768 x 384 x 384 (Lx = 2 pi,
+Lz = pi, tanh faces with beta = 2, Poiseuille predictor plus N(0, 0.1) noise,
+v = 0 at the walls), divergence-consistent bands so that max|div u| reaches
+round-off.  Seeded synthetic inputs are generated on the device (no dataset
+exists for this path).  The three input fields (0.92 GB each) are larger than
+the 126 MB L2, so no flush is needed between steps.
+
+value: Gpts/s = (points of all ranks x K) / (max over ranks of the device time
+of K steps), CUDA events on the launching stream.  e2e: the same metric through
+the host-buffer C-ABI call prj_projection_step_host (H2D of u_hat, projection,
+D2H of u, v, w, p inside the timed region).  Multi-GPU runs are independent
+replicas (the path does not shard): weak scaling, no collective.
+
+--impl reference times the CPU restatement of the reference's FFTW path
+(oracle/, all host threads) on the same workload, per step a bounded sample
+(768 x ny_s x 384, ny_s chosen so the run ends within a few minutes).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dns-supercritical-ibm_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "projection Gpts/s 768x384x384: FP32+refine vs FP64 @div<1e-10; served p99 ms"
+NX, NY, NZ = 768, 384, 384
+ALG_BYTES_PER_POINT = 88  # projection: 56 B/pt compulsory FP64 I/O + 32 B/pt spectrum round trips
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock and clock-event reasons of one GPU through NVML while running."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index: int, period_s: float = 0.01):
+        self.index, self.period = index, period_s
+        self.samples, self.reasons = [], 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thr = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                self.reasons |= nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._thr = threading.Thread(target=self._run, daemon=True)
+            self._thr.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thr:
+            self._thr.join()
+
+    def summary(self):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
+        names = [v for k, v in self.REASONS.items() if self.reasons & k]
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": names, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------- workload
+def device_inputs(nx, ny, nz, seed, device):
+    """Channel predictor on the device: halo'd [y+2, z+2, x+2] tensors (interior filled)."""
+    import torch
+    import workloads
+    yu = workloads.tanh_faces(ny, 2.0)
+    yp = torch.tensor((yu[:-1] + yu[1:]) / 2, dtype=torch.float64, device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    hs = (ny + 2, nz + 2, nx + 2)
+    Uh = torch.zeros(hs, dtype=torch.float64, device=device)
+    Vh = torch.zeros(hs, dtype=torch.float64, device=device)
+    Wh = torch.zeros(hs, dtype=torch.float64, device=device)
+    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+    Uh[inner] = 1.5 * (1.0 - (yp.view(-1, 1, 1) - 1.0) ** 2) + 0.1 * torch.randn((ny, nz, nx), generator=g,
+                                                                                 dtype=torch.float64, device=device)
+    Vh[inner] = 0.1 * torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=device)
+    Wh[inner] = 0.1 * torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=device)
+    Vh[1] = 0.0  # bottom wall face V(k=0)
+    return Uh, Vh, Wh, yu
+
+
+def kernel_alg_bytes(nx, ny, nz):
+    """Algorithmic bytes per launch of each kernel (what crosses its boundary)."""
+    N = nx * ny * nz
+    Nh = (nx + 2) * (nz + 2) * (ny + 2)
+    S = (nx // 2 + 1) * nz * ny * 16  # one pass over the complex half-spectrum
+    return {"k_fwd_x": 24 * N + S, "k_zsolve": 2 * S, "k_bwd_x": S + 8 * N, "k_correct": 32 * N + 24 * Nh}
+
+
+def read_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"dram_traffic_projection_{NX}x{NY}x{NZ}.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+    import workloads
+    C = pyoracle.COracle()
+    cores = os.cpu_count() or 1
+    # probe the per-point cost on a thin slab, then size the per-step sample
+    probe_ny = 16
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(NX, probe_ny, NZ, seed=1)
+    t0 = time.perf_counter()
+    C.projection(Uh, Vh, Wh, dx, dz, 1.0, yu, "consistent", nthreads=cores)
+    per_pt = (time.perf_counter() - t0) / (NX * probe_ny * NZ)
+    budget = 100.0
+    nsteps = args.steps + args.warmup
+    ny_s = int(budget / max(nsteps, 1) / (per_pt * NX * NZ))
+    ny_s = max(8, min(NY, ny_s - ny_s % 2))
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(NX, ny_s, NZ, seed=1)
+    for _ in range(args.warmup):
+        C.projection(Uh, Vh, Wh, dx, dz, 1.0, yu, "consistent", nthreads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        C.projection(Uh, Vh, Wh, dx, dz, 1.0, yu, "consistent", nthreads=cores)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = NX * ny_s * NZ * args.steps / total / 1e9
+    sample = f"{NX}x{ny_s}x{NZ} projection per step (nx, nz and the stretching of the full case; ny reduced to bound the run)"
+    line = {"metric": METRIC, "value": value, "unit": "Gpts/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "pressure projection step 768x384x384 (channel, tanh beta=2)", "nx": NX, "ny": NY,
+                       "nz": NZ, "bands": "consistent", "sample_ny": ny_s},
+            "cpu_baseline": {"value": value, "unit": "Gpts/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference FFTW/MPI build unavailable (no Fortran/MPI/FFTW on the box); the C restatement "
+                    "of its FFTW path (oracle/prj_oracle.c, OpenMP) is timed instead"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- engine arm
+def cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz):
+    """Time the oracle projection once on the bench workload (host copies of the inputs)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    C = pyoracle.COracle()
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    C.projection(Uh_h, Vh_h, Wh_h, dx, dz, 1.0, yu, "consistent", nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": NX * NY * NZ / dt / 1e9, "unit": "Gpts/s", "cores": cores, "kind": "port",
+            "sample": f"one full {NX}x{NY}x{NZ} projection step ({dt:.2f} s)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import numpy as np
+    import torch
+    import prj
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    mode = prj.MODE_FP64 if args.mode == "fp64" else prj.MODE_FP32_REFINE
+    Uh, Vh, Wh, yu = device_inputs(NX, NY, NZ, seed=1 + rank, device=device)
+    dx, dz = 2 * math.pi / NX, math.pi / NZ
+    hs = (NY + 2, NZ + 2, NX + 2)
+    U = torch.empty(hs, dtype=torch.float64, device=device)
+    V = torch.empty_like(U)
+    W = torch.empty_like(U)
+    P = torch.empty((NY, NZ, NX), dtype=torch.float64, device=device)
+    plan = prj.Plan.from_yu(NX, NZ, dx, dz, yu, "consistent", device=local)
+    stream = torch.cuda.current_stream(device)
+
+    def step(stats=False):
+        return plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=mode, stats=stats, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    plan.enable_stage_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    plan.enable_stage_timing(False)
+    ms = e0.elapsed_time(e1)
+    stages = plan.stage_times()
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * NX * NY * NZ * args.steps / (ms_max / 1e3) / 1e9
+
+    # accuracy record of the same step (outside the timed region)
+    st = step(stats=True)
+
+    # e2e through the host-buffer C-ABI call
+    Uh_h = np.asfortranarray(Uh.cpu().numpy().T)
+    Vh_h = np.asfortranarray(Vh.cpu().numpy().T)
+    Wh_h = np.asfortranarray(Wh.cpu().numpy().T)
+    pin = lambda shape: torch.empty(tuple(reversed(shape)), dtype=torch.float64).pin_memory().numpy().T
+    hshape = (NX + 2, NZ + 2, NY + 2)
+    pUh, pVh, pWh, pU, pV, pW = (pin(hshape) for _ in range(6))
+    pP = pin((NX, NZ, NY))
+    pUh[...] = Uh_h
+    pVh[...] = Vh_h
+    pWh[...] = Wh_h
+    plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)  # warm (staging alloc)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = float(te.item())
+    nh = (NX + 2) * (NZ + 2) * (NY + 2)
+    e2e = {"value": world * NX * NY * NZ / e2e_s / 1e9, "unit": "Gpts/s", "h2d_bytes_per_step": 3 * 8 * nh,
+           "d2h_bytes_per_step": 3 * 8 * nh + 8 * NX * NY * NZ, "ms_per_step": 1e3 * e2e_s,
+           "call": "prj_projection_step_host (pinned host buffers)"}
+
+    # roofline of the dominant kernel
+    peak, peak_kind = peaks()
+    alg = kernel_alg_bytes(NX, NY, NZ)
+    dom = max(stages, key=lambda k: stages[k][0])
+    dom_ms = stages[dom][0] / stages[dom][1]
+    achieved = alg[dom] / (dom_ms / 1e3) / 1e9
+    traffic = read_traffic(dom)
+    step_ms = ms_max / args.steps
+    roof_step = ALG_BYTES_PER_POINT * NX * NY * NZ / (step_ms / 1e3) / 1e9
+    launches = sum(c for _, c in stages.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "pressure projection step 768x384x384 (channel Lx=2pi Lz=pi, tanh beta=2, "
+                                   "Poiseuille + N(0,0.1) predictor)", "nx": NX, "ny": NY, "nz": NZ,
+                       "mode": args.mode, "bands": "consistent", "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (3 x 0.92 GB fields), no flush"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "alg_bytes_per_launch": alg[dom], "avg_launch_ms": dom_ms},
+            "roofline_step": {"alg_bytes_per_point": ALG_BYTES_PER_POINT, "achieved": roof_step, "peak": peak,
+                              "unit": "GB/s", "frac": roof_step / peak},
+            "stages_ms_per_launch": {k: v[0] / v[1] for k, v in stages.items()},
+            "stage_share": {k: v[0] / sum(x[0] for x in stages.values()) for k, v in stages.items()},
+            "gpu_launches": launches,
+            "accuracy": {"div_maxabs": st["div_maxabs"], "p_maxabs": st["p_maxabs"], "min_pivot": st["min_pivot"]},
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,62 @@
+"""Build the engine's shared library for sm_100a with nvcc.
+
+    python dns-supercritical-ibm_b200/build.py [--verbose]
+
+Output: dns-supercritical-ibm_b200/libprj_b200.so (in-tree; it travels with the
+source tree to the GPU host).  Rebuilds only when a source is newer than the
+library unless ``force`` is set.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libprj_b200.so")
+SOURCES = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+DEPS = SOURCES + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + sorted(
+    glob.glob(os.path.join(HERE, "csrc", "*.h"))) + [os.path.join(REPO, "include", "projection.h")]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(p) > t for p in DEPS)
+
+
+def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    if not force and not needs_build():
+        return LIB
+    cmd = [nvcc_path(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+           "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp", *SOURCES, "-lcudart"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    if extra:
+        cmd[1:1] = list(extra)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libprj_b200.so")
+    if verbose:
+        sys.stderr.write(res.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose="--verbose" in sys.argv)
+    print(LIB)

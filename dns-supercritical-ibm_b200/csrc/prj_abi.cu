@@ -1,0 +1,588 @@
+// prj_abi.cu -- host side of the engine: FFT planning, plan set-up and the
+// extern "C" entry points declared in include/projection.h.
+//
+// The plan builder takes over the work of init_spec_poisson_multigpu
+// (src/poisson_solver_mgpu_dtdma/poisson_solver_multigpu.f90:33-326) for one
+// rank: FFT plans, the a_x / a_z wavenumber tables (:133-155, computed here in
+// host double precision with the C library's sin, as the reference does on the
+// CPU build), and the Thomas pivot table (the analogue of poi_C, :164-179).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/projection.h"
+#include "prj_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(PRJ_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+    return fail(PRJ_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+// radix sequence of a complex FFT of length n (8 first, then 4, 2, 3, 5, others)
+std::vector<int> factorize(int n) {
+    std::vector<int> f;
+    int m = n;
+    while (m % 8 == 0 && m != 16) { f.push_back(8); m /= 8; }
+    while (m % 4 == 0) { f.push_back(4); m /= 4; }
+    while (m % 2 == 0) { f.push_back(2); m /= 2; }
+    for (int r : {3, 5}) while (m % r == 0) { f.push_back(r); m /= r; }
+    for (int r = 7; m > 1; r += 2) {
+        while (m % r == 0) { f.push_back(r); m /= r; }
+        if ((long)r * r > m && m > 1) { f.push_back(m); m = 1; }
+    }
+    return f;
+}
+
+const long double kTwoPi = 6.283185307179586476925286766559005768L;
+
+template <typename T>
+using C2 = typename prj::C2<T>::t;
+
+template <typename T>
+C2<T> cexpm(long double num, long double den) {  // exp(-2 pi i num/den)
+    const long double a = kTwoPi * num / den;
+    C2<T> v;
+    v.x = (T)cosl(a);
+    v.y = (T)(-sinl(a));
+    return v;
+}
+
+// Build stage tables on the host; returns the device twiddle buffer.
+template <typename T>
+int make_cfft(int n, prj::FftDev* f, C2<T>** d_tw, size_t* bytes) {
+    std::vector<int> fac = factorize(n);
+    if ((int)fac.size() > prj::kMaxStages) return fail(PRJ_ERR_UNSUPPORTED, "FFT length %d needs too many stages", n);
+    std::memset(f, 0, sizeof(*f));
+    f->n = n;
+    f->nst = (int)fac.size();
+    std::vector<C2<T>> tw;
+    int p = 1;
+    for (int s = 0; s < f->nst; s++) {
+        const int R = fac[s];
+        if (R > 64) return fail(PRJ_ERR_UNSUPPORTED, "FFT length %d has prime factor %d > 64", n, R);
+        f->radix[s] = R;
+        f->p[s] = p;
+        f->twoff[s] = (int)tw.size();
+        for (int k = 0; k < p; k++)
+            for (int r = 1; r < R; r++) tw.push_back(cexpm<T>((long double)r * k, (long double)p * R));
+        const bool hard = (R == 2 || R == 3 || R == 4 || R == 5 || R == 8);
+        if (!hard)
+            for (int m = 0; m < R; m++) tw.push_back(cexpm<T>((long double)m, (long double)R));
+        p *= R;
+    }
+    if (tw.empty()) tw.push_back(cexpm<T>(0, 1));
+    *bytes += tw.size() * sizeof(C2<T>);
+    CK(cudaMalloc((void**)d_tw, tw.size() * sizeof(C2<T>)), "cudaMalloc(twiddles)");
+    CK(cudaMemcpy(*d_tw, tw.data(), tw.size() * sizeof(C2<T>), cudaMemcpyHostToDevice), "cudaMemcpy(twiddles)");
+    return PRJ_OK;
+}
+
+template <typename T>
+int make_rfft(int n, prj::RealFftPlan<T>* r, size_t* bytes) {
+    r->n = n;
+    r->nh = n / 2 + 1;
+    r->even = (n % 2 == 0);
+    r->m = r->even ? n / 2 : n;
+    int rc = make_cfft<T>(r->m, &r->f, &r->tw, bytes);
+    if (rc) return rc;
+    std::vector<C2<T>> post((size_t)r->m + 1);
+    for (int k = 0; k <= r->m; k++) post[k] = cexpm<T>((long double)k, (long double)n);
+    *bytes += post.size() * sizeof(C2<T>);
+    CK(cudaMalloc((void**)&r->post, post.size() * sizeof(C2<T>)), "cudaMalloc(post twiddles)");
+    CK(cudaMemcpy(r->post, post.data(), post.size() * sizeof(C2<T>), cudaMemcpyHostToDevice), "cudaMemcpy(post)");
+    return PRJ_OK;
+}
+
+template <typename P>
+void dfree(P*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+void free_plan_buffers(prj_plan* pl) {
+    dfree(pl->t.bands);
+    dfree(pl->t.inv_dy_p);
+    dfree(pl->t.dpdy_lo);
+    dfree(pl->t.dpdy_hi);
+    dfree(pl->t.ax);
+    dfree(pl->t.az);
+    dfree(pl->t.piv);
+    dfree(pl->fx64.tw);
+    dfree(pl->fx64.post);
+    dfree(pl->fz64.tw);
+    dfree(pl->spec);
+    dfree(pl->stat_buf);
+    dfree(pl->host_stage);
+    pl->host_stage_elems = 0;
+}
+
+bool finite_all(const double* v, int n) {
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int check_plan(const prj_plan* pl) {
+    if (!pl) return fail(PRJ_ERR_ARG, "plan is NULL");
+    if (!pl->spec) return fail(PRJ_ERR_STATE, "plan has no device buffers");
+    return PRJ_OK;
+}
+
+// Stage timing: events around one kernel launch when the plan's record is on.
+struct StageTimer {
+    prj_plan* pl;
+    int stage;
+    cudaStream_t st;
+    cudaEvent_t t0 = nullptr;
+    StageTimer(prj_plan* p, int s, cudaStream_t stream) : pl(p), stage(s), st(stream) {
+        if (!pl->timing) return;
+        t0 = take();
+        if (t0) cudaEventRecord(t0, st);
+    }
+    cudaEvent_t take() {
+        cudaEvent_t e = nullptr;
+        if (!pl->event_pool.empty()) {
+            e = pl->event_pool.back();
+            pl->event_pool.pop_back();
+        } else if (cudaEventCreate(&e) != cudaSuccess) {
+            e = nullptr;
+        }
+        return e;
+    }
+    ~StageTimer() {
+        if (!t0) return;
+        cudaEvent_t t1 = take();
+        if (!t1) { pl->event_pool.push_back(t0); return; }
+        cudaEventRecord(t1, st);
+        pl->rec.push_back(prj::StageRecord{stage, t0, t1});
+    }
+};
+
+int run_poisson(prj_plan* pl, double* d_P, cudaStream_t st) {
+    {
+        StageTimer tm(pl, prj::kStFwdX, st);
+        CK(prj::launch_fwd_x(pl, prj::FwdSource::Pressure, d_P, nullptr, nullptr, nullptr, nullptr, st), "forward x");
+    }
+    {
+        StageTimer tm(pl, prj::kStZSolve, st);
+        CK(prj::launch_zsolve(pl, st), "z transform + Thomas");
+    }
+    {
+        StageTimer tm(pl, prj::kStBwdX, st);
+        CK(prj::launch_bwd_x(pl, d_P, st), "inverse x");
+    }
+    return PRJ_OK;
+}
+
+void release_events(prj_plan* pl) {
+    for (auto& r : pl->rec) {
+        cudaEventDestroy(r.t0);
+        cudaEventDestroy(r.t1);
+    }
+    pl->rec.clear();
+    for (auto e : pl->event_pool) cudaEventDestroy(e);
+    pl->event_pool.clear();
+}
+
+int ensure_host_stage(prj_plan* pl, size_t elems) {
+    if (pl->host_stage_elems >= elems) return PRJ_OK;
+    dfree(pl->host_stage);
+    pl->host_stage_elems = 0;
+    CK(cudaMalloc((void**)&pl->host_stage, elems * sizeof(double)), "cudaMalloc(host staging)");
+    pl->host_stage_elems = elems;
+    return PRJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* prj_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* prj_version(void) { return "prj_b200 0.1 (sm_100a)"; }
+
+int prj_bands_from_yu(int ny, const double* yu, int mode, double* a, double* b, double* c, double* a00, double* b00,
+                      double* c00) {
+    if (ny < 2) return fail(PRJ_ERR_ARG, "ny=%d < 2", ny);
+    if (!yu || !a || !b || !c || !a00 || !b00 || !c00) return fail(PRJ_ERR_ARG, "NULL argument");
+    for (int i = 0; i < ny; i++)
+        if (!(yu[i + 1] > yu[i])) return fail(PRJ_ERR_ARG, "yu must increase strictly (yu[%d] >= yu[%d])", i, i + 1);
+    std::vector<double> ext((size_t)ny + 2);  // yp_ext, calc_bands.py:226-227
+    ext[0] = yu[0];
+    for (int i = 0; i < ny; i++) ext[i + 1] = (yu[i] + yu[i + 1]) / 2;
+    ext[ny + 1] = yu[ny];
+    if (mode == PRJ_BANDS_REFERENCE) {
+        // mk_P_abc, calc_bands.py:181-201 (once plain, once is_dirich_first)
+        std::vector<double> pad(ext);
+        pad[0] = 2 * ext[0] - ext[1];
+        pad[ny + 1] = 2 * ext[ny + 1] - ext[ny];
+        for (int pass = 0; pass < 2; pass++) {
+            double* A = pass ? a00 : a;
+            double* B = pass ? b00 : b;
+            double* C = pass ? c00 : c;
+            for (int i = 0; i < ny; i++) {
+                const double x0 = pad[i], x1 = pad[i + 1], x2 = pad[i + 2];
+                const double dy = 0.5 * (x2 - x0);
+                A[i] = 1.0 / ((x1 - x0) * dy);
+                C[i] = 1.0 / ((x2 - x1) * dy);
+                B[i] = -(A[i] + C[i]);
+            }
+            if (pass) B[0] -= A[0];
+            else B[0] += A[0];
+            B[ny - 1] += C[ny - 1];
+            A[0] = 0.0;
+            C[ny - 1] = 0.0;
+        }
+        return PRJ_OK;
+    }
+    if (mode == PRJ_BANDS_CONSISTENT) {
+        const double* yp = ext.data() + 1;
+        for (int k = 0; k < ny; k++) {
+            const double idy = 1.0 / (yu[k + 1] - yu[k]);
+            a[k] = (k > 0) ? idy / (yp[k] - yp[k - 1]) : 0.0;
+            c[k] = (k < ny - 1) ? idy / (yp[k + 1] - yp[k]) : 0.0;
+            b[k] = -(a[k] + c[k]);
+            a00[k] = a[k];
+            b00[k] = b[k];
+            c00[k] = c[k];
+        }
+        const double ghost = 2 * yu[0] - yp[0];  // mirrored ghost, as yp_pad[0] of mk_P_abc
+        b00[0] -= 2.0 * (1.0 / (yu[1] - yu[0])) / (yp[0] - ghost);
+        return PRJ_OK;
+    }
+    return fail(PRJ_ERR_ARG, "unknown band mode %d", mode);
+}
+
+int prj_metrics_from_yu(int ny, const double* yu, double* inv_dy_p, double* dPdy_lo, double* dPdy_hi) {
+    if (ny < 2) return fail(PRJ_ERR_ARG, "ny=%d < 2", ny);
+    if (!yu || !inv_dy_p || !dPdy_lo || !dPdy_hi) return fail(PRJ_ERR_ARG, "NULL argument");
+    for (int i = 0; i < ny; i++) {
+        if (!(yu[i + 1] > yu[i])) return fail(PRJ_ERR_ARG, "yu must increase strictly (yu[%d] >= yu[%d])", i, i + 1);
+        inv_dy_p[i] = 1. / (yu[i + 1] - yu[i]);
+    }
+    dPdy_lo[0] = 0.0;
+    dPdy_hi[0] = 0.0;
+    for (int i = 1; i < ny; i++) {
+        const double dy = (yu[i] + yu[i + 1]) / 2 - (yu[i - 1] + yu[i]) / 2;
+        dPdy_lo[i] = -1 / dy;
+        dPdy_hi[i] = 1 / dy;
+    }
+    return PRJ_OK;
+}
+
+int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* band_a, const double* band_b,
+                    const double* band_c, const double* band_a00, const double* band_b00, const double* band_c00,
+                    const double* inv_dy_p, const double* dPdy_lo, const double* dPdy_hi, unsigned flags, int device,
+                    prj_plan** out) {
+    if (!out) return fail(PRJ_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (nx < 1 || nx > 8192) return fail(PRJ_ERR_ARG, "nx=%d outside [1, 8192]", nx);
+    if (nz < 1 || nz > 4094) return fail(PRJ_ERR_ARG, "nz=%d outside [1, 4094]", nz);
+    if (ny < 2 || ny > 65536) return fail(PRJ_ERR_ARG, "ny=%d outside [2, 65536] (ny_glob < 2 is rejected as in the reference)", ny);
+    if (!(dx > 0) || !(dz > 0) || !std::isfinite(dx) || !std::isfinite(dz))
+        return fail(PRJ_ERR_ARG, "dx=%g, dz=%g must be finite and positive", dx, dz);
+    if (!band_a || !band_b || !band_c || !band_a00 || !band_b00 || !band_c00)
+        return fail(PRJ_ERR_ARG, "band pointer is NULL");
+    const int nmet = (inv_dy_p != nullptr) + (dPdy_lo != nullptr) + (dPdy_hi != nullptr);
+    if (nmet != 0 && nmet != 3) return fail(PRJ_ERR_ARG, "inv_dy_p, dPdy_lo, dPdy_hi must be all set or all NULL");
+    if (flags != PRJ_FLAG_NONE) return fail(PRJ_ERR_ARG, "unknown flags 0x%x", flags);
+    const double* bandv[6] = {band_a, band_b, band_c, band_a00, band_b00, band_c00};
+    for (int i = 0; i < 6; i++)
+        if (!finite_all(bandv[i], ny)) return fail(PRJ_ERR_ARG, "band array %d holds a non-finite value", i);
+    if (nmet == 3 && (!finite_all(inv_dy_p, ny) || !finite_all(dPdy_lo, ny) || !finite_all(dPdy_hi, ny)))
+        return fail(PRJ_ERR_ARG, "a 1-D metric holds a non-finite value");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PRJ_ERR_CUDA, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(PRJ_ERR_ARG, "device %d outside [0, %d)", device, ndev);
+    DeviceGuard dg(device);
+
+    prj_plan* pl = new prj_plan();
+    pl->device = device;
+    pl->flags = flags;
+    pl->has_metrics = (nmet == 3);
+    prj::Geometry& g = pl->g;
+    g.nx = nx; g.nz = nz; g.ny = ny; g.dx = dx; g.dz = dz;
+    g.nxh = nx / 2 + 1;
+    g.nzh = nz / 2 + 1;
+    g.mzp = (g.nzh + 1) / 2 * 2;
+    size_t bytes = 0;
+    int rc = PRJ_OK;
+    auto bail = [&](int code) {
+        free_plan_buffers(pl);
+        delete pl;
+        return code;
+    };
+    if ((rc = make_rfft<double>(nx, &pl->fx64, &bytes))) return bail(rc);
+    if ((rc = make_cfft<double>(nz, &pl->fz64.f, &pl->fz64.tw, &bytes))) return bail(rc);
+
+    // rows per CTA of the x kernels: fit two ping-pong buffers in ~100 KB
+    {
+        const size_t per_row = (size_t)2 * (pl->fx64.m + 1) * sizeof(double2);
+        int tz = (int)((100 * 1024) / per_row);
+        if (tz > 16) tz = 16;
+        if (tz < 1) tz = 1;
+        if (per_row * tz > 200 * 1024) return bail(fail(PRJ_ERR_UNSUPPORTED, "nx=%d too large for one CTA", nx));
+        pl->tz_fwd = tz;
+    }
+
+    // wavenumber tables, poisson_solver_multigpu.f90:147-148
+    const double const_pi = 4.0 * std::atan(1.0);
+    const double inv_dx = 1.0 / dx, inv_dz = 1.0 / dz;
+    std::vector<double> ax(g.nxh), az(g.nzh);
+    for (int i = 0; i < g.nxh; i++) {
+        const double s = std::sin(i * const_pi / nx);
+        ax[i] = -4 * (inv_dx * inv_dx) * (s * s);
+    }
+    for (int j = 0; j < g.nzh; j++) {
+        const double s = std::sin(j * const_pi / nz);
+        az[j] = -4 * (inv_dz * inv_dz) * (s * s);
+    }
+    std::vector<double> bands((size_t)6 * ny);
+    for (int i = 0; i < 6; i++) std::memcpy(&bands[(size_t)i * ny], bandv[i], sizeof(double) * ny);
+
+    auto up = [&](double** d, const double* h, size_t n, const char* what) -> int {
+        cudaError_t e = cudaMalloc((void**)d, n * sizeof(double));
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        bytes += n * sizeof(double);
+        e = cudaMemcpy(*d, h, n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        return PRJ_OK;
+    };
+    if ((rc = up(&pl->t.bands, bands.data(), bands.size(), "bands"))) return bail(rc);
+    if ((rc = up(&pl->t.ax, ax.data(), ax.size(), "a_x"))) return bail(rc);
+    if ((rc = up(&pl->t.az, az.data(), az.size(), "a_z"))) return bail(rc);
+    if (pl->has_metrics) {
+        if ((rc = up(&pl->t.inv_dy_p, inv_dy_p, ny, "inv_dy_p"))) return bail(rc);
+        if ((rc = up(&pl->t.dpdy_lo, dPdy_lo, ny, "dPdy_lo"))) return bail(rc);
+        if ((rc = up(&pl->t.dpdy_hi, dPdy_hi, ny, "dPdy_hi"))) return bail(rc);
+    }
+    const size_t spec_elems = (size_t)ny * g.nxh * nz;
+    const size_t piv_elems = (size_t)ny * g.nxh * g.mzp;
+    cudaError_t e;
+    if ((e = cudaMalloc((void**)&pl->spec, spec_elems * sizeof(double2))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(spectrum)"));
+    bytes += spec_elems * sizeof(double2);
+    if ((e = cudaMalloc((void**)&pl->t.piv, piv_elems * sizeof(double))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(pivots)"));
+    bytes += piv_elems * sizeof(double);
+    if ((e = cudaMalloc((void**)&pl->stat_buf, 8 * sizeof(double))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(stats)"));
+    bytes += 8 * sizeof(double);
+    if ((e = prj::launch_build_pivots(pl, 0)) != cudaSuccess) return bail(cuda_fail(e, "pivot table"));
+    double mp = 0;
+    if ((e = cudaMemcpy(&mp, pl->stat_buf, sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return bail(cuda_fail(e, "pivot table"));
+    pl->min_pivot = mp;
+    if (!(mp > 0) || !std::isfinite(mp))
+        return bail(fail(PRJ_ERR_NUMERIC, "zero or non-finite Thomas pivot (min_abs_div_bacp = %g)", mp));
+    pl->device_bytes = bytes;
+    *out = pl;
+    return PRJ_OK;
+}
+
+int prj_plan_destroy(prj_plan* plan) {
+    if (!plan) return PRJ_OK;
+    DeviceGuard dg(plan->device);
+    cudaDeviceSynchronize();
+    release_events(plan);
+    free_plan_buffers(plan);
+    delete plan;
+    return PRJ_OK;
+}
+
+int prj_plan_min_pivot(const prj_plan* plan, double* out) {
+    if (!plan || !out) return fail(PRJ_ERR_ARG, "NULL argument");
+    *out = plan->min_pivot;
+    return PRJ_OK;
+}
+
+int prj_plan_device_bytes(const prj_plan* plan, size_t* out) {
+    if (!plan || !out) return fail(PRJ_ERR_ARG, "NULL argument");
+    *out = plan->device_bytes + plan->host_stage_elems * sizeof(double);
+    return PRJ_OK;
+}
+
+int prj_plan_enable_stage_timing(prj_plan* plan, int enable) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    plan->timing = enable != 0;
+    return PRJ_OK;
+}
+
+int prj_plan_stage_times(prj_plan* plan, double* ms, int* launches, int max_stages, int* n_stages) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!ms || !launches || max_stages <= 0) return fail(PRJ_ERR_ARG, "NULL or empty output");
+    DeviceGuard dg(plan->device);
+    for (int i = 0; i < max_stages; i++) { ms[i] = 0.0; launches[i] = 0; }
+    int top = 0;
+    cudaError_t err = cudaSuccess;
+    for (auto& r : plan->rec) {
+        float t = 0.f;
+        cudaError_t e = cudaEventSynchronize(r.t1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.t0, r.t1);
+        if (e != cudaSuccess && err == cudaSuccess) err = e;
+        if (r.stage < max_stages) {
+            ms[r.stage] += t;
+            launches[r.stage] += 1;
+            if (r.stage + 1 > top) top = r.stage + 1;
+        }
+        plan->event_pool.push_back(r.t0);
+        plan->event_pool.push_back(r.t1);
+    }
+    plan->rec.clear();
+    if (n_stages) *n_stages = top;
+    if (err != cudaSuccess) return cuda_fail(err, "stage timing");
+    return PRJ_OK;
+}
+
+const char* prj_stage_name(int stage) {
+    switch (stage) {
+    case prj::kStFwdX: return "k_fwd_x";
+    case prj::kStZSolve: return "k_zsolve";
+    case prj::kStBwdX: return "k_bwd_x";
+    case prj::kStCorrect: return "k_correct";
+    case prj::kStStats: return "k_stats";
+    default: return "";
+    }
+}
+
+int prj_poisson_fp64(prj_plan* plan, double* d_P, void* stream) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!d_P) return fail(PRJ_ERR_ARG, "P is NULL");
+    DeviceGuard dg(plan->device);
+    return run_poisson(plan, d_P, (cudaStream_t)stream);
+}
+
+int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, const double* d_Wh, double* d_U,
+                        double* d_V, double* d_W, double* d_P, const prj_step_params* params, int mode,
+                        prj_stats* stats, void* stream) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!plan->has_metrics) return fail(PRJ_ERR_STATE, "plan was created without inv_dy_p / dPdy (Poisson-only)");
+    if (!d_Uh || !d_Vh || !d_Wh || !d_U || !d_V || !d_W || !d_P || !params)
+        return fail(PRJ_ERR_ARG, "NULL array or params");
+    if (!(params->dt > 0) || !std::isfinite(params->dt)) return fail(PRJ_ERR_ARG, "dt=%g must be finite and positive", params->dt);
+    if (mode != PRJ_MODE_FP64 && mode != PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_ARG, "unknown mode %d", mode);
+    if (mode == PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_UNSUPPORTED, "mixed-precision mode not built yet");
+    DeviceGuard dg(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    prj::StepScalars sc{};
+    sc.dt = params->dt;
+    sc.inv_dt = 1.0 / params->dt;
+    sc.wall[0] = params->wall_U_bot; sc.wall[1] = params->wall_V_bot; sc.wall[2] = params->wall_W_bot;
+    sc.wall[3] = params->wall_U_top; sc.wall[4] = params->wall_V_top; sc.wall[5] = params->wall_W_top;
+    {
+        StageTimer tm(plan, prj::kStFwdX, st);
+        CK(prj::launch_fwd_x(plan, prj::FwdSource::Divergence, nullptr, d_Uh, d_Vh, d_Wh, &sc, st), "divergence + forward x");
+    }
+    {
+        StageTimer tm(plan, prj::kStZSolve, st);
+        CK(prj::launch_zsolve(plan, st), "z transform + Thomas");
+    }
+    {
+        StageTimer tm(plan, prj::kStBwdX, st);
+        CK(prj::launch_bwd_x(plan, d_P, st), "inverse x");
+    }
+    {
+        StageTimer tm(plan, prj::kStCorrect, st);
+        CK(prj::launch_correction(plan, d_P, d_Uh, d_Vh, d_Wh, d_U, d_V, d_W, sc, st), "correction");
+    }
+    if (stats || params->compute_stats) {
+        {
+            StageTimer tm(plan, prj::kStStats, st);
+            CK(prj::launch_stats(plan, d_U, d_V, d_W, d_P, plan->stat_buf + 2, st), "stats");
+        }
+        double h[2] = {-1, -1};
+        CK(cudaMemcpyAsync(h, plan->stat_buf + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "stats copy");
+        CK(cudaStreamSynchronize(st), "stats sync");
+        if (stats) {
+            stats->div_maxabs = h[0];
+            stats->p_maxabs = h[1];
+            stats->min_pivot = plan->min_pivot;
+            stats->refine_iters = 0;
+            stats->fp64_lines = plan->g.nxh * plan->g.nz;
+            stats->last_update_rel = 0.0;
+        }
+        if (!std::isfinite(h[0]) || !std::isfinite(h[1])) return fail(PRJ_ERR_NUMERIC, "NaN detected in the projection");
+    }
+    return PRJ_OK;
+}
+
+int prj_poisson_fp64_host(prj_plan* plan, double* h_P) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!h_P) return fail(PRJ_ERR_ARG, "P is NULL");
+    DeviceGuard dg(plan->device);
+    const size_t n = (size_t)plan->g.nx * plan->g.nz * plan->g.ny;
+    if ((rc = ensure_host_stage(plan, n))) return rc;
+    double* d = plan->host_stage;
+    CK(cudaMemcpy(d, h_P, n * sizeof(double), cudaMemcpyHostToDevice), "copy P to device");
+    if ((rc = run_poisson(plan, d, 0))) return rc;
+    CK(cudaMemcpy(h_P, d, n * sizeof(double), cudaMemcpyDeviceToHost), "copy P to host");
+    return PRJ_OK;
+}
+
+int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h_Vh, const double* h_Wh, double* h_U,
+                             double* h_V, double* h_W, double* h_P, const prj_step_params* params, int mode,
+                             prj_stats* stats) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!h_Uh || !h_Vh || !h_Wh || !h_U || !h_V || !h_W || !h_P || !params) return fail(PRJ_ERR_ARG, "NULL argument");
+    DeviceGuard dg(plan->device);
+    const prj::Geometry& g = plan->g;
+    const size_t nh = (size_t)(g.nx + 2) * (g.nz + 2) * (g.ny + 2);
+    const size_t np = (size_t)g.nx * g.nz * g.ny;
+    if ((rc = ensure_host_stage(plan, 6 * nh + np))) return rc;
+    double* d = plan->host_stage;
+    double *dUh = d, *dVh = d + nh, *dWh = d + 2 * nh, *dU = d + 3 * nh, *dV = d + 4 * nh, *dW = d + 5 * nh,
+           *dP = d + 6 * nh;
+    CK(cudaMemcpy(dUh, h_Uh, nh * sizeof(double), cudaMemcpyHostToDevice), "copy Uh");
+    CK(cudaMemcpy(dVh, h_Vh, nh * sizeof(double), cudaMemcpyHostToDevice), "copy Vh");
+    CK(cudaMemcpy(dWh, h_Wh, nh * sizeof(double), cudaMemcpyHostToDevice), "copy Wh");
+    if ((rc = prj_projection_step(plan, dUh, dVh, dWh, dU, dV, dW, dP, params, mode, stats, 0))) return rc;
+    CK(cudaMemcpy(h_U, dU, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy U");
+    CK(cudaMemcpy(h_V, dV, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy V");
+    CK(cudaMemcpy(h_W, dW, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy W");
+    CK(cudaMemcpy(h_P, dP, np * sizeof(double), cudaMemcpyDeviceToHost), "copy P");
+    return PRJ_OK;
+}
+
+}  // extern "C"

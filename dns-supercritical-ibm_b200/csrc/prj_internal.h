@@ -1,0 +1,107 @@
+// prj_internal.h -- plan layout and kernel launchers shared by the engine's
+// translation units.  Not part of the public ABI (include/projection.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "fft_device.cuh"
+
+namespace prj {
+
+// One real-to-complex transform of length n along a contiguous axis, done as a
+// complex FFT of length m (m = n/2 for even n, packed even/odd samples; m = n
+// for odd n) plus a post-processing pass.  `nh` = n/2+1 spectral modes.
+template <typename T>
+struct RealFftPlan {
+    int n = 0, m = 0, nh = 0;
+    bool even = false;
+    FftDev f{};                                  // complex FFT of length m
+    typename C2<T>::t* tw = nullptr;             // stage twiddles (device)
+    typename C2<T>::t* post = nullptr;           // exp(-2 pi i k / n), k = 0..m (device, even n only)
+};
+
+template <typename T>
+struct ComplexFftPlan {
+    FftDev f{};
+    typename C2<T>::t* tw = nullptr;
+};
+
+// Spectral layout: X[y][kx][z] complex, kx in [0, nxh), z in [0, nz).
+// Pivot table: D[y][kx][kzs], kzs in [0, mzp) covers the folded z wavenumber
+// min(kz, nz - kz) = 0..nz/2 (padded to an even count).
+struct Geometry {
+    int nx, nz, ny;
+    int nxh;      // nx/2 + 1
+    int nzh;      // nz/2 + 1
+    int mzp;      // nzh rounded up to a multiple of 2
+    double dx, dz;
+};
+
+struct DeviceTables {
+    double* bands = nullptr;     // a, b, c, a00, b00, c00 (6 ny)
+    double* inv_dy_p = nullptr;  // ny
+    double* dpdy_lo = nullptr;   // ny
+    double* dpdy_hi = nullptr;   // ny
+    double* ax = nullptr;        // nxh: -4/dx^2 sin^2(kx pi / nx)
+    double* az = nullptr;        // nzh: -4/dz^2 sin^2(kzs pi / nz)
+    double* piv = nullptr;       // D[y][kx][kzs]: Thomas pivots b + lambda - a c'
+};
+
+}  // namespace prj
+
+namespace prj {
+// stage ids of the per-kernel timing record
+enum Stage { kStFwdX = 0, kStZSolve = 1, kStBwdX = 2, kStCorrect = 3, kStStats = 4, kNumStages = 8 };
+
+struct StageRecord {
+    int stage;
+    cudaEvent_t t0, t1;
+};
+}  // namespace prj
+
+struct prj_plan {
+    int device = 0;
+    bool timing = false;
+    std::vector<prj::StageRecord> rec;       // events of the enabled timing window
+    std::vector<cudaEvent_t> event_pool;     // reusable events
+    double* host_stage = nullptr;            // device staging of the host-buffer entry points
+    size_t host_stage_elems = 0;
+    unsigned flags = 0;
+    bool has_metrics = false;
+    prj::Geometry g{};
+    prj::DeviceTables t{};
+    prj::RealFftPlan<double> fx64;
+    prj::ComplexFftPlan<double> fz64;
+    double2* spec = nullptr;      // X[y][kx][z] complex FP64 (scratch of the solve)
+    double* stat_buf = nullptr;   // device reduction slots
+    double min_pivot = 0.0;
+    size_t device_bytes = 0;
+    int tz_fwd = 1;               // rows per CTA of the x-transform kernels
+};
+
+namespace prj {
+
+// Kernel launchers (prj_kernels.cu).  All are asynchronous on `st`.
+enum class FwdSource { Pressure, Divergence };
+
+struct StepScalars {
+    double dt, inv_dt;
+    double wall[6];  // U_bot, V_bot, W_bot, U_top, V_top, W_top
+};
+
+cudaError_t launch_fwd_x(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
+                         const double* Wh, const StepScalars* sc, cudaStream_t st);
+cudaError_t launch_zsolve(const prj_plan* pl, cudaStream_t st);
+cudaError_t launch_bwd_x(const prj_plan* pl, double* P, cudaStream_t st);
+cudaError_t launch_correction(const prj_plan* pl, const double* P, const double* Uh, const double* Vh,
+                              const double* Wh, double* U, double* V, double* W, const StepScalars& sc,
+                              cudaStream_t st);
+cudaError_t launch_build_pivots(const prj_plan* pl, cudaStream_t st);
+cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, const double* W, const double* P,
+                         double* out2, cudaStream_t st);
+cudaError_t launch_min_abs(const double* x, size_t n, double* out, cudaStream_t st);
+
+}  // namespace prj

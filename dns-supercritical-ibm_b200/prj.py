@@ -1,0 +1,332 @@
+"""ctypes harness of the B200 pressure-projection engine (libprj_b200.so).
+
+Two faces over the same C ABI (include/projection.h):
+
+* ``Plan`` -- Pythonic: build from the face grid ``yu`` (or explicit band
+  arrays), then ``poisson_fp64(P)`` / ``projection_step(...)`` on torch CUDA
+  tensors (device-resident, asynchronous on the current stream) or on numpy
+  arrays (host buffers; copies in and out).
+* ``init_spec_poisson_multigpu`` / ``run_spec_poisson_multigpu`` -- the two
+  entry points of the reference's Fortran module ``poisson_solver_multigpu``
+  (src/poisson_solver_mgpu_dtdma/poisson_solver_multigpu.f90:33, :328) with
+  their argument meaning kept for the single-rank case: the first builds the
+  solver from the bands and grid spacings, the second overwrites P (RHS in,
+  solution out).
+
+Layouts follow the reference: numpy arrays are Fortran-ordered ``[x, z, y]``;
+torch tensors use the same memory as C-contiguous ``[y, z, x]``.
+
+The engine has no CPU fallback: if the library is missing or no GPU is
+visible, creating a plan raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libprj_b200.so")
+
+PRJ_OK = 0
+PRJ_ERR_ARG = -1
+PRJ_ERR_UNSUPPORTED = -2
+PRJ_ERR_CUDA = -3
+PRJ_ERR_OOM = -4
+PRJ_ERR_NUMERIC = -5
+PRJ_ERR_TIMEOUT = -6
+PRJ_ERR_STATE = -7
+
+MODE_FP64 = 0
+MODE_FP32_REFINE = 1
+
+# every symbol include/projection.h declares
+EXPORTS = (
+    "prj_plan_create", "prj_plan_destroy", "prj_poisson_fp64", "prj_projection_step",
+    "prj_poisson_fp64_host", "prj_projection_step_host", "prj_plan_min_pivot",
+    "prj_plan_device_bytes", "prj_last_error_string", "prj_version",
+    "prj_bands_from_yu", "prj_metrics_from_yu",
+    "prj_plan_enable_stage_timing", "prj_plan_stage_times", "prj_stage_name",
+)
+
+BANDS_REFERENCE = 0
+BANDS_CONSISTENT = 1
+
+
+class PrjError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"prj error {code}: {msg}")
+        self.code = code
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("div_maxabs", ctypes.c_double), ("p_maxabs", ctypes.c_double),
+                ("min_pivot", ctypes.c_double), ("refine_iters", ctypes.c_int),
+                ("fp64_lines", ctypes.c_int), ("last_update_rel", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double),
+                ("wall_U_bot", ctypes.c_double), ("wall_V_bot", ctypes.c_double), ("wall_W_bot", ctypes.c_double),
+                ("wall_U_top", ctypes.c_double), ("wall_V_top", ctypes.c_double), ("wall_W_top", ctypes.c_double),
+                ("compute_stats", ctypes.c_int)]
+
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load libprj_b200.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    path = path or LIB_PATH
+    if path == LIB_PATH:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("_prj_build", os.path.join(HERE, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        if mod.needs_build():
+            mod.build()
+    if not os.path.exists(path):
+        raise RuntimeError(f"engine library missing: {path} (run dns-supercritical-ibm_b200/build.py)")
+    L = ctypes.CDLL(path)
+    i, d, u = ctypes.c_int, ctypes.c_double, ctypes.c_uint
+    L.prj_plan_create.argtypes = [i, i, i, d, d, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, u, i, ctypes.POINTER(_vp)]
+    L.prj_plan_destroy.argtypes = [_vp]
+    L.prj_poisson_fp64.argtypes = [_vp, _vp, _vp]
+    L.prj_projection_step.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams), i,
+                                      ctypes.POINTER(Stats), _vp]
+    L.prj_poisson_fp64_host.argtypes = [_vp, _dp]
+    L.prj_projection_step_host.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.POINTER(StepParams), i,
+                                           ctypes.POINTER(Stats)]
+    L.prj_plan_min_pivot.argtypes = [_vp, _dp]
+    L.prj_plan_device_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.prj_bands_from_yu.argtypes = [i, _dp, i, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.prj_metrics_from_yu.argtypes = [i, _dp, _dp, _dp, _dp]
+    L.prj_plan_enable_stage_timing.argtypes = [_vp, i]
+    L.prj_plan_stage_times.argtypes = [_vp, _dp, ctypes.POINTER(ctypes.c_int), i, ctypes.POINTER(ctypes.c_int)]
+    L.prj_stage_name.argtypes = [i]
+    for name in EXPORTS:
+        getattr(L, name).restype = ctypes.c_int
+    L.prj_last_error_string.restype = ctypes.c_char_p
+    L.prj_version.restype = ctypes.c_char_p
+    L.prj_stage_name.restype = ctypes.c_char_p
+    if path == LIB_PATH:
+        _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != PRJ_OK:
+        raise PrjError(rc, load_library().prj_last_error_string().decode())
+
+
+def _arr(v, n=None):
+    a = np.ascontiguousarray(v, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _is_tensor(x):
+    try:
+        torch = _torch()
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(x, torch.Tensor)
+
+
+def _stream_ptr(stream):
+    if stream is not None:
+        return ctypes.c_void_p(int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream))
+    torch = _torch()
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def bands(yu, mode="reference"):
+    """(a, b, c, a00, b00, c00) from the face grid (prj_bands_from_yu; host-only).
+
+    mode "reference": calc_bands.mk_P_abc; "consistent": div(grad p) bands."""
+    yu = _arr(yu)
+    ny = yu.size - 1
+    out = [np.zeros(ny) for _ in range(6)]
+    m = {"reference": BANDS_REFERENCE, "consistent": BANDS_CONSISTENT}[mode]
+    _check(load_library().prj_bands_from_yu(ny, _p(yu), m, *[_p(v) for v in out]))
+    return tuple(out)
+
+
+def metrics(yu):
+    """(inv_dy_p, dPdy_lo, dPdy_hi) from the face grid (prj_metrics_from_yu; host-only)."""
+    yu = _arr(yu)
+    ny = yu.size - 1
+    out = [np.zeros(ny) for _ in range(3)]
+    _check(load_library().prj_metrics_from_yu(ny, _p(yu), *[_p(v) for v in out]))
+    return tuple(out)
+
+
+@dataclass
+class Grid:
+    nx: int
+    nz: int
+    ny: int
+    dx: float
+    dz: float
+
+
+class Plan:
+    """A solver plan on one GPU (prj_plan_create / prj_plan_destroy)."""
+
+    def __init__(self, nx, nz, ny, dx, dz, bands6, metrics3=None, device=0):
+        L = load_library()
+        b = [_arr(v, ny) for v in bands6]
+        m = [_arr(v, ny) for v in metrics3] if metrics3 is not None else [None, None, None]
+        h = _vp()
+        _check(L.prj_plan_create(nx, nz, ny, float(dx), float(dz), *[_p(v) for v in b], *[_p(v) for v in m], 0,
+                                 device, ctypes.byref(h)))
+        self._h = h
+        self.grid = Grid(nx, nz, ny, float(dx), float(dz))
+        self.device = device
+        self.has_metrics = metrics3 is not None
+
+    @classmethod
+    def from_yu(cls, nx, nz, dx, dz, yu, band_mode="reference", device=0):
+        """Build bands and metrics from the face grid ``yu`` (ny+1 values)."""
+        yu = np.asarray(yu, dtype=np.float64)
+        return cls(nx, nz, len(yu) - 1, dx, dz, bands(yu, band_mode), metrics(yu), device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().prj_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise PrjError(PRJ_ERR_STATE, "plan destroyed")
+        return self._h
+
+    @property
+    def min_pivot(self) -> float:
+        v = ctypes.c_double()
+        _check(load_library().prj_plan_min_pivot(self.handle, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def device_bytes(self) -> int:
+        v = ctypes.c_size_t()
+        _check(load_library().prj_plan_device_bytes(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def enable_stage_timing(self, on=True):
+        _check(load_library().prj_plan_enable_stage_timing(self.handle, 1 if on else 0))
+
+    def stage_times(self):
+        """{kernel name: (total ms, launches)} recorded since the last call (synchronises)."""
+        L = load_library()
+        n = 8
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int * n)()
+        ns = ctypes.c_int()
+        _check(L.prj_plan_stage_times(self.handle, ms, cnt, n, ctypes.byref(ns)))
+        return {L.prj_stage_name(i).decode(): (ms[i], cnt[i]) for i in range(ns.value) if cnt[i]}
+
+    # ---------------------------------------------------------------- solve
+    def poisson_fp64(self, P, stream=None):
+        """In-place FP64 solve.  torch CUDA tensor [y, z, x] (async) or numpy [x, z, y] F-order (sync)."""
+        g = self.grid
+        L = load_library()
+        if _is_tensor(P):
+            torch = _torch()
+            if not (P.is_cuda and P.dtype == torch.float64 and P.is_contiguous() and tuple(P.shape) == (g.ny, g.nz, g.nx)):
+                raise ValueError("P must be a contiguous float64 CUDA tensor of shape (ny, nz, nx)")
+            _check(L.prj_poisson_fp64(self.handle, ctypes.c_void_p(P.data_ptr()), _stream_ptr(stream)))
+            return P
+        if not (isinstance(P, np.ndarray) and P.dtype == np.float64 and P.flags.f_contiguous and P.shape == (g.nx, g.nz, g.ny)):
+            raise ValueError("P must be a Fortran-ordered float64 array of shape (nx, nz, ny)")
+        _check(L.prj_poisson_fp64_host(self.handle, _p(P)))
+        return P
+
+    def projection_step(self, Uh, Vh, Wh, U, V, W, P, dt, mode=MODE_FP64, wall=(0.0,) * 6, stats=True, stream=None):
+        """One projection.  All torch CUDA tensors (halo'd [y+2, z+2, x+2], P [y, z, x]) or all numpy
+        (halo'd F-order [x+2, z+2, y+2], P [x, z, y]).  Returns a Stats dict (or None if stats=False)."""
+        g = self.grid
+        L = load_library()
+        par = StepParams(float(dt), *[float(w) for w in wall], 1 if stats else 0)
+        st = Stats()
+        sp = ctypes.byref(st) if stats else None
+        if _is_tensor(Uh):
+            torch = _torch()
+            hs = (g.ny + 2, g.nz + 2, g.nx + 2)
+            for t in (Uh, Vh, Wh, U, V, W):
+                if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and tuple(t.shape) == hs):
+                    raise ValueError(f"halo'd fields must be contiguous float64 CUDA tensors of shape {hs}")
+            if not (P.is_cuda and P.dtype == torch.float64 and P.is_contiguous() and tuple(P.shape) == (g.ny, g.nz, g.nx)):
+                raise ValueError("P must be a contiguous float64 CUDA tensor of shape (ny, nz, nx)")
+            ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+            _check(L.prj_projection_step(self.handle, ptr(Uh), ptr(Vh), ptr(Wh), ptr(U), ptr(V), ptr(W), ptr(P),
+                                         ctypes.byref(par), mode, sp, _stream_ptr(stream)))
+        else:
+            hs = (g.nx + 2, g.nz + 2, g.ny + 2)
+            for a in (Uh, Vh, Wh, U, V, W):
+                if not (a.dtype == np.float64 and a.flags.f_contiguous and a.shape == hs):
+                    raise ValueError(f"halo'd fields must be Fortran-ordered float64 arrays of shape {hs}")
+            if not (P.dtype == np.float64 and P.flags.f_contiguous and P.shape == (g.nx, g.nz, g.ny)):
+                raise ValueError("P must be a Fortran-ordered float64 array of shape (nx, nz, ny)")
+            _check(L.prj_projection_step_host(self.handle, _p(Uh), _p(Vh), _p(Wh), _p(U), _p(V), _p(W), _p(P),
+                                              ctypes.byref(par), mode, sp))
+        return st.as_dict() if stats else None
+
+
+# ------------------------------------------------------------------------------
+# Mirror of the reference's Fortran module interface (single rank)
+# ------------------------------------------------------------------------------
+
+def init_spec_poisson_multigpu(P_band_a, P_band_b, P_band_c, P_band_a_00, P_band_b_00, P_band_c_00,
+                               nx_glob, nz_glob, ny_loc, inv_dx, inv_dz, mpi_divs_z=1, mpi_divs_y=1, device=0):
+    """Build the solver (init_spec_poisson_multigpu, poisson_solver_multigpu.f90:33-326).
+
+    Arguments keep the reference's meaning; the FFT plans, a_x/a_z tables and
+    the pivot table live inside the returned plan.  More than one rank is
+    rejected (the reference would run its DTDMA path; the engine holds all of
+    y on one GPU).  Prints the reference's min_abs_div_bacp INFO line.
+    """
+    if mpi_divs_z * mpi_divs_y != 1:
+        raise PrjError(PRJ_ERR_UNSUPPORTED, "the engine runs one rank per solve (mpi_divs_z = mpi_divs_y = 1)")
+    plan = Plan(nx_glob, nz_glob, ny_loc, 1.0 / inv_dx, 1.0 / inv_dz,
+                (P_band_a, P_band_b, P_band_c, P_band_a_00, P_band_b_00, P_band_c_00), None, device)
+    print(f"{'INFO: init_spec_poisson_multigpu, min_abs_div_bacp: ':>52}{plan.min_pivot:14.6E}", flush=True)
+    return plan
+
+
+def run_spec_poisson_multigpu(plan: Plan, P):
+    """Solve in place (run_spec_poisson_multigpu, poisson_solver_multigpu.f90:328-554)."""
+    return plan.poisson_fp64(P)

@@ -1,0 +1,88 @@
+"""Seeded synthetic workloads of the channel projection (no dataset is involved).
+
+The reference measures on user cases (``input/yu.txt`` + restart files); these
+generators stand in for them with the shapes, grids and value distributions of
+the channel configurations the engine is benchmarked on.
+
+Layout: numpy arrays indexed ``[x, z, y]`` in Fortran order (x fastest, the
+reference's ``P(i, j, k)``); halo'd fields are ``(nx+2, nz+2, ny+2)``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def tanh_faces(ny: int, beta: float = 2.0) -> np.ndarray:
+    """Faces y_j = 1 + tanh(beta (2j/ny - 1)) / tanh(beta), j = 0..ny; walls at y = 0 and 2."""
+    j = np.arange(ny + 1, dtype=np.float64)
+    return 1.0 + np.tanh(beta * (2.0 * j / ny - 1.0)) / np.tanh(beta)
+
+
+def wall_refined_faces(ny: int, h_uniform: float = 0.1, growth: float = 0.015) -> np.ndarray:
+    """Faces uniform for y < h_uniform, then growing by ``growth`` per cell toward the
+    centre, mirrored about y = 1 (walls at 0 and 2).  ny must be even."""
+    if ny % 2:
+        raise ValueError("ny must be even")
+    half = ny // 2
+    # find the first spacing d0 such that the half channel closes at y = 1
+    def total(d0):
+        y, d, out = 0.0, d0, [0.0]
+        for _ in range(half):
+            y += d
+            out.append(y)
+            if y >= h_uniform:
+                d *= 1.0 + growth
+        return y, out
+    lo, hi = 1e-9, 1.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if total(mid)[0] > 1.0:
+            hi = mid
+        else:
+            lo = mid
+    _, half_faces = total(0.5 * (lo + hi))
+    h = np.array(half_faces) / half_faces[-1]
+    return np.concatenate([h, 2.0 - h[-2::-1]])
+
+
+def channel_spacing(nx: int, nz: int, lx: float = 2 * np.pi, lz: float = np.pi):
+    return lx / nx, lz / nz
+
+
+def poisson_rhs(nx: int, ny: int, nz: int, beta: float = 2.0, seed: int = 0):
+    """Poisson case: uniform[-1,1] RHS minus its dy-weighted mean on tanh faces.
+
+    Lx = 2 pi, Lz = pi.  Returns (rhs [x, z, y] F-order, yu, dx, dz)."""
+    yu = tanh_faces(ny, beta)
+    dx, dz = channel_spacing(nx, nz)
+    rng = np.random.default_rng(seed)
+    rhs = rng.uniform(-1.0, 1.0, size=(nx, nz, ny))
+    w = np.diff(yu)
+    rhs -= (rhs.sum(axis=(0, 1)) * w).sum() / (nx * nz * w.sum())
+    return np.asfortranarray(rhs), yu, dx, dz
+
+
+def projection_inputs(nx: int, ny: int, nz: int, beta: float = 2.0, seed: int = 1, sigma: float = 0.1, yu=None):
+    """Predictor field of the channel projection: Poiseuille u = 1.5 (1 - (y-1)^2) plus
+    N(0, sigma) noise in u, v, w (drawn in that order from default_rng(seed)); v = 0 on
+    both walls.  Interior values only (the engine wraps periodic halos itself).
+
+    Returns (Uh, Vh, Wh, yu, dx, dz)."""
+    if yu is None:
+        yu = tanh_faces(ny, beta)
+    yp = (yu[:-1] + yu[1:]) / 2
+    dx, dz = channel_spacing(nx, nz)
+    rng = np.random.default_rng(seed)
+    shape = (nx + 2, nz + 2, ny + 2)
+    Uh = np.zeros(shape, order="F")
+    Vh = np.zeros(shape, order="F")
+    Wh = np.zeros(shape, order="F")
+    Uh[1:-1, 1:-1, 1:-1] = 1.5 * (1.0 - (yp[None, None, :] - 1.0) ** 2) + rng.normal(0.0, sigma, size=(nx, nz, ny))
+    Vh[1:-1, 1:-1, 1:-1] = rng.normal(0.0, sigma, size=(nx, nz, ny))
+    Wh[1:-1, 1:-1, 1:-1] = rng.normal(0.0, sigma, size=(nx, nz, ny))
+    Vh[:, :, 1] = 0.0  # V(k = 0) is the bottom wall face
+    return Uh, Vh, Wh, yu, dx, dz
+
+
+def halo_shape(nx, nz, ny):
+    return (nx + 2, nz + 2, ny + 2)

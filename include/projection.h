@@ -1,0 +1,179 @@
+/*
+ * projection.h -- C ABI of the B200 pressure-projection engine.
+ *
+ * The engine replaces, on one GPU, the pressure projection of the channel DNS
+ * Rafael10Diez/DNS-Supercritical-IBM: the predictor divergence, the FFT-based
+ * pressure Poisson solve (periodic x and z, Neumann walls in y, stretched y
+ * grid, pinned kx = kz = 0 mode) and the velocity correction.
+ *
+ * Conventions (identical to the reference's Fortran arrays):
+ *   - arrays are column-major with x fastest: P(i=x, j=z, k=y);
+ *   - P has shape (nx, nz, ny)                        (alloc_poisson_solver_multigpu.f90:40);
+ *   - halo'd velocity fields have shape (nx+2, nz+2, ny+2) and cover
+ *     (-1:nx, -1:nz, -1:ny)                           (inc_set_alloc_arrays.f90:93-101);
+ *   - band arrays and 1-D metrics have ny entries, row k of the wall-normal
+ *     tridiagonal / metric of cell or face k          (inc_set_alloc_arrays.f90:51-61).
+ * Device pointers are raw CUDA device addresses; streams are cudaStream_t
+ * passed as void* (NULL = the legacy default stream).
+ *
+ * Every function returns PRJ_OK (0) or a negative status; none aborts the
+ * process.  prj_last_error_string() describes the last failure of the calling
+ * thread.
+ */
+#ifndef PRJ_PROJECTION_H
+#define PRJ_PROJECTION_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum prj_status {
+    PRJ_OK = 0,
+    PRJ_ERR_ARG = -1,        /* bad size, pointer or flag */
+    PRJ_ERR_UNSUPPORTED = -2,/* valid request the engine does not implement */
+    PRJ_ERR_CUDA = -3,       /* a CUDA runtime call failed */
+    PRJ_ERR_OOM = -4,        /* device allocation failed or budget exceeded */
+    PRJ_ERR_NUMERIC = -5,    /* zero pivot, NaN or refinement that did not converge */
+    PRJ_ERR_TIMEOUT = -6,    /* a bounded device-side wait gave up */
+    PRJ_ERR_STATE = -7       /* call out of order (e.g. destroyed plan) */
+};
+
+/* plan flags */
+#define PRJ_FLAG_NONE 0u
+
+/* precision modes of prj_projection_step */
+#define PRJ_MODE_FP64 0            /* plain FP64 path: the drop-in */
+#define PRJ_MODE_FP32_REFINE 1     /* FP32 spectral work + FP64 iterative refinement */
+
+typedef struct prj_plan prj_plan;
+
+/* Result record of one projection step. */
+typedef struct prj_stats {
+    double div_maxabs;      /* max |div u| after the correction (mod_get_bulk.f90:94-116); -1 if not computed */
+    double p_maxabs;        /* max |P| */
+    double min_pivot;       /* min |pivot| of the Thomas factorisation (min_abs_div_bacp, PSM:181-222) */
+    int refine_iters;       /* refinement iterations used (0 for FP64) */
+    int fp64_lines;         /* spectral lines solved in FP64 by the mixed path */
+    double last_update_rel; /* rel-L2 of the last refinement update (mixed path) */
+} prj_stats;
+
+/* Scalars of one projection step (update_vars / build_vars arguments). */
+typedef struct prj_step_params {
+    double dt;              /* dtmax: P = (1/dt) div(u_hat); u = u_hat - dt grad P */
+    double wall_U_bot, wall_V_bot, wall_W_bot;  /* wall_BC_*_bot */
+    double wall_U_top, wall_V_top, wall_W_top;  /* wall_BC_*_top */
+    int compute_stats;      /* nonzero: fill prj_stats.div_maxabs / p_maxabs */
+} prj_step_params;
+
+/*
+ * Create a solver plan on `device` for an nx x nz x ny grid.
+ * Replaces init_spec_poisson_multigpu (poisson_solver_multigpu.f90:33-326)
+ * for mpi_divs_z = mpi_divs_y = 1: builds the FFT plans (:77-129), the
+ * a_x / a_z / poi_is_00 tables (:133-155) and the Thomas pivot table that
+ * takes the place of poi_C (:164-179), and records min_abs_div_bacp (:181-222).
+ *   band_*     P_band_a/b/c      (ny)  bands of all non-(0,0) modes
+ *   band_*00   P_band_a/b/c_00   (ny)  bands of the pinned (0,0) mode
+ *   inv_dy_p   (ny)   1/(yu(k+1)-yu(k))          (divergence, MCS:534)
+ *   dPdy_lo/hi (ny)   dPdy_ddy_lo/hi rows 0..ny-1 (correction, MCS:1148-1149);
+ *              these three may be NULL for a Poisson-only plan.
+ * Limits: 1 <= nx <= 8192, 1 <= nz <= 4094, 2 <= ny <= 65536; every prime
+ * factor of nz and of nx (nx/2 for even nx) is at most 64.
+ */
+int prj_plan_create(int nx, int nz, int ny, double dx, double dz,
+                    const double* band_a, const double* band_b, const double* band_c,
+                    const double* band_a00, const double* band_b00, const double* band_c00,
+                    const double* inv_dy_p, const double* dPdy_lo, const double* dPdy_hi,
+                    unsigned flags, int device, prj_plan** out);
+
+/* Release every device buffer of the plan.  Replaces
+ * dealloc_poisson_solver_multigpu.f90:1-39.  NULL is accepted. */
+int prj_plan_destroy(prj_plan* plan);
+
+/*
+ * FP64 Poisson solve in place on a device array P (nx, nz, ny): the RHS on
+ * entry, the solution on exit.  Drop-in for run_spec_poisson_multigpu
+ * (poisson_solver_multigpu.f90:328-554) with mpi_divs_y = 1: forward FFTs,
+ * per-line Thomas with the pinned (0,0) mode, inverse FFTs, 1/(nx nz).
+ * Asynchronous on `stream`.
+ */
+int prj_poisson_fp64(prj_plan* plan, double* d_P, void* stream);
+
+/*
+ * One pressure projection on device arrays: P = (1/dt) div(u_hat)
+ * (mod_cfd_subroutines.f90:504-537), Poisson solve, and
+ * u = u_hat - dt grad P with the boundary fill of update_vars
+ * (mod_cfd_subroutines.f90:1086-1152, :1223-1243).  Uh, Vh, Wh (inputs) and
+ * U, V, W (outputs) are halo'd; only interior input values are read (x and z
+ * wrap periodically, V_hat at the walls is wall_V_bot / wall_V_top).  The
+ * outputs are written everywhere, halos included.  P (nx, nz, ny) receives
+ * the pressure.  `mode` is PRJ_MODE_FP64 or PRJ_MODE_FP32_REFINE.  `stats`
+ * may be NULL; when non-NULL (or compute_stats is set) the call synchronises
+ * `stream` to return the record.
+ */
+int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, const double* d_Wh,
+                        double* d_U, double* d_V, double* d_W, double* d_P,
+                        const prj_step_params* params, int mode, prj_stats* stats, void* stream);
+
+/* Host-buffer form of prj_poisson_fp64: copies P to the device, solves, and
+ * copies the solution back (synchronous).  For callers that hold host arrays,
+ * like the reference's FFTW build. */
+int prj_poisson_fp64_host(prj_plan* plan, double* h_P);
+
+/* Host-buffer form of prj_projection_step (synchronous, copies included). */
+int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h_Vh, const double* h_Wh,
+                             double* h_U, double* h_V, double* h_W, double* h_P,
+                             const prj_step_params* params, int mode, prj_stats* stats);
+
+/* band modes of prj_bands_from_yu */
+#define PRJ_BANDS_REFERENCE 0   /* the reference's mk_P_abc bands */
+#define PRJ_BANDS_CONSISTENT 1  /* bands of div(grad p) with the divergence/correction metrics */
+
+/*
+ * Wall-normal bands from the face coordinates yu (ny+1 values, increasing).
+ * PRJ_BANDS_REFERENCE restates mk_P_abc (src/pycode/calc_bands.py:181-201) on
+ * yp_ext = [yu_0, yp_0 .. yp_{ny-1}, yu_ny] (calc_bands.py:226-227); the _00
+ * arrays are its is_dirich_first variant (the pinned (0,0) mode).
+ * PRJ_BANDS_CONSISTENT gives a_k = inv_dy_p(k)/(yp_k - yp_{k-1}),
+ * c_k = inv_dy_p(k)/(yp_{k+1} - yp_k), b_k = -(a_k + c_k), a_0 = c_{ny-1} = 0,
+ * so that the discrete Laplacian equals div(grad p) of the divergence and
+ * correction stencils; its pinned variant subtracts the same mirrored-ghost
+ * term from b_0.  Host-only (no GPU needed).
+ */
+int prj_bands_from_yu(int ny, const double* yu, int mode, double* a, double* b, double* c,
+                      double* a00, double* b00, double* c00);
+
+/* 1-D metrics from yu: inv_dy_p (calc_bands.py:274) and rows 0..ny-1 of
+ * dPdy_ddy_lh (calc_bands.py:336-343).  Host-only. */
+int prj_metrics_from_yu(int ny, const double* yu, double* inv_dy_p, double* dPdy_lo, double* dPdy_hi);
+
+/* min_abs_div_bacp of the plan (poisson_solver_multigpu.f90:181-222). */
+int prj_plan_min_pivot(const prj_plan* plan, double* out);
+
+/* Device bytes the plan holds (for HBM-budget admission). */
+int prj_plan_device_bytes(const prj_plan* plan, size_t* out);
+
+/*
+ * Per-kernel device timing (diagnostics; no counterpart in the reference,
+ * which only prints wall time per iteration, mod_get_bulk.f90:174-175).
+ * While enabled, every call records CUDA events around each kernel on the
+ * caller's stream.  prj_plan_stage_times synchronises those events, writes
+ * the summed milliseconds and launch counts per stage (index = stage id, up
+ * to max_stages entries), sets *n_stages and clears the record.
+ */
+int prj_plan_enable_stage_timing(prj_plan* plan, int enable);
+int prj_plan_stage_times(prj_plan* plan, double* ms, int* launches, int max_stages, int* n_stages);
+/* Kernel name of a stage id ("" if unknown). */
+const char* prj_stage_name(int stage);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* prj_last_error_string(void);
+
+/* Engine version string. */
+const char* prj_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRJ_PROJECTION_H */
