@@ -231,6 +231,11 @@ int ensure_host_stage(prj_plan* pl, size_t elems) {
 
 }  // namespace
 
+int prj::record_error(int code, const char* msg) {
+    g_last_error = msg;
+    return code;
+}
+
 extern "C" {
 
 const char* prj_last_error_string(void) { return g_last_error.c_str(); }

@@ -104,4 +104,7 @@ cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, c
                          double* out2, cudaStream_t st);
 cudaError_t launch_min_abs(const double* x, size_t n, double* out, cudaStream_t st);
 
+// Sets the calling thread's prj_last_error_string() message and returns code.
+int record_error(int code, const char* msg);
+
 }  // namespace prj

@@ -49,6 +49,7 @@ EXPORTS = (
     "prj_plan_device_bytes", "prj_last_error_string", "prj_version",
     "prj_bands_from_yu", "prj_metrics_from_yu",
     "prj_plan_enable_stage_timing", "prj_plan_stage_times", "prj_stage_name",
+    "prj_poisson_fp64_noalloc",
 )
 
 BANDS_REFERENCE = 0
@@ -114,6 +115,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_enable_stage_timing.argtypes = [_vp, i]
     L.prj_plan_stage_times.argtypes = [_vp, _dp, ctypes.POINTER(ctypes.c_int), i, ctypes.POINTER(ctypes.c_int)]
     L.prj_stage_name.argtypes = [i]
+    L.prj_poisson_fp64_noalloc.argtypes = [i, i, i, d, d, _dp, _dp, _dp, _dp, _dp, _dp, _vp, _vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.prj_last_error_string.restype = ctypes.c_char_p

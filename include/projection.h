@@ -167,6 +167,32 @@ int prj_plan_stage_times(prj_plan* plan, double* ms, int* launches, int max_stag
 /* Kernel name of a stage id ("" if unknown). */
 const char* prj_stage_name(int stage);
 
+/*
+ * FP64 Poisson solve for callers that cannot allocate device memory.
+ * No counterpart in the reference (there, Fortran allocates every array up
+ * front, alloc_poisson_solver_multigpu.f90:39-64); it serves host programs
+ * whose device memory is owned elsewhere (an OpenACC/Fortran runtime, a time
+ * loop under a memory cap, code that must not call cudaMalloc, which may
+ * synchronise the device).  Same arguments and result as prj_plan_create
+ * followed by prj_poisson_fp64 (bands are host arrays of ny values, d_P is the
+ * device array (nx, nz, ny), solved in place), but it allocates nothing: all
+ * scratch (tables, pivots, spectrum) lives in one static device array of
+ * PRJ_NOALLOC_SCRATCH_BYTES that every GPU using the library holds until the
+ * process exits.  Grids whose scratch exceeds that size are rejected with
+ * PRJ_ERR_ARG (roughly 10 bytes per grid point: about 6.5e6 points at most;
+ * 256 x 128 x 128 fits).
+ * The first call on a device resolves the array's address on that device
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Calls share the array: the function is synchronous on `stream` and
+ * serialises its callers with a process lock; work that overlapped on the
+ * GPU with another user of the array would race.
+ */
+#define PRJ_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int prj_poisson_fp64_noalloc(int nx, int nz, int ny, double dx, double dz,
+                             const double* band_a, const double* band_b, const double* band_c,
+                             const double* band_a00, const double* band_b00, const double* band_c00,
+                             double* d_P, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* prj_last_error_string(void);
 
