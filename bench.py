@@ -207,17 +207,20 @@ def cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz):
 
 
 def main():
+    global NX, NY, NZ
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3, help="0 skips the end-to-end leg")
+    ap.add_argument("--grid", default=f"{NX}x{NY}x{NZ}", help="nx x ny x nz (profiling of smaller cases)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    NX, NY, NZ = (int(v) for v in args.grid.lower().split("x"))
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -287,27 +290,29 @@ def main():
     Uh_h = np.asfortranarray(Uh.cpu().numpy().T)
     Vh_h = np.asfortranarray(Vh.cpu().numpy().T)
     Wh_h = np.asfortranarray(Wh.cpu().numpy().T)
-    pin = lambda shape: torch.empty(tuple(reversed(shape)), dtype=torch.float64).pin_memory().numpy().T
-    hshape = (NX + 2, NZ + 2, NY + 2)
-    pUh, pVh, pWh, pU, pV, pW = (pin(hshape) for _ in range(6))
-    pP = pin((NX, NZ, NY))
-    pUh[...] = Uh_h
-    pVh[...] = Vh_h
-    pWh[...] = Wh_h
-    plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)  # warm (staging alloc)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)
-    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-    if dist is not None:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_s = float(te.item())
-    nh = (NX + 2) * (NZ + 2) * (NY + 2)
-    e2e = {"value": world * NX * NY * NZ / e2e_s / 1e9, "unit": "Gpts/s", "h2d_bytes_per_step": 3 * 8 * nh,
-           "d2h_bytes_per_step": 3 * 8 * nh + 8 * NX * NY * NZ, "ms_per_step": 1e3 * e2e_s,
-           "call": "prj_projection_step_host (pinned host buffers)"}
+    e2e = None
+    if args.e2e_steps > 0:
+        pin = lambda shape: torch.empty(tuple(reversed(shape)), dtype=torch.float64).pin_memory().numpy().T
+        hshape = (NX + 2, NZ + 2, NY + 2)
+        pUh, pVh, pWh, pU, pV, pW = (pin(hshape) for _ in range(6))
+        pP = pin((NX, NZ, NY))
+        pUh[...] = Uh_h
+        pVh[...] = Vh_h
+        pWh[...] = Wh_h
+        plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)  # warm (staging alloc)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        te = torch.tensor([e2e_s], dtype=torch.float64, device=device)
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_s = float(te.item())
+        nh = (NX + 2) * (NZ + 2) * (NY + 2)
+        e2e = {"value": world * NX * NY * NZ / e2e_s / 1e9, "unit": "Gpts/s", "h2d_bytes_per_step": 3 * 8 * nh,
+               "d2h_bytes_per_step": 3 * 8 * nh + 8 * NX * NY * NZ, "ms_per_step": 1e3 * e2e_s,
+               "call": "prj_projection_step_host (pinned host buffers)"}
 
     # roofline of the dominant kernel
     peak, peak_kind = peaks()
@@ -329,7 +334,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "pressure projection step 768x384x384 (channel Lx=2pi Lz=pi, tanh beta=2, "
+            "config": {"workload": f"pressure projection step {NX}x{NY}x{NZ} (channel Lx=2pi Lz=pi, tanh beta=2, "
                                    "Poiseuille + N(0,0.1) predictor)", "nx": NX, "ny": NY, "nz": NZ,
                        "mode": args.mode, "bands": "consistent", "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (3 x 0.92 GB fields), no flush"},
