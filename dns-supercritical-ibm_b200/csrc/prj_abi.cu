@@ -409,6 +409,8 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if ((e = cudaMalloc((void**)&pl->stat_buf, 8 * sizeof(double))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(stats)"));
     bytes += 8 * sizeof(double);
+    if ((e = cudaMemset(pl->stat_buf, 0, 8 * sizeof(double))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMemset(stats)"));
     if ((e = prj::launch_build_pivots(pl, 0)) != cudaSuccess) return bail(cuda_fail(e, "pivot table"));
     double mp = 0;
     if ((e = cudaMemcpy(&mp, pl->stat_buf, sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess)
@@ -535,9 +537,12 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
             StageTimer tm(plan, prj::kStStats, st);
             CK(prj::launch_stats(plan, d_U, d_V, d_W, d_P, plan->stat_buf + 2, st), "stats");
         }
-        double h[2] = {-1, -1};
-        CK(cudaMemcpyAsync(h, plan->stat_buf + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "stats copy");
+        double h[5] = {-1, -1, 0, 0, 0};
+        CK(cudaMemcpyAsync(h, plan->stat_buf + 2, 5 * sizeof(double), cudaMemcpyDeviceToHost, st), "stats copy");
         CK(cudaStreamSynchronize(st), "stats sync");
+        int dev_err = 0;
+        std::memcpy(&dev_err, &h[prj::kStatErrSlot - 2], sizeof(int));
+        if (dev_err) return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
         if (stats) {
             stats->div_maxabs = h[0];
             stats->p_maxabs = h[1];

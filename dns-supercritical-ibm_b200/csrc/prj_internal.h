@@ -102,7 +102,13 @@ cudaError_t launch_correction(const prj_plan* pl, const double* P, const double*
 cudaError_t launch_build_pivots(const prj_plan* pl, cudaStream_t st);
 cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, const double* W, const double* P,
                          double* out2, cudaStream_t st);
-cudaError_t launch_min_abs(const double* x, size_t n, double* out, cudaStream_t st);
+// z transform + Thomas with bulk-copy prefetch (prj_zsolve.cu); cudaErrorNotSupported
+// when the grid does not fit its shared-memory budget.  *err_word is raised if a
+// bounded wait gives up.
+cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStream_t st);
+
+// stat_buf slots: [0] min pivot (bits), [2] max|div u|, [3] max|P|, [6] device error word
+constexpr int kStatErrSlot = 6;
 
 // Sets the calling thread's prj_last_error_string() message and returns code.
 int record_error(int code, const char* msg);

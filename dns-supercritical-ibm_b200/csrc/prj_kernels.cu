@@ -443,6 +443,10 @@ cudaError_t launch_bwd_x(const prj_plan* pl, double* P, cudaStream_t st) {
 }
 
 cudaError_t launch_zsolve(const prj_plan* pl, cudaStream_t st) {
+    {
+        cudaError_t ep = launch_zsolve_pipelined(pl, reinterpret_cast<int*>(pl->stat_buf + kStatErrSlot), st);
+        if (ep != cudaErrorNotSupported) return ep;
+    }
     const Geometry& g = pl->g;
     ZArgs a{};
     a.nz = g.nz; a.ny = g.ny; a.nh = g.nxh; a.nzh = g.nzh; a.mzp = g.mzp;

@@ -100,7 +100,7 @@ def test_mms_convergence_matches_reference(cuda_device, mms):
 
 @pytest.mark.parametrize("shape", [(1, 1, 2), (2, 1, 3), (1, 7, 4), (3, 3, 6), (5, 10, 10), (17, 13, 9),
                                    (37, 11, 5), (29, 31, 7), (64, 96, 33), (96, 128, 40), (250, 6, 3),
-                                   (162, 125, 12)])
+                                   (162, 125, 12), (6, 2000, 5), (2, 4000, 3)])
 def test_odd_and_prime_sizes(cuda_device, oracle, shape):
     import prj
     nx, nz, ny = shape
