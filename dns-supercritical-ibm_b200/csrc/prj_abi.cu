@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/projection.h"
+#include "fft_host.h"
 #include "prj_internal.h"
 
 namespace {
@@ -123,6 +124,24 @@ void dfree(P*& p) {
     p = nullptr;
 }
 
+// in-place DIF tables of a length-n transform (left unset when a radix is unsupported)
+int make_dif(int n, prj::DifFft* d, size_t* bytes) {
+    d->ok = false;
+    if (!prj::dif_supported(n)) return PRJ_OK;
+    const long ntw = prj::dif_plan(n, &d->f);
+    if (ntw < 0) return PRJ_OK;
+    std::vector<double2> tw((size_t)ntw);
+    std::vector<int> pos((size_t)n);
+    prj::dif_fill(d->f, tw.data(), pos.data());
+    CK(cudaMalloc((void**)&d->tw, tw.size() * sizeof(double2)), "cudaMalloc(DIF twiddles)");
+    CK(cudaMemcpy(d->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice), "cudaMemcpy(DIF twiddles)");
+    CK(cudaMalloc((void**)&d->pos, pos.size() * sizeof(int)), "cudaMalloc(DIF positions)");
+    CK(cudaMemcpy(d->pos, pos.data(), pos.size() * sizeof(int), cudaMemcpyHostToDevice), "cudaMemcpy(DIF positions)");
+    *bytes += tw.size() * sizeof(double2) + pos.size() * sizeof(int);
+    d->ok = true;
+    return PRJ_OK;
+}
+
 void free_plan_buffers(prj_plan* pl) {
     dfree(pl->t.bands);
     dfree(pl->t.inv_dy_p);
@@ -134,6 +153,11 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->fx64.tw);
     dfree(pl->fx64.post);
     dfree(pl->fz64.tw);
+    dfree(pl->xd.tw);
+    dfree(pl->xd.pos);
+    dfree(pl->zd.tw);
+    dfree(pl->zd.pos);
+    pl->xd.ok = pl->zd.ok = false;
     dfree(pl->spec);
     dfree(pl->stat_buf);
     dfree(pl->host_stage);
@@ -355,6 +379,9 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     };
     if ((rc = make_rfft<double>(nx, &pl->fx64, &bytes))) return bail(rc);
     if ((rc = make_cfft<double>(nz, &pl->fz64.f, &pl->fz64.tw, &bytes))) return bail(rc);
+    if ((rc = make_dif(pl->fx64.m, &pl->xd, &bytes))) return bail(rc);
+    if ((rc = make_dif(nz, &pl->zd, &bytes))) return bail(rc);
+    pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);
 
     // rows per CTA of the x kernels: fit two ping-pong buffers in ~100 KB
     {

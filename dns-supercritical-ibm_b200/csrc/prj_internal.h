@@ -8,8 +8,19 @@
 #include <vector>
 
 #include "fft_device.cuh"
+#include "fft_dif.cuh"
 
 namespace prj {
+
+// In-place DIF transform of one length (fft_dif.cuh): descriptor and device tables.
+// `ok` is false when a radix has no hard-coded butterfly; the out-of-place
+// Stockham kernels serve those lengths.
+struct DifFft {
+    bool ok = false;
+    DifDev f{};
+    double2* tw = nullptr;  // stage twiddles (forward sign)
+    int* pos = nullptr;     // pos[k]: slot of index k after the transform
+};
 
 // One real-to-complex transform of length n along a contiguous axis, done as a
 // complex FFT of length m (m = n/2 for even n, packed even/odd samples; m = n
@@ -79,7 +90,10 @@ struct prj_plan {
     double* stat_buf = nullptr;   // device reduction slots
     double min_pivot = 0.0;
     size_t device_bytes = 0;
-    int tz_fwd = 1;               // rows per CTA of the x-transform kernels
+    int tz_fwd = 1;               // rows per CTA of the out-of-place x-transform kernels
+    prj::DifFft xd;               // in-place transform of length fx64.m (x rows)
+    prj::DifFft zd;               // in-place transform of length nz (z rows)
+    int tz_xd = 1;                // rows per CTA of the in-place x-transform kernels
 };
 
 namespace prj {
@@ -106,6 +120,12 @@ cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, c
 // when the grid does not fit its shared-memory budget.  *err_word is raised if a
 // bounded wait gives up.
 cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStream_t st);
+
+// x transforms with the in-place DIF FFT (prj_xfft.cu); used when pl->xd.ok
+cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
+                          const double* Wh, const StepScalars* sc, cudaStream_t st);
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st);
+int choose_tz_xd(int m, bool even);
 
 // stat_buf slots: [0] min pivot (bits), [2] max|div u|, [3] max|P|, [6] device error word
 constexpr int kStatErrSlot = 6;

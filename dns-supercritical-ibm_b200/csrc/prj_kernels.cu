@@ -404,6 +404,7 @@ int sm_count() {
 
 cudaError_t launch_fwd_x(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
                          const double* Wh, const StepScalars* sc, cudaStream_t st) {
+    if (pl->xd.ok) return launch_fwd_xd(pl, src, P, Uh, Vh, Wh, sc, st);
     const Geometry& g = pl->g;
     FwdArgs a{};
     a.nx = g.nx; a.nz = g.nz; a.ny = g.ny; a.nh = g.nxh;
@@ -427,6 +428,7 @@ cudaError_t launch_fwd_x(const prj_plan* pl, FwdSource src, const double* P, con
 }
 
 cudaError_t launch_bwd_x(const prj_plan* pl, double* P, cudaStream_t st) {
+    if (pl->xd.ok) return launch_bwd_xd(pl, P, st);
     const Geometry& g = pl->g;
     BwdArgs a{};
     a.nx = g.nx; a.nz = g.nz; a.ny = g.ny; a.nh = g.nxh;

@@ -1,0 +1,234 @@
+// prj_xfft.cu -- x-direction real transforms with in-place DIF FFTs.
+//
+// k_fwd_xd: divergence of the predictor (or P itself) -> real FFT along x of
+//           `tz` x-rows at one y -> transposed store X[y][kx][z0 .. z0+tz).
+// k_bwd_xd: transposed load of X -> inverse real FFT along x, 1/(nx nz) ->
+//           P rows.
+// The real transform of even length n is a complex transform of length m = n/2
+// on the packed samples x_2j + i x_2j+1 plus a split pass; odd n uses a
+// complex transform of length n.  The in-place DIF transform (fft_dif.cuh)
+// needs one row buffer per x-row, half of an out-of-place transform, so more
+// CTAs fit on an SM.  Loads and stores of P and u_hat are one element per
+// thread along x (fully coalesced).
+#include "fft_dif.cuh"
+#include "prj_internal.h"
+
+namespace prj {
+
+namespace {
+
+__device__ __forceinline__ size_t hidx_d(int nx, int nz, int i, int j, int k) {
+    return (size_t)(i + 1) + (size_t)(nx + 2) * ((size_t)(j + 1) + (size_t)(nz + 2) * (size_t)(k + 1));
+}
+
+struct XArgs {
+    int nx, nz, ny, nh, m, tz, rs, even;
+    DifDev f;
+    const double2* tw;
+    const int* pos;
+    const double2* post;
+    const double* P;
+    const double* Uh;
+    const double* Vh;
+    const double* Wh;
+    const double* inv_dy_p;
+    double inv_dx, inv_dz, inv_dt, vbot, vtop, scale;
+    double2* X;
+    double* Pout;
+};
+
+// divergence at cell (i, j, k), mod_cfd_subroutines.f90:532-534 (periodic wrap in x and z,
+// V_hat walls from the step parameters); reference operation order, no contraction
+__device__ __forceinline__ double div_at(const XArgs& a, int i, int j, int k) {
+    const int nx = a.nx, nz = a.nz;
+    const int ip = (i + 1 == nx) ? 0 : i + 1;
+    const int jp = (j + 1 == nz) ? 0 : j + 1;
+    const double u1 = a.Uh[hidx_d(nx, nz, ip, j, k)], u0 = a.Uh[hidx_d(nx, nz, i, j, k)];
+    const double w1 = a.Wh[hidx_d(nx, nz, i, jp, k)], w0 = a.Wh[hidx_d(nx, nz, i, j, k)];
+    const double v1 = (k + 1 == a.ny) ? a.vtop : a.Vh[hidx_d(nx, nz, i, j, k + 1)];
+    const double v0 = (k == 0) ? a.vbot : a.Vh[hidx_d(nx, nz, i, j, k)];
+    double s = __dmul_rn(__dsub_rn(u1, u0), a.inv_dx);
+    s = __dadd_rn(s, __dmul_rn(__dsub_rn(w1, w0), a.inv_dz));
+    s = __dadd_rn(s, __dmul_rn(__dsub_rn(v1, v0), a.inv_dy_p[k]));
+    return __dmul_rn(a.inv_dt, s);
+}
+
+template <int SRC>
+__global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* A = reinterpret_cast<double2*>(sm);
+    int* pos = reinterpret_cast<int*>(sm + (size_t)a.tz * a.rs * sizeof(double2));
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int m = a.m, nx = a.nx;
+    for (int i = tid; i < m; i += nthr) pos[i] = a.pos[i];
+    for (int idx = tid; idx < a.tz * nx; idx += nthr) {
+        const int r = idx / nx, i = idx - r * nx;
+        const int z = z0 + r;
+        double v = 0.0;
+        if (z < a.nz) v = (SRC == 0) ? a.P[((size_t)y * a.nz + z) * nx + i] : div_at(a, i, z, y);
+        if (a.even) reinterpret_cast<double*>(A + (size_t)r * a.rs)[i] = v;
+        else A[(size_t)r * a.rs + i] = make_double2(v, 0.0);
+    }
+    __syncthreads();
+    dif_rows<-1>(A, a.tz, a.rs, a.f, a.tw);
+    if (a.even) {
+        // split: X_k = E_k + W^k O_k and X_{m-k} = conj(E_k) + W^{m-k} conj(O_k), in place
+        const int half = m / 2;
+        for (int idx = tid; idx < a.tz * (half + 1); idx += nthr) {
+            const int r = idx / (half + 1), k = idx - r * (half + 1);
+            double2* Z = A + (size_t)r * a.rs;
+            if (k == 0) {
+                const double2 z = Z[pos[0]];
+                Z[pos[0]] = make_double2(z.x + z.y, 0.0);
+                Z[m] = make_double2(z.x - z.y, 0.0);
+            } else {
+                const int kk = m - k;
+                const double2 zk = Z[pos[k]];
+                const double2 zm = cconj(Z[pos[kk]]);
+                const double2 e = cscale(cadd(zk, zm), 0.5);
+                const double2 d = csub(zk, zm);
+                const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
+                Z[pos[k]] = cadd(e, cmul(a.post[k], o));
+                if (kk != k) Z[pos[kk]] = cadd(cconj(e), cmul(a.post[kk], cconj(o)));
+            }
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < a.nh * a.tz; idx += nthr) {
+        const int kx = idx / a.tz, r = idx - kx * a.tz;
+        const int z = z0 + r;
+        if (z >= a.nz) continue;
+        const int slot = (a.even && kx == m) ? m : pos[kx];
+        a.X[((size_t)y * a.nh + kx) * a.nz + z] = A[(size_t)r * a.rs + slot];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* A = reinterpret_cast<double2*>(sm);
+    int* pos = reinterpret_cast<int*>(sm + (size_t)a.tz * a.rs * sizeof(double2));
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int m = a.m, nx = a.nx;
+    for (int i = tid; i < m; i += nthr) pos[i] = a.pos[i];
+    for (int idx = tid; idx < a.nh * a.tz; idx += nthr) {
+        const int kx = idx / a.tz, r = idx - kx * a.tz;
+        const int z = z0 + r;
+        A[(size_t)r * a.rs + kx] = (z < a.nz) ? a.X[((size_t)y * a.nh + kx) * a.nz + z] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const double s = a.scale;
+    if (a.even) {
+        // inverse split, in place on pairs (k, m-k); imaginary parts of X_0 and X_m ignored
+        const int half = m / 2;
+        for (int idx = tid; idx < a.tz * (half + 1); idx += nthr) {
+            const int r = idx / (half + 1), k = idx - r * (half + 1);
+            double2* Z = A + (size_t)r * a.rs;
+            if (k == 0) {
+                const double x0 = Z[0].x, xm = Z[m].x;
+                Z[0] = make_double2((x0 + xm) * s, (x0 - xm) * s);
+            } else {
+                const int kk = m - k;
+                const double2 xk = Z[k], xkk = Z[kk];
+                const double2 e1 = cadd(xk, cconj(xkk));
+                const double2 o1 = cmulc(csub(xk, cconj(xkk)), a.post[k]);
+                Z[k] = cscale(make_double2(e1.x - o1.y, e1.y + o1.x), s);
+                if (kk != k) {
+                    const double2 e2 = cadd(xkk, cconj(xk));
+                    const double2 o2 = cmulc(csub(xkk, cconj(xk)), a.post[kk]);
+                    Z[kk] = cscale(make_double2(e2.x - o2.y, e2.y + o2.x), s);
+                }
+            }
+        }
+    } else {
+        // Hermitian completion of the odd-length row, scaled
+        for (int idx = tid; idx < a.tz * a.nh; idx += nthr) {
+            const int r = idx / a.nh, k = idx - r * a.nh;
+            double2* Z = A + (size_t)r * a.rs;
+            double2 v = Z[k];
+            if (k == 0) v.y = 0.0;
+            v = cscale(v, s);
+            Z[k] = v;
+            if (k > 0) Z[m - k] = cconj(v);
+        }
+    }
+    __syncthreads();
+    dif_rows<+1>(A, a.tz, a.rs, a.f, a.tw);
+    for (int idx = tid; idx < a.tz * nx; idx += nthr) {
+        const int r = idx / nx, i = idx - r * nx;
+        const int z = z0 + r;
+        if (z >= a.nz) continue;
+        double v;
+        if (a.even) {
+            const double2 c = A[(size_t)r * a.rs + pos[i >> 1]];
+            v = (i & 1) ? c.y : c.x;
+        } else {
+            v = A[(size_t)r * a.rs + pos[i]].x;
+        }
+        a.Pout[((size_t)y * a.nz + z) * nx + i] = v;
+    }
+}
+
+XArgs make_args(const prj_plan* pl) {
+    const Geometry& g = pl->g;
+    XArgs a{};
+    a.nx = g.nx; a.nz = g.nz; a.ny = g.ny; a.nh = g.nxh;
+    a.m = pl->fx64.m; a.even = pl->fx64.even;
+    a.tz = pl->tz_xd;
+    a.rs = a.even ? a.m + 1 : a.m;
+    a.f = pl->xd.f; a.tw = pl->xd.tw; a.pos = pl->xd.pos; a.post = pl->fx64.post;
+    a.inv_dx = 1.0 / g.dx; a.inv_dz = 1.0 / g.dz;
+    a.X = pl->spec;
+    return a;
+}
+
+size_t smem_bytes(const XArgs& a) { return (size_t)a.tz * a.rs * sizeof(double2) + (size_t)a.m * sizeof(int); }
+
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+// rows per CTA of the in-place x kernels: a power of two up to 16 within ~56 KB
+int choose_tz_xd(int m, bool even) {
+    const size_t row = (size_t)(even ? m + 1 : m) * sizeof(double2);
+    int tz = 16;
+    while (tz > 1 && (size_t)tz * row + (size_t)m * sizeof(int) > 56 * 1024) tz /= 2;
+    return tz;
+}
+
+cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
+                          const double* Wh, const StepScalars* sc, cudaStream_t st) {
+    XArgs a = make_args(pl);
+    a.P = P; a.Uh = Uh; a.Vh = Vh; a.Wh = Wh; a.inv_dy_p = pl->t.inv_dy_p;
+    if (sc) { a.inv_dt = sc->inv_dt; a.vbot = sc->wall[1]; a.vtop = sc->wall[4]; }
+    const size_t smem = smem_bytes(a);
+    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
+    cudaError_t e;
+    if (src == FwdSource::Pressure) {
+        if ((e = allow_smem(k_fwd_xd<0>, smem)) != cudaSuccess) return e;
+        k_fwd_xd<0><<<grid, 256, smem, st>>>(a);
+    } else {
+        if ((e = allow_smem(k_fwd_xd<1>, smem)) != cudaSuccess) return e;
+        k_fwd_xd<1><<<grid, 256, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st) {
+    XArgs a = make_args(pl);
+    a.Pout = P;
+    a.scale = 1.0 / ((double)pl->g.nx * (double)pl->g.nz + 0.0);
+    const size_t smem = smem_bytes(a);
+    cudaError_t e = allow_smem(k_bwd_xd, smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
+    k_bwd_xd<<<grid, 256, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace prj

@@ -16,6 +16,8 @@
 // (poisson_solver_multigpu.f90:401-419) through round-to-nearest intrinsics.
 // Every mbarrier wait is bounded; on a timeout the CTA raises *err, waits
 // (bounded) for its copies in flight and returns.
+#include <cstdlib>
+
 #include "prj_internal.h"
 #include "tma_util.cuh"
 
@@ -32,17 +34,25 @@ struct ZPipeArgs {
     const double* piv;    // D[y][kx][kzs]
     double2* X;
     int* err;
+    DifDev fd;            // in-place transform (DIF variant)
+    const double2* dtw;
+    const int* dpos;
 };
 
-template <int PPT>
+// DIF = true: in-place transforms (no work buffer), spectrum read through the
+// position table; DIF = false: out-of-place Stockham transforms with a work buffer.
+template <int PPT, bool DIF>
 __global__ void __launch_bounds__(512) k_zsolve_pipe(const ZPipeArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int nz = a.nz, ny = a.ny, yb = a.yb, ns = a.ns, mzp = a.mzp, nh = a.nh;
     const uint32_t xrow = (uint32_t)nz * sizeof(double2);
     const uint32_t prow = (uint32_t)mzp * sizeof(double);
     const size_t stage_bytes = (size_t)yb * (xrow + prow);
+    // after the stages: DIF -> position table (nz ints, padded to 16 B); Stockham -> work rows
+    const size_t extra = DIF ? ((size_t)nz * sizeof(int) + 15) / 16 * 16 : (size_t)yb * xrow;
     double2* work = reinterpret_cast<double2*>(smraw + ns * stage_bytes);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + ns * stage_bytes + (size_t)yb * xrow);
+    int* pos = reinterpret_cast<int*>(smraw + ns * stage_bytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + ns * stage_bytes + extra);
 
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int kx = blockIdx.x;
@@ -52,6 +62,8 @@ __global__ void __launch_bounds__(512) k_zsolve_pipe(const ZPipeArgs a) {
     const double* ba0 = a.bands + 3 * ny;
     const double* bc0 = a.bands + 5 * ny;
 
+    if (DIF)
+        for (int i = tid; i < nz; i += nthr) pos[i] = a.dpos[i];
     if (tid == 0) {
         for (int s = 0; s < ns; s++) mbar_init(&bars[s], 1);
         mbar_fence_init();
@@ -108,7 +120,13 @@ __global__ void __launch_bounds__(512) k_zsolve_pipe(const ZPipeArgs a) {
         if (!acquire(s)) { bail(); return; }
         const int y0 = c * yb;
         const int nr = min(yb, ny - y0);
-        const double2* F = fft_rows<-1>(stage_x(s), work, nr, nz, a.f, a.tw);
+        const double2* F;
+        if (DIF) {
+            dif_rows<-1>(stage_x(s), nr, nz, a.fd, a.dtw);
+            F = stage_x(s);
+        } else {
+            F = fft_rows<-1>(stage_x(s), work, nr, nz, a.f, a.tw);
+        }
         const double* Ds = stage_d(s);
         for (int r = 0; r < nr; r++) {
             const int y = y0 + r;
@@ -120,8 +138,8 @@ __global__ void __launch_bounds__(512) k_zsolve_pipe(const ZPipeArgs a) {
                 if (t < a.nzh) {
                     const bool two = (t > 0) && (2 * t != nz);
                     const double D = Ds[(size_t)r * mzp + t];
-                    double2 v0 = F[(size_t)r * nz + t];
-                    double2 v1 = two ? F[(size_t)r * nz + nz - t] : make_double2(0, 0);
+                    double2 v0 = F[(size_t)r * nz + (DIF ? pos[t] : t)];
+                    double2 v1 = two ? F[(size_t)r * nz + (DIF ? pos[nz - t] : nz - t)] : make_double2(0, 0);
                     if (y == 0) {
                         v0.x = __ddiv_rn(v0.x, D); v0.y = __ddiv_rn(v0.y, D);
                         v1.x = __ddiv_rn(v1.x, D); v1.y = __ddiv_rn(v1.y, D);
@@ -189,43 +207,74 @@ __global__ void __launch_bounds__(512) k_zsolve_pipe(const ZPipeArgs a) {
             }
         }
         __syncthreads();
-        const double2* G = fft_rows<+1>(Xs, work, nr, nz, a.f, a.tw);
-        for (int i = tid; i < nr * nz; i += nthr) {
-            const int r = i / nz, z = i - r * nz;
-            a.X[((size_t)(y0 + r) * nh + kx) * nz + z] = G[i];
+        if (DIF) {
+            dif_rows<+1>(Xs, nr, nz, a.fd, a.dtw);
+            for (int i = tid; i < nr * nz; i += nthr) {
+                const int r = i / nz, z = i - r * nz;
+                a.X[((size_t)(y0 + r) * nh + kx) * nz + z] = Xs[(size_t)r * nz + pos[z]];
+            }
+        } else {
+            const double2* G = fft_rows<+1>(Xs, work, nr, nz, a.f, a.tw);
+            for (int i = tid; i < nr * nz; i += nthr) {
+                const int r = i / nz, z = i - r * nz;
+                a.X[((size_t)(y0 + r) * nh + kx) * nz + z] = G[i];
+            }
         }
         __syncthreads();
     }
 }
 
-template <int PPT>
+template <int PPT, bool DIF>
 cudaError_t launch_pipe(const ZPipeArgs& a, int nthr, size_t smem, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_zsolve_pipe<PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_zsolve_pipe<PPT, DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_zsolve_pipe<PPT><<<a.nh, nthr, smem, st>>>(a);
+    k_zsolve_pipe<PPT, DIF><<<a.nh, nthr, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <bool DIF>
+cudaError_t launch_ppt(const ZPipeArgs& a, int ppt, int nthr, size_t smem, cudaStream_t st) {
+    switch (ppt) {
+    case 1: return launch_pipe<1, DIF>(a, nthr, smem, st);
+    case 2: return launch_pipe<2, DIF>(a, nthr, smem, st);
+    default: return launch_pipe<4, DIF>(a, nthr, smem, st);
+    }
 }
 
 }  // namespace
 
-// Chooses the chunk size and ring depth for ~72 KB of shared memory (three
-// CTAs per SM); returns cudaErrorNotSupported when even one plane per chunk
-// with two stages does not fit, so the caller can use the unpipelined kernel.
+int env_int(const char* name, int dflt) {
+    const char* v = getenv(name);
+    return (v && *v) ? atoi(v) : dflt;
+}
+
+// Chooses the chunk size and ring depth for about 72 KB of shared memory (three
+// CTAs per SM; PRJ_ZSOLVE_YB / PRJ_ZSOLVE_NS override them for tuning) and
+// returns cudaErrorNotSupported when even one plane per chunk with two stages
+// does not fit, so the caller can use the unpipelined kernel.
 cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStream_t st) {
     const Geometry& g = pl->g;
     ZPipeArgs a{};
     a.nz = g.nz; a.ny = g.ny; a.nh = g.nxh; a.nzh = g.nzh; a.mzp = g.mzp;
     a.f = pl->fz64.f; a.tw = pl->fz64.tw; a.bands = pl->t.bands; a.piv = pl->t.piv; a.X = pl->spec;
     a.err = err_word;
+    const bool dif = pl->zd.ok;
+    if (dif) { a.fd = pl->zd.f; a.dtw = pl->zd.tw; a.dpos = pl->zd.pos; }
     const size_t xrow = (size_t)g.nz * sizeof(double2), prow = (size_t)g.mzp * sizeof(double);
-    auto bytes = [&](int yb, int ns) { return (size_t)ns * yb * (xrow + prow) + (size_t)yb * xrow + 8 * (size_t)ns; };
-    int yb = 0, ns = 3;
-    for (int cand = 8; cand >= 1; cand /= 2)
-        if (bytes(cand, 3) <= 72 * 1024) { yb = cand; break; }
-    if (!yb) {
-        ns = 2;
-        for (int cand = 2; cand >= 1; cand /= 2)
-            if (bytes(cand, 2) <= 200 * 1024) { yb = cand; break; }
+    auto bytes = [&](int yb, int ns) {
+        const size_t extra = dif ? ((size_t)g.nz * sizeof(int) + 15) / 16 * 16 : (size_t)yb * xrow;
+        return (size_t)ns * yb * (xrow + prow) + extra + 8 * (size_t)ns;
+    };
+    int yb = env_int("PRJ_ZSOLVE_YB", 0), ns = env_int("PRJ_ZSOLVE_NS", 0);
+    if (yb < 1 || ns < 2 || ns > 8 || bytes(yb, ns) > 200 * 1024) {
+        yb = 0;
+        const int pref_ns = dif ? 2 : 3;
+        for (int cand = 8; cand >= 1; cand /= 2)
+            if (bytes(cand, pref_ns) <= 72 * 1024) { yb = cand; ns = pref_ns; break; }
+        if (!yb)
+            for (int cand = 2; cand >= 1; cand /= 2)
+                if (bytes(cand, 2) <= 200 * 1024) { yb = cand; ns = 2; break; }
     }
     if (!yb) return cudaErrorNotSupported;
     a.yb = yb; a.ns = ns;
@@ -234,13 +283,9 @@ cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStrea
     if (ppt > 4) return cudaErrorNotSupported;
     int nthr = (g.nzh + ppt - 1) / ppt;
     nthr = (nthr + 31) / 32 * 32;
-    if (nthr < 64) nthr = 64;
+    if (nthr < 128) nthr = 128;
     const size_t smem = bytes(yb, ns);
-    switch (ppt) {
-    case 1: return launch_pipe<1>(a, nthr, smem, st);
-    case 2: return launch_pipe<2>(a, nthr, smem, st);
-    default: return launch_pipe<4>(a, nthr, smem, st);
-    }
+    return dif ? launch_ppt<true>(a, ppt, nthr, smem, st) : launch_ppt<false>(a, ppt, nthr, smem, st);
 }
 
 }  // namespace prj
