@@ -130,4 +130,79 @@ __device__ void dif_rows(V* buf, int nrows, int rs, const DifDev& f, const V* __
     }
 }
 
+// One DIT butterfly: the transpose of dif_bfly (twiddles first, then the DFT).
+template <int DIR, typename V>
+__device__ __forceinline__ void dit_bfly(V* __restrict__ p, int mm, int R, int j, const V* __restrict__ w) {
+    switch (R) {
+    case 2: {
+        V a0 = p[0], a1 = p[mm];
+        if (j) a1 = twiddle<DIR>(a1, w[0]);
+        dft2<DIR>(a0, a1);
+        p[0] = a0; p[mm] = a1;
+    } break;
+    case 3: {
+        V a0 = p[0], a1 = p[mm], a2 = p[2 * mm];
+        if (j) { a1 = twiddle<DIR>(a1, w[0]); a2 = twiddle<DIR>(a2, w[1]); }
+        dft3<DIR>(a0, a1, a2);
+        p[0] = a0; p[mm] = a1; p[2 * mm] = a2;
+    } break;
+    case 4: {
+        V a0 = p[0], a1 = p[mm], a2 = p[2 * mm], a3 = p[3 * mm];
+        if (j) { a1 = twiddle<DIR>(a1, w[0]); a2 = twiddle<DIR>(a2, w[1]); a3 = twiddle<DIR>(a3, w[2]); }
+        dft4<DIR>(a0, a1, a2, a3);
+        p[0] = a0; p[mm] = a1; p[2 * mm] = a2; p[3 * mm] = a3;
+    } break;
+    case 5: {
+        V a[5];
+#pragma unroll
+        for (int r = 0; r < 5; r++) a[r] = p[r * mm];
+        if (j) {
+#pragma unroll
+            for (int q = 1; q < 5; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
+        }
+        dft5<DIR>(a[0], a[1], a[2], a[3], a[4]);
+#pragma unroll
+        for (int r = 0; r < 5; r++) p[r * mm] = a[r];
+    } break;
+    case 8: {
+        V a[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) a[r] = p[r * mm];
+        if (j) {
+#pragma unroll
+            for (int q = 1; q < 8; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
+        }
+        dft8<DIR>(a);
+#pragma unroll
+        for (int r = 0; r < 8; r++) p[r * mm] = a[r];
+    } break;
+    default:
+        break;
+    }
+}
+
+// In-place decimation-in-time transform with the same plan as dif_rows: input in
+// digit-reversed order (index k at slot pos[k]), output in natural order.  With
+// DIR = +1 it inverts dif_rows<-1> up to the factor n (unnormalised inverse).
+template <int DIR, typename V>
+__device__ void dit_rows(V* buf, int nrows, int rs, const DifDev& f, const V* __restrict__ tw) {
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int n = f.n;
+    for (int s = f.nst - 1; s >= 0; s--) {
+        const int R = f.radix[s], L = f.span[s];
+        const int mm = L / R;
+        const int nb = n / R;
+        const V* tws = tw + f.twoff[s];
+        const FastDiv dnb = f.nbdiv[s], dmm = f.mmdiv[s];
+        for (int idx = tid; idx < nb * nrows; idx += nthr) {
+            const int row = fdiv(idx, dnb);
+            const int bi = idx - row * nb;
+            const int b = fdiv(bi, dmm);
+            const int j = bi - b * mm;
+            dit_bfly<DIR>(buf + (size_t)row * rs + b * L + j, mm, R, j, tws + j * (R - 1));
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace prj

@@ -142,6 +142,29 @@ int make_dif(int n, prj::DifFft* d, size_t* bytes) {
     return PRJ_OK;
 }
 
+// slot -> wavenumber table of the length-n in-place plan (inverse of its position table)
+int make_slot_table(int n, int** d_out, size_t* bytes) {
+    prj::DifDev f{};
+    const long ntw = prj::dif_plan(n, &f);
+    if (ntw < 0) return fail(PRJ_ERR_UNSUPPORTED, "no in-place plan for length %d", n);
+    std::vector<double2> tw((size_t)ntw);
+    std::vector<int> pos((size_t)n), kz((size_t)n);
+    prj::dif_fill(f, tw.data(), pos.data());
+    for (int k = 0; k < n; k++) kz[pos[k]] = k;
+    CK(cudaMalloc((void**)d_out, kz.size() * sizeof(int)), "cudaMalloc(slot table)");
+    CK(cudaMemcpy(*d_out, kz.data(), kz.size() * sizeof(int), cudaMemcpyHostToDevice), "cudaMemcpy(slot table)");
+    *bytes += kz.size() * sizeof(int);
+    return PRJ_OK;
+}
+
+// z-direction kernel choice: PRJ_ZSOLVE=split|fused|basic (split needs the in-place plan)
+int z_mode(bool split_ok) {
+    const char* v = getenv("PRJ_ZSOLVE");
+    if (v && !strcmp(v, "fused")) return 1;
+    if (v && !strcmp(v, "basic")) return 2;
+    return split_ok ? 0 : 1;
+}
+
 void free_plan_buffers(prj_plan* pl) {
     dfree(pl->t.bands);
     dfree(pl->t.inv_dy_p);
@@ -157,6 +180,7 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->xd.pos);
     dfree(pl->zd.tw);
     dfree(pl->zd.pos);
+    dfree(pl->kz_of_slot);
     pl->xd.ok = pl->zd.ok = false;
     dfree(pl->spec);
     dfree(pl->stat_buf);
@@ -218,14 +242,36 @@ struct StageTimer {
     }
 };
 
+// z transforms + Thomas: three kernels (split) or one fused kernel
+int run_zsolve(prj_plan* pl, cudaStream_t st) {
+    if (pl->zmode == 0) {
+        {
+            StageTimer tm(pl, prj::kStZfftFwd, st);
+            CK(prj::launch_zfft(pl, -1, st), "z transform");
+        }
+        {
+            StageTimer tm(pl, prj::kStThomas, st);
+            CK(prj::launch_thomas(pl, st), "Thomas sweeps");
+        }
+        {
+            StageTimer tm(pl, prj::kStZfftInv, st);
+            CK(prj::launch_zfft(pl, +1, st), "inverse z transform");
+        }
+        return PRJ_OK;
+    }
+    StageTimer tm(pl, prj::kStZSolve, st);
+    CK(prj::launch_zsolve(pl, st), "z transform + Thomas");
+    return PRJ_OK;
+}
+
 int run_poisson(prj_plan* pl, double* d_P, cudaStream_t st) {
     {
         StageTimer tm(pl, prj::kStFwdX, st);
         CK(prj::launch_fwd_x(pl, prj::FwdSource::Pressure, d_P, nullptr, nullptr, nullptr, nullptr, st), "forward x");
     }
     {
-        StageTimer tm(pl, prj::kStZSolve, st);
-        CK(prj::launch_zsolve(pl, st), "z transform + Thomas");
+        const int rz = run_zsolve(pl, st);
+        if (rz) return rz;
     }
     {
         StageTimer tm(pl, prj::kStBwdX, st);
@@ -381,6 +427,8 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if ((rc = make_cfft<double>(nz, &pl->fz64.f, &pl->fz64.tw, &bytes))) return bail(rc);
     if ((rc = make_dif(pl->fx64.m, &pl->xd, &bytes))) return bail(rc);
     if ((rc = make_dif(nz, &pl->zd, &bytes))) return bail(rc);
+    if (pl->zd.ok && (rc = make_slot_table(nz, &pl->kz_of_slot, &bytes))) return bail(rc);
+    pl->zmode = z_mode(pl->zd.ok && pl->kz_of_slot);
     pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);
 
     // rows per CTA of the x kernels: fit two ping-pong buffers in ~100 KB
@@ -513,6 +561,9 @@ const char* prj_stage_name(int stage) {
     case prj::kStBwdX: return "k_bwd_x";
     case prj::kStCorrect: return "k_correct";
     case prj::kStStats: return "k_stats";
+    case prj::kStZfftFwd: return "k_zfft_fwd";
+    case prj::kStThomas: return "k_thomas";
+    case prj::kStZfftInv: return "k_zfft_inv";
     default: return "";
     }
 }
@@ -548,8 +599,8 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
         CK(prj::launch_fwd_x(plan, prj::FwdSource::Divergence, nullptr, d_Uh, d_Vh, d_Wh, &sc, st), "divergence + forward x");
     }
     {
-        StageTimer tm(plan, prj::kStZSolve, st);
-        CK(prj::launch_zsolve(plan, st), "z transform + Thomas");
+        const int rz = run_zsolve(plan, st);
+        if (rz) return rz;
     }
     {
         StageTimer tm(plan, prj::kStBwdX, st);

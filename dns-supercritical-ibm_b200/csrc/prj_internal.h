@@ -65,7 +65,10 @@ struct DeviceTables {
 
 namespace prj {
 // stage ids of the per-kernel timing record
-enum Stage { kStFwdX = 0, kStZSolve = 1, kStBwdX = 2, kStCorrect = 3, kStStats = 4, kNumStages = 8 };
+enum Stage {
+    kStFwdX = 0, kStZSolve = 1, kStBwdX = 2, kStCorrect = 3, kStStats = 4,
+    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kNumStages = 8
+};
 
 struct StageRecord {
     int stage;
@@ -94,6 +97,8 @@ struct prj_plan {
     prj::DifFft xd;               // in-place transform of length fx64.m (x rows)
     prj::DifFft zd;               // in-place transform of length nz (z rows)
     int tz_xd = 1;                // rows per CTA of the in-place x-transform kernels
+    int* kz_of_slot = nullptr;    // z wavenumber held by each slot of zd's output
+    int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
 };
 
 namespace prj {
@@ -126,6 +131,10 @@ cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, co
                           const double* Wh, const StepScalars* sc, cudaStream_t st);
 cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st);
 int choose_tz_xd(int m, bool even);
+
+// z direction as separate kernels (prj_zsplit.cu); need pl->zd.ok and pl->kz_of_slot
+cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st);
+cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st);
 
 // stat_buf slots: [0] min pivot (bits), [2] max|div u|, [3] max|P|, [6] device error word
 constexpr int kStatErrSlot = 6;

@@ -320,39 +320,44 @@ struct CorrArgs {
 // u = u_hat - dt grad P on the whole halo'd box (mod_cfd_subroutines.f90:1124-1152);
 // x/z halos take the periodic image (the halo exchange of :1225-1231), the
 // y slices -1 and ny (and V at k = 0) take the wall values (:1234-1244).
-__global__ void k_correct(const CorrArgs a) {
+__global__ void __launch_bounds__(128) k_correct(const CorrArgs a) {
+    // one block per halo'd x-row (jh, kh): no index division, coalesced along x
     const int nx = a.nx, nz = a.nz, ny = a.ny;
-    const size_t tot = (size_t)(nx + 2) * (nz + 2) * (ny + 2);
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < tot; idx += (size_t)gridDim.x * blockDim.x) {
-        const int ih = (int)(idx % (size_t)(nx + 2));
-        const size_t rest = idx / (size_t)(nx + 2);
-        const int jh = (int)(rest % (size_t)(nz + 2));
-        const int k = (int)(rest / (size_t)(nz + 2)) - 1;
-        double u, v, w;
-        if (k < 0) { u = a.wall[0]; v = a.wall[1]; w = a.wall[2]; }
-        else if (k == ny) { u = a.wall[3]; v = a.wall[4]; w = a.wall[5]; }
-        else {
-            const int i = ih - 1, j = jh - 1;
-            const int iw = i < 0 ? nx - 1 : (i == nx ? 0 : i);
-            const int jw = j < 0 ? nz - 1 : (j == nz ? 0 : j);
-            const int im = iw == 0 ? nx - 1 : iw - 1;
-            const int jm = jw == 0 ? nz - 1 : jw - 1;
-            const size_t pr = ((size_t)k * nz + jw) * nx;
-            const double p0 = a.P[pr + iw];
-            const double pim = a.P[pr + im];
-            const double pjm = a.P[((size_t)k * nz + jm) * nx + iw];
-            const size_t hw = hidx(nx, nz, iw, jw, k);
-            u = __dsub_rn(a.Uh[hw], __dmul_rn(__dmul_rn(a.dt, __dsub_rn(p0, pim)), a.inv_dx));
-            w = __dsub_rn(a.Wh[hw], __dmul_rn(__dmul_rn(a.dt, __dsub_rn(p0, pjm)), a.inv_dz));
-            if (k == 0) v = a.wall[1];
-            else {
-                const double pkm = a.P[((size_t)(k - 1) * nz + jw) * nx + iw];
-                v = __dsub_rn(a.Vh[hw], __dmul_rn(a.dt, __dadd_rn(__dmul_rn(a.hi[k], p0), __dmul_rn(a.lo[k], pkm))));
-            }
+    const int jh = blockIdx.y;
+    const int k = (int)blockIdx.x - 1;
+    const size_t rowh = (size_t)(nx + 2) * ((size_t)jh + (size_t)(nz + 2) * (size_t)(k + 1));
+    if (k < 0 || k == ny) {
+        const double u = k < 0 ? a.wall[0] : a.wall[3];
+        const double v = k < 0 ? a.wall[1] : a.wall[4];
+        const double w = k < 0 ? a.wall[2] : a.wall[5];
+        for (int ih = threadIdx.x; ih < nx + 2; ih += blockDim.x) {
+            a.U[rowh + ih] = u;
+            a.V[rowh + ih] = v;
+            a.W[rowh + ih] = w;
         }
-        a.U[idx] = u;
-        a.V[idx] = v;
-        a.W[idx] = w;
+        return;
+    }
+    const int j = jh - 1;
+    const int jw = j < 0 ? nz - 1 : (j == nz ? 0 : j);
+    const int jm = jw == 0 ? nz - 1 : jw - 1;
+    const double* P0 = a.P + ((size_t)k * nz + jw) * nx;
+    const double* Pjm = a.P + ((size_t)k * nz + jm) * nx;
+    const double* Pkm = a.P + ((size_t)(k > 0 ? k - 1 : 0) * nz + jw) * nx;
+    const size_t roww = (size_t)(nx + 2) * ((size_t)(jw + 1) + (size_t)(nz + 2) * (size_t)(k + 1));
+    const double hi = a.hi[k], lo = a.lo[k];
+    for (int ih = threadIdx.x; ih < nx + 2; ih += blockDim.x) {
+        const int i = ih - 1;
+        const int iw = i < 0 ? nx - 1 : (i == nx ? 0 : i);
+        const int im = iw == 0 ? nx - 1 : iw - 1;
+        const double p0 = P0[iw];
+        const size_t hw = roww + (size_t)(iw + 1);
+        const double u = __dsub_rn(a.Uh[hw], __dmul_rn(__dmul_rn(a.dt, __dsub_rn(p0, P0[im])), a.inv_dx));
+        const double w = __dsub_rn(a.Wh[hw], __dmul_rn(__dmul_rn(a.dt, __dsub_rn(p0, Pjm[iw])), a.inv_dz));
+        double v = a.wall[1];
+        if (k > 0) v = __dsub_rn(a.Vh[hw], __dmul_rn(a.dt, __dadd_rn(__dmul_rn(hi, p0), __dmul_rn(lo, Pkm[iw]))));
+        a.U[rowh + ih] = u;
+        a.V[rowh + ih] = v;
+        a.W[rowh + ih] = w;
     }
 }
 
@@ -445,7 +450,7 @@ cudaError_t launch_bwd_x(const prj_plan* pl, double* P, cudaStream_t st) {
 }
 
 cudaError_t launch_zsolve(const prj_plan* pl, cudaStream_t st) {
-    {
+    if (pl->zmode != 2) {
         cudaError_t ep = launch_zsolve_pipelined(pl, reinterpret_cast<int*>(pl->stat_buf + kStatErrSlot), st);
         if (ep != cudaErrorNotSupported) return ep;
     }
@@ -487,11 +492,8 @@ cudaError_t launch_correction(const prj_plan* pl, const double* P, const double*
     a.U = U; a.V = V; a.W = W;
     a.dt = sc.dt; a.inv_dx = 1.0 / g.dx; a.inv_dz = 1.0 / g.dz;
     for (int i = 0; i < 6; i++) a.wall[i] = sc.wall[i];
-    const size_t tot = (size_t)(g.nx + 2) * (g.nz + 2) * (g.ny + 2);
-    size_t blocks = (tot + 255) / 256;
-    const size_t cap = (size_t)sm_count() * 16;
-    if (blocks > cap) blocks = cap;
-    k_correct<<<(unsigned)blocks, 256, 0, st>>>(a);
+    const dim3 grid((unsigned)(g.ny + 2), (unsigned)(g.nz + 2));
+    k_correct<<<grid, 128, 0, st>>>(a);
     return cudaGetLastError();
 }
 

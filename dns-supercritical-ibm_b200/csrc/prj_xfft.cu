@@ -17,6 +17,8 @@ namespace prj {
 
 namespace {
 
+constexpr int kUnroll = 4;  // global loads kept in flight per thread in the load phases
+
 __device__ __forceinline__ size_t hidx_d(int nx, int nz, int i, int j, int k) {
     return (size_t)(i + 1) + (size_t)(nx + 2) * ((size_t)(j + 1) + (size_t)(nz + 2) * (size_t)(k + 1));
 }
@@ -62,13 +64,29 @@ __global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
     const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
     const int m = a.m, nx = a.nx;
     for (int i = tid; i < m; i += nthr) pos[i] = a.pos[i];
-    for (int idx = tid; idx < a.tz * nx; idx += nthr) {
-        const int r = idx / nx, i = idx - r * nx;
-        const int z = z0 + r;
-        double v = 0.0;
-        if (z < a.nz) v = (SRC == 0) ? a.P[((size_t)y * a.nz + z) * nx + i] : div_at(a, i, z, y);
-        if (a.even) reinterpret_cast<double*>(A + (size_t)r * a.rs)[i] = v;
-        else A[(size_t)r * a.rs + i] = make_double2(v, 0.0);
+    // kUnroll elements per thread per batch: their loads are independent and in flight together
+    const int total = a.tz * nx;
+    for (int base = tid; base < total; base += kUnroll * nthr) {
+        double v[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int idx = base + u * nthr;
+            v[u] = 0.0;
+            if (idx < total) {
+                const int r = idx / nx, i = idx - r * nx;
+                const int z = z0 + r;
+                if (z < a.nz) v[u] = (SRC == 0) ? a.P[((size_t)y * a.nz + z) * nx + i] : div_at(a, i, z, y);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int idx = base + u * nthr;
+            if (idx < total) {
+                const int r = idx / nx, i = idx - r * nx;
+                if (a.even) reinterpret_cast<double*>(A + (size_t)r * a.rs)[i] = v[u];
+                else A[(size_t)r * a.rs + i] = make_double2(v[u], 0.0);
+            }
+        }
     }
     __syncthreads();
     dif_rows<-1>(A, a.tz, a.rs, a.f, a.tw);
@@ -112,10 +130,27 @@ __global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
     const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
     const int m = a.m, nx = a.nx;
     for (int i = tid; i < m; i += nthr) pos[i] = a.pos[i];
-    for (int idx = tid; idx < a.nh * a.tz; idx += nthr) {
-        const int kx = idx / a.tz, r = idx - kx * a.tz;
-        const int z = z0 + r;
-        A[(size_t)r * a.rs + kx] = (z < a.nz) ? a.X[((size_t)y * a.nh + kx) * a.nz + z] : make_double2(0.0, 0.0);
+    const int total = a.nh * a.tz;
+    for (int base = tid; base < total; base += kUnroll * nthr) {
+        double2 v[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int idx = base + u * nthr;
+            v[u] = make_double2(0.0, 0.0);
+            if (idx < total) {
+                const int kx = idx / a.tz, r = idx - kx * a.tz;
+                const int z = z0 + r;
+                if (z < a.nz) v[u] = a.X[((size_t)y * a.nh + kx) * a.nz + z];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int idx = base + u * nthr;
+            if (idx < total) {
+                const int kx = idx / a.tz, r = idx - kx * a.tz;
+                A[(size_t)r * a.rs + kx] = v[u];
+            }
+        }
     }
     __syncthreads();
     const double s = a.scale;
