@@ -55,51 +55,50 @@ __device__ __forceinline__ V twiddle(V a, V w) {
     return DIR < 0 ? cmul(a, w) : cmulc(a, w);
 }
 
-template <int DIR, typename V>
-__device__ __forceinline__ void dif_bfly(V* __restrict__ p, int mm, int R, int j, const V* __restrict__ w) {
+// Shared-memory slot of element g.  PAD inserts one empty 16-byte slot after
+// every 8 elements, so strides that are multiples of 8 elements (the late
+// stages and the digit-reversal gathers) spread over all bank groups.
+template <bool PAD>
+__device__ __forceinline__ int sidx(int g) {
+    return PAD ? g + (g >> 3) : g;
+}
+
+// elements per row buffer of n slots with optional padding
+__host__ __device__ inline int padded_len(int n, bool pad) { return pad ? n + (n >> 3) + 1 : n; }
+
+// One butterfly of radix R on elements g0 + r mm (r < R) of buf.
+// DIT = false: DFT, then twiddles (decimation in frequency);
+// DIT = true: twiddles, then DFT (its transpose).
+template <int DIR, bool DIT, bool PAD, int R, typename V>
+__device__ __forceinline__ void bfly_r(V* __restrict__ buf, int g0, int mm, int j, const V* __restrict__ w) {
+    V a[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) a[r] = buf[sidx<PAD>(g0 + r * mm)];
+    if (DIT && j) {
+#pragma unroll
+        for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
+    }
+    if (R == 2) dft2<DIR>(a[0], a[1]);
+    else if (R == 3) dft3<DIR>(a[0], a[1], a[2]);
+    else if (R == 4) dft4<DIR>(a[0], a[1], a[2], a[3]);
+    else if (R == 5) dft5<DIR>(a[0], a[1], a[2], a[3], a[4]);
+    else dft8<DIR>(a);
+    if (!DIT && j) {
+#pragma unroll
+        for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) buf[sidx<PAD>(g0 + r * mm)] = a[r];
+}
+
+template <int DIR, bool DIT, bool PAD, typename V>
+__device__ __forceinline__ void bfly(V* __restrict__ buf, int g0, int mm, int R, int j, const V* __restrict__ w) {
     switch (R) {
-    case 2: {
-        V a0 = p[0], a1 = p[mm];
-        dft2<DIR>(a0, a1);
-        if (j) a1 = twiddle<DIR>(a1, w[0]);
-        p[0] = a0; p[mm] = a1;
-    } break;
-    case 3: {
-        V a0 = p[0], a1 = p[mm], a2 = p[2 * mm];
-        dft3<DIR>(a0, a1, a2);
-        if (j) { a1 = twiddle<DIR>(a1, w[0]); a2 = twiddle<DIR>(a2, w[1]); }
-        p[0] = a0; p[mm] = a1; p[2 * mm] = a2;
-    } break;
-    case 4: {
-        V a0 = p[0], a1 = p[mm], a2 = p[2 * mm], a3 = p[3 * mm];
-        dft4<DIR>(a0, a1, a2, a3);
-        if (j) { a1 = twiddle<DIR>(a1, w[0]); a2 = twiddle<DIR>(a2, w[1]); a3 = twiddle<DIR>(a3, w[2]); }
-        p[0] = a0; p[mm] = a1; p[2 * mm] = a2; p[3 * mm] = a3;
-    } break;
-    case 5: {
-        V a[5];
-#pragma unroll
-        for (int r = 0; r < 5; r++) a[r] = p[r * mm];
-        dft5<DIR>(a[0], a[1], a[2], a[3], a[4]);
-        if (j) {
-#pragma unroll
-            for (int q = 1; q < 5; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
-        }
-#pragma unroll
-        for (int r = 0; r < 5; r++) p[r * mm] = a[r];
-    } break;
-    case 8: {
-        V a[8];
-#pragma unroll
-        for (int r = 0; r < 8; r++) a[r] = p[r * mm];
-        dft8<DIR>(a);
-        if (j) {
-#pragma unroll
-            for (int q = 1; q < 8; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
-        }
-#pragma unroll
-        for (int r = 0; r < 8; r++) p[r * mm] = a[r];
-    } break;
+    case 2: bfly_r<DIR, DIT, PAD, 2>(buf, g0, mm, j, w); break;
+    case 3: bfly_r<DIR, DIT, PAD, 3>(buf, g0, mm, j, w); break;
+    case 4: bfly_r<DIR, DIT, PAD, 4>(buf, g0, mm, j, w); break;
+    case 5: bfly_r<DIR, DIT, PAD, 5>(buf, g0, mm, j, w); break;
+    case 8: bfly_r<DIR, DIT, PAD, 8>(buf, g0, mm, j, w); break;
     default:
         // other radices are planned on the out-of-place Stockham path (fft_device.cuh);
         // the host never builds a DifDev containing them (dif_supported)
@@ -107,102 +106,42 @@ __device__ __forceinline__ void dif_bfly(V* __restrict__ p, int mm, int R, int j
     }
 }
 
-// In-place transform of `nrows` rows (stride rs).  Starts and ends with the
-// CTA synchronised.
+// In-place transform of `nrows` rows of n elements (row r starts at element
+// r * rs; with PAD, element g of the buffer lives at slot g + g/8).  DIT = false:
+// decimation in frequency, natural order in, digit-reversed out.  DIT = true:
+// decimation in time with the same plan, digit-reversed in, natural out; with
+// DIR = +1 it inverts the DIF transform up to the factor n.  Starts and ends
+// with the CTA synchronised.
+template <int DIR, bool DIT, bool PAD, typename V>
+__device__ void inplace_rows(V* buf, int nrows, int rs, const DifDev& f, const V* __restrict__ tw) {
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int n = f.n;
+    for (int t = 0; t < f.nst; t++) {
+        const int s = DIT ? f.nst - 1 - t : t;
+        const int R = f.radix[s], L = f.span[s];
+        const int mm = L / R;
+        const int nb = n / R;
+        const V* tws = tw + f.twoff[s];
+        const FastDiv dnb = f.nbdiv[s], dmm = f.mmdiv[s];
+        for (int idx = tid; idx < nb * nrows; idx += nthr) {
+            const int row = fdiv(idx, dnb);
+            const int bi = idx - row * nb;
+            const int b = fdiv(bi, dmm);
+            const int j = bi - b * mm;
+            bfly<DIR, DIT, PAD>(buf, row * rs + b * L + j, mm, R, j, tws + j * (R - 1));
+        }
+        __syncthreads();
+    }
+}
+
 template <int DIR, typename V>
 __device__ void dif_rows(V* buf, int nrows, int rs, const DifDev& f, const V* __restrict__ tw) {
-    const int nthr = blockDim.x, tid = threadIdx.x;
-    const int n = f.n;
-    for (int s = 0; s < f.nst; s++) {
-        const int R = f.radix[s], L = f.span[s];
-        const int mm = L / R;
-        const int nb = n / R;
-        const V* tws = tw + f.twoff[s];
-        const FastDiv dnb = f.nbdiv[s], dmm = f.mmdiv[s];
-        for (int idx = tid; idx < nb * nrows; idx += nthr) {
-            const int row = fdiv(idx, dnb);
-            const int bi = idx - row * nb;
-            const int b = fdiv(bi, dmm);
-            const int j = bi - b * mm;
-            dif_bfly<DIR>(buf + (size_t)row * rs + b * L + j, mm, R, j, tws + j * (R - 1));
-        }
-        __syncthreads();
-    }
+    inplace_rows<DIR, false, false>(buf, nrows, rs, f, tw);
 }
 
-// One DIT butterfly: the transpose of dif_bfly (twiddles first, then the DFT).
-template <int DIR, typename V>
-__device__ __forceinline__ void dit_bfly(V* __restrict__ p, int mm, int R, int j, const V* __restrict__ w) {
-    switch (R) {
-    case 2: {
-        V a0 = p[0], a1 = p[mm];
-        if (j) a1 = twiddle<DIR>(a1, w[0]);
-        dft2<DIR>(a0, a1);
-        p[0] = a0; p[mm] = a1;
-    } break;
-    case 3: {
-        V a0 = p[0], a1 = p[mm], a2 = p[2 * mm];
-        if (j) { a1 = twiddle<DIR>(a1, w[0]); a2 = twiddle<DIR>(a2, w[1]); }
-        dft3<DIR>(a0, a1, a2);
-        p[0] = a0; p[mm] = a1; p[2 * mm] = a2;
-    } break;
-    case 4: {
-        V a0 = p[0], a1 = p[mm], a2 = p[2 * mm], a3 = p[3 * mm];
-        if (j) { a1 = twiddle<DIR>(a1, w[0]); a2 = twiddle<DIR>(a2, w[1]); a3 = twiddle<DIR>(a3, w[2]); }
-        dft4<DIR>(a0, a1, a2, a3);
-        p[0] = a0; p[mm] = a1; p[2 * mm] = a2; p[3 * mm] = a3;
-    } break;
-    case 5: {
-        V a[5];
-#pragma unroll
-        for (int r = 0; r < 5; r++) a[r] = p[r * mm];
-        if (j) {
-#pragma unroll
-            for (int q = 1; q < 5; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
-        }
-        dft5<DIR>(a[0], a[1], a[2], a[3], a[4]);
-#pragma unroll
-        for (int r = 0; r < 5; r++) p[r * mm] = a[r];
-    } break;
-    case 8: {
-        V a[8];
-#pragma unroll
-        for (int r = 0; r < 8; r++) a[r] = p[r * mm];
-        if (j) {
-#pragma unroll
-            for (int q = 1; q < 8; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
-        }
-        dft8<DIR>(a);
-#pragma unroll
-        for (int r = 0; r < 8; r++) p[r * mm] = a[r];
-    } break;
-    default:
-        break;
-    }
-}
-
-// In-place decimation-in-time transform with the same plan as dif_rows: input in
-// digit-reversed order (index k at slot pos[k]), output in natural order.  With
-// DIR = +1 it inverts dif_rows<-1> up to the factor n (unnormalised inverse).
 template <int DIR, typename V>
 __device__ void dit_rows(V* buf, int nrows, int rs, const DifDev& f, const V* __restrict__ tw) {
-    const int nthr = blockDim.x, tid = threadIdx.x;
-    const int n = f.n;
-    for (int s = f.nst - 1; s >= 0; s--) {
-        const int R = f.radix[s], L = f.span[s];
-        const int mm = L / R;
-        const int nb = n / R;
-        const V* tws = tw + f.twoff[s];
-        const FastDiv dnb = f.nbdiv[s], dmm = f.mmdiv[s];
-        for (int idx = tid; idx < nb * nrows; idx += nthr) {
-            const int row = fdiv(idx, dnb);
-            const int bi = idx - row * nb;
-            const int b = fdiv(bi, dmm);
-            const int j = bi - b * mm;
-            dit_bfly<DIR>(buf + (size_t)row * rs + b * L + j, mm, R, j, tws + j * (R - 1));
-        }
-        __syncthreads();
-    }
+    inplace_rows<DIR, true, false>(buf, nrows, rs, f, tw);
 }
 
 }  // namespace prj

@@ -55,11 +55,14 @@ __device__ __forceinline__ double div_at(const XArgs& a, int i, int j, int k) {
     return __dmul_rn(a.inv_dt, s);
 }
 
+// element g of the tz x rs row buffer lives at slot S(g) = g + g/8 (bank-conflict padding)
+#define S(g) sidx<true>(g)
+
 template <int SRC>
 __global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
-    int* pos = reinterpret_cast<int*>(sm + (size_t)a.tz * a.rs * sizeof(double2));
+    int* pos = reinterpret_cast<int*>(sm + (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2));
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
     const int m = a.m, nx = a.nx;
@@ -83,32 +86,32 @@ __global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
             const int idx = base + u * nthr;
             if (idx < total) {
                 const int r = idx / nx, i = idx - r * nx;
-                if (a.even) reinterpret_cast<double*>(A + (size_t)r * a.rs)[i] = v[u];
-                else A[(size_t)r * a.rs + i] = make_double2(v[u], 0.0);
+                if (a.even) reinterpret_cast<double*>(A)[2 * S(r * a.rs + (i >> 1)) + (i & 1)] = v[u];
+                else A[S(r * a.rs + i)] = make_double2(v[u], 0.0);
             }
         }
     }
     __syncthreads();
-    dif_rows<-1>(A, a.tz, a.rs, a.f, a.tw);
+    inplace_rows<-1, false, true>(A, a.tz, a.rs, a.f, a.tw);
     if (a.even) {
         // split: X_k = E_k + W^k O_k and X_{m-k} = conj(E_k) + W^{m-k} conj(O_k), in place
         const int half = m / 2;
         for (int idx = tid; idx < a.tz * (half + 1); idx += nthr) {
             const int r = idx / (half + 1), k = idx - r * (half + 1);
-            double2* Z = A + (size_t)r * a.rs;
+            const int base = r * a.rs;
             if (k == 0) {
-                const double2 z = Z[pos[0]];
-                Z[pos[0]] = make_double2(z.x + z.y, 0.0);
-                Z[m] = make_double2(z.x - z.y, 0.0);
+                const double2 z = A[S(base + pos[0])];
+                A[S(base + pos[0])] = make_double2(z.x + z.y, 0.0);
+                A[S(base + m)] = make_double2(z.x - z.y, 0.0);
             } else {
                 const int kk = m - k;
-                const double2 zk = Z[pos[k]];
-                const double2 zm = cconj(Z[pos[kk]]);
+                const double2 zk = A[S(base + pos[k])];
+                const double2 zm = cconj(A[S(base + pos[kk])]);
                 const double2 e = cscale(cadd(zk, zm), 0.5);
                 const double2 d = csub(zk, zm);
                 const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
-                Z[pos[k]] = cadd(e, cmul(a.post[k], o));
-                if (kk != k) Z[pos[kk]] = cadd(cconj(e), cmul(a.post[kk], cconj(o)));
+                A[S(base + pos[k])] = cadd(e, cmul(a.post[k], o));
+                if (kk != k) A[S(base + pos[kk])] = cadd(cconj(e), cmul(a.post[kk], cconj(o)));
             }
         }
         __syncthreads();
@@ -118,14 +121,14 @@ __global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
         const int z = z0 + r;
         if (z >= a.nz) continue;
         const int slot = (a.even && kx == m) ? m : pos[kx];
-        a.X[((size_t)y * a.nh + kx) * a.nz + z] = A[(size_t)r * a.rs + slot];
+        a.X[((size_t)y * a.nh + kx) * a.nz + z] = A[S(r * a.rs + slot)];
     }
 }
 
 __global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
-    int* pos = reinterpret_cast<int*>(sm + (size_t)a.tz * a.rs * sizeof(double2));
+    int* pos = reinterpret_cast<int*>(sm + (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2));
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
     const int m = a.m, nx = a.nx;
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
             const int idx = base + u * nthr;
             if (idx < total) {
                 const int kx = idx / a.tz, r = idx - kx * a.tz;
-                A[(size_t)r * a.rs + kx] = v[u];
+                A[S(r * a.rs + kx)] = v[u];
             }
         }
     }
@@ -159,20 +162,20 @@ __global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
         const int half = m / 2;
         for (int idx = tid; idx < a.tz * (half + 1); idx += nthr) {
             const int r = idx / (half + 1), k = idx - r * (half + 1);
-            double2* Z = A + (size_t)r * a.rs;
+            const int base = r * a.rs;
             if (k == 0) {
-                const double x0 = Z[0].x, xm = Z[m].x;
-                Z[0] = make_double2((x0 + xm) * s, (x0 - xm) * s);
+                const double x0 = A[S(base)].x, xm = A[S(base + m)].x;
+                A[S(base)] = make_double2((x0 + xm) * s, (x0 - xm) * s);
             } else {
                 const int kk = m - k;
-                const double2 xk = Z[k], xkk = Z[kk];
+                const double2 xk = A[S(base + k)], xkk = A[S(base + kk)];
                 const double2 e1 = cadd(xk, cconj(xkk));
                 const double2 o1 = cmulc(csub(xk, cconj(xkk)), a.post[k]);
-                Z[k] = cscale(make_double2(e1.x - o1.y, e1.y + o1.x), s);
+                A[S(base + k)] = cscale(make_double2(e1.x - o1.y, e1.y + o1.x), s);
                 if (kk != k) {
                     const double2 e2 = cadd(xkk, cconj(xk));
                     const double2 o2 = cmulc(csub(xkk, cconj(xk)), a.post[kk]);
-                    Z[kk] = cscale(make_double2(e2.x - o2.y, e2.y + o2.x), s);
+                    A[S(base + kk)] = cscale(make_double2(e2.x - o2.y, e2.y + o2.x), s);
                 }
             }
         }
@@ -180,26 +183,26 @@ __global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
         // Hermitian completion of the odd-length row, scaled
         for (int idx = tid; idx < a.tz * a.nh; idx += nthr) {
             const int r = idx / a.nh, k = idx - r * a.nh;
-            double2* Z = A + (size_t)r * a.rs;
-            double2 v = Z[k];
+            const int base = r * a.rs;
+            double2 v = A[S(base + k)];
             if (k == 0) v.y = 0.0;
             v = cscale(v, s);
-            Z[k] = v;
-            if (k > 0) Z[m - k] = cconj(v);
+            A[S(base + k)] = v;
+            if (k > 0) A[S(base + m - k)] = cconj(v);
         }
     }
     __syncthreads();
-    dif_rows<+1>(A, a.tz, a.rs, a.f, a.tw);
+    inplace_rows<+1, false, true>(A, a.tz, a.rs, a.f, a.tw);
     for (int idx = tid; idx < a.tz * nx; idx += nthr) {
         const int r = idx / nx, i = idx - r * nx;
         const int z = z0 + r;
         if (z >= a.nz) continue;
         double v;
         if (a.even) {
-            const double2 c = A[(size_t)r * a.rs + pos[i >> 1]];
+            const double2 c = A[S(r * a.rs + pos[i >> 1])];
             v = (i & 1) ? c.y : c.x;
         } else {
-            v = A[(size_t)r * a.rs + pos[i]].x;
+            v = A[S(r * a.rs + pos[i])].x;
         }
         a.Pout[((size_t)y * a.nz + z) * nx + i] = v;
     }
@@ -218,7 +221,9 @@ XArgs make_args(const prj_plan* pl) {
     return a;
 }
 
-size_t smem_bytes(const XArgs& a) { return (size_t)a.tz * a.rs * sizeof(double2) + (size_t)a.m * sizeof(int); }
+size_t smem_bytes(const XArgs& a) {
+    return (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2) + (size_t)a.m * sizeof(int);
+}
 
 template <typename K>
 cudaError_t allow_smem(K kernel, size_t bytes) {
@@ -230,9 +235,9 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 // rows per CTA of the in-place x kernels: a power of two up to 16 within ~56 KB
 int choose_tz_xd(int m, bool even) {
-    const size_t row = (size_t)(even ? m + 1 : m) * sizeof(double2);
+    const int rs = even ? m + 1 : m;
     int tz = 16;
-    while (tz > 1 && (size_t)tz * row + (size_t)m * sizeof(int) > 56 * 1024) tz /= 2;
+    while (tz > 1 && (size_t)padded_len(tz * rs, true) * sizeof(double2) + (size_t)m * sizeof(int) > 56 * 1024) tz /= 2;
     return tz;
 }
 
@@ -265,5 +270,7 @@ cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st) {
     k_bwd_xd<<<grid, 256, smem, st>>>(a);
     return cudaGetLastError();
 }
+
+#undef S
 
 }  // namespace prj

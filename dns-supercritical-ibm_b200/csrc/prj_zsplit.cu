@@ -48,14 +48,14 @@ __global__ void __launch_bounds__(256) k_zfft(const ZfftArgs a) {
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const int i = base + u * nthr;
-            if (i < tot) zs[i] = v[u];
+            if (i < tot) zs[sidx<true>(i)] = v[u];
         }
     }
     __syncthreads();
-    if (DIR < 0) dif_rows<-1>(zs, nr, a.nz, a.f, a.tw);
-    else dit_rows<+1>(zs, nr, a.nz, a.f, a.tw);
+    if (DIR < 0) inplace_rows<-1, false, true>(zs, nr, a.nz, a.f, a.tw);
+    else inplace_rows<+1, true, true>(zs, nr, a.nz, a.f, a.tw);
     double2* dst = a.X + row0 * a.nz;
-    for (int i = tid; i < tot; i += nthr) dst[i] = zs[i];
+    for (int i = tid; i < tot; i += nthr) dst[i] = zs[sidx<true>(i)];
 }
 
 struct ThomasArgs {
@@ -67,7 +67,7 @@ struct ThomasArgs {
 };
 
 constexpr int kThomasTile = 128;
-constexpr int kBlock = 8;  // planes loaded together (independent loads in flight)
+constexpr int kBlock = 4;  // planes loaded together (independent loads in flight)
 
 __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
     const int kx = blockIdx.x / a.tiles;
@@ -164,9 +164,10 @@ cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st) {
     a.X = pl->spec;
     const size_t row = (size_t)g.nz * sizeof(double2);
     int rb = 16;
-    while (rb > 1 && rb * row > 48 * 1024) rb /= 2;
+    while (rb > 1 && (size_t)padded_len(rb * g.nz, true) * sizeof(double2) > 48 * 1024) rb /= 2;
     a.rb = rb;
-    const size_t smem = rb * row;
+    const size_t smem = (size_t)padded_len(rb * g.nz, true) * sizeof(double2);
+    (void)row;
     const unsigned grid = (unsigned)((a.nrow_total + rb - 1) / rb);
     cudaError_t e;
     if (dir < 0) {
