@@ -132,7 +132,8 @@ def kernel_alg_bytes(nx, ny, nz):
     N = nx * ny * nz
     Nh = (nx + 2) * (nz + 2) * (ny + 2)
     S = (nx // 2 + 1) * nz * ny * 16  # one pass over the complex half-spectrum
-    return {"k_fwd_x": 24 * N + S, "k_zsolve": 2 * S, "k_bwd_x": S + 8 * N, "k_correct": 32 * N + 24 * Nh}
+    return {"k_fwd_x": 24 * N + S, "k_zsolve": 2 * S, "k_bwd_x": S + 8 * N, "k_correct": 32 * N + 24 * Nh,
+            "k_zfft_fwd": 2 * S, "k_thomas": 2 * S, "k_zfft_inv": 2 * S, "k_stats": 32 * N}
 
 
 def read_traffic(kernel):

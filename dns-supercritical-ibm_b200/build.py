@@ -47,6 +47,8 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
         cmd.insert(1, "-Xptxas=-v")
     if extra:
         cmd[1:1] = list(extra)
+    if os.environ.get("PRJ_NVCC_FLAGS"):  # experiments: extra -D options
+        cmd[1:1] = os.environ["PRJ_NVCC_FLAGS"].split()
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)

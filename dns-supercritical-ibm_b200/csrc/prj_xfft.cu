@@ -13,6 +13,11 @@
 #include "fft_dif.cuh"
 #include "prj_internal.h"
 
+// minimum resident CTAs per SM requested for the shared-memory FFT kernels
+#ifndef PRJ_FFT_MINB
+#define PRJ_FFT_MINB 4
+#endif
+
 namespace prj {
 
 namespace {
@@ -59,7 +64,7 @@ __device__ __forceinline__ double div_at(const XArgs& a, int i, int j, int k) {
 #define S(g) sidx<true>(g)
 
 template <int SRC>
-__global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
+__global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_fwd_xd(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
     int* pos = reinterpret_cast<int*>(sm + (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2));
@@ -96,8 +101,10 @@ __global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
     if (a.even) {
         // split: X_k = E_k + W^k O_k and X_{m-k} = conj(E_k) + W^{m-k} conj(O_k), in place
         const int half = m / 2;
+        // row index fastest: the rows are rs (odd) slots apart, so a warp's
+        // digit-reversed gathers land in distinct bank groups
         for (int idx = tid; idx < a.tz * (half + 1); idx += nthr) {
-            const int r = idx / (half + 1), k = idx - r * (half + 1);
+            const int k = idx / a.tz, r = idx - k * a.tz;
             const int base = r * a.rs;
             if (k == 0) {
                 const double2 z = A[S(base + pos[0])];
@@ -125,7 +132,7 @@ __global__ void __launch_bounds__(256) k_fwd_xd(const XArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
+__global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
     int* pos = reinterpret_cast<int*>(sm + (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2));
@@ -193,8 +200,9 @@ __global__ void __launch_bounds__(256) k_bwd_xd(const XArgs a) {
     }
     __syncthreads();
     inplace_rows<+1, false, true>(A, a.tz, a.rs, a.f, a.tw);
+    // row index fastest (conflict-free gathers); each warp still writes whole 32-byte sectors
     for (int idx = tid; idx < a.tz * nx; idx += nthr) {
-        const int r = idx / nx, i = idx - r * nx;
+        const int i = idx / a.tz, r = idx - i * a.tz;
         const int z = z0 + r;
         if (z >= a.nz) continue;
         double v;

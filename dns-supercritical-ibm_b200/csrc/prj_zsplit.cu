@@ -17,6 +17,11 @@
 // plan's table (the pair kz, nz-kz shares one pivot row entry).
 #include "prj_internal.h"
 
+// minimum resident CTAs per SM requested for the shared-memory FFT kernels
+#ifndef PRJ_FFT_MINB
+#define PRJ_FFT_MINB 4
+#endif
+
 namespace prj {
 
 namespace {
@@ -30,7 +35,7 @@ struct ZfftArgs {
 };
 
 template <int DIR>
-__global__ void __launch_bounds__(256) k_zfft(const ZfftArgs a) {
+__global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
     extern __shared__ __align__(16) double2 zs[];
     const int tid = threadIdx.x, nthr = blockDim.x;
     const size_t row0 = (size_t)blockIdx.x * a.rb;
@@ -67,7 +72,7 @@ struct ThomasArgs {
 };
 
 constexpr int kThomasTile = 128;
-constexpr int kBlock = 4;  // planes loaded together (independent loads in flight)
+constexpr int kBlock = 8;  // planes loaded together (independent loads in flight)
 
 __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
     const int kx = blockIdx.x / a.tiles;
