@@ -6,6 +6,7 @@
 // rank: FFT plans, the a_x / a_z wavenumber tables (:133-155, computed here in
 // host double precision with the C library's sin, as the reference does on the
 // CPU build), and the Thomas pivot table (the analogue of poi_C, :164-179).
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -181,6 +182,8 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->zd.tw);
     dfree(pl->zd.pos);
     dfree(pl->kz_of_slot);
+    dfree(pl->spec32);
+    dfree(pl->pbar);
     pl->xd.ok = pl->zd.ok = false;
     dfree(pl->spec);
     dfree(pl->stat_buf);
@@ -241,6 +244,103 @@ struct StageTimer {
         pl->rec.push_back(prj::StageRecord{stage, t0, t1});
     }
 };
+
+double env_double(const char* name, double dflt) {
+    const char* v = getenv(name);
+    return (v && *v) ? atof(v) : dflt;
+}
+
+// Mixed-path set-up on first use: FP64 rows are the x-wavenumbers whose lines
+// are badly conditioned, |a_x(kx)| < tau * max_k |b_k| (their condition number
+// exceeds about 1/tau; with FP32 storage their error would not contract under
+// refinement); kx = 0 (the pinned mean mode) is always FP64.
+int ensure_mixed(prj_plan* pl) {
+    if (pl->spec32 || pl->kxs_mixed == pl->g.nxh) return PRJ_OK;
+    const prj::Geometry& g = pl->g;
+    std::vector<double> ax(g.nxh), bands((size_t)6 * g.ny);
+    CK(cudaMemcpy(ax.data(), pl->t.ax, ax.size() * sizeof(double), cudaMemcpyDeviceToHost), "mixed set-up");
+    CK(cudaMemcpy(bands.data(), pl->t.bands, bands.size() * sizeof(double), cudaMemcpyDeviceToHost), "mixed set-up");
+    double bmax = 0.0;
+    for (int k = 0; k < g.ny; k++) bmax = std::max(bmax, std::fabs(bands[(size_t)g.ny + k]));
+    const double tau = env_double("PRJ_MIXED_TAU", 1e-3);
+    int kxs = g.nxh;
+    for (int kx = 1; kx < g.nxh; kx++)
+        if (std::fabs(ax[kx]) >= tau * bmax) { kxs = kx; break; }
+    pl->kxs_mixed = kxs;
+    pl->mixed_iters = (int)env_double("PRJ_MIXED_ITERS", 2);
+    if (pl->mixed_iters < 0) pl->mixed_iters = 0;
+    const size_t n32 = (size_t)(g.nxh - kxs) * g.nz * g.ny;
+    if (n32) {
+        CK(cudaMalloc((void**)&pl->spec32, n32 * sizeof(float2)), "cudaMalloc(FP32 spectrum)");
+        pl->device_bytes += n32 * sizeof(float2);
+    }
+    if (!pl->pbar) {
+        CK(cudaMalloc((void**)&pl->pbar, (size_t)g.ny * sizeof(double)), "cudaMalloc(plane means)");
+        pl->device_bytes += (size_t)g.ny * sizeof(double);
+    }
+    return PRJ_OK;
+}
+
+int run_zsolve_mixed(prj_plan* pl, cudaStream_t st) {
+    {
+        StageTimer tm(pl, prj::kStZfftFwd, st);
+        CK(prj::launch_zfft_mixed(pl, -1, st), "z transform");
+    }
+    {
+        StageTimer tm(pl, prj::kStThomas, st);
+        CK(prj::launch_thomas_mixed(pl, st), "Thomas sweeps");
+    }
+    {
+        StageTimer tm(pl, prj::kStZfftInv, st);
+        CK(prj::launch_zfft_mixed(pl, +1, st), "inverse z transform");
+    }
+    return PRJ_OK;
+}
+
+// FP32-storage solve with FP64 refinement: p = solve(b); repeat mixed_iters times
+// { r = b - A p; p += solve(r) }.  b and r live in the (still unused) output
+// buffers U and V, which the correction overwrites afterwards.
+int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, double* U, double* V,
+                    double* P, const prj::StepScalars& sc, cudaStream_t st) {
+    int rc = ensure_mixed(pl);
+    if (rc) return rc;
+    double* b = U;
+    double* r = V;
+    struct KxsScope {
+        prj_plan* pl;
+        int saved;
+        KxsScope(prj_plan* p) : pl(p), saved(p->kxs) { pl->kxs = pl->kxs_mixed; }
+        ~KxsScope() { pl->kxs = saved; }
+    } scope(pl);
+    {
+        StageTimer tm(pl, prj::kStFwdX, st);
+        CK(prj::launch_fwd_xd(pl, prj::FwdSource::Divergence, nullptr, Uh, Vh, Wh, &sc, st, b), "divergence + forward x");
+    }
+    if ((rc = run_zsolve_mixed(pl, st))) return rc;
+    {
+        StageTimer tm(pl, prj::kStBwdX, st);
+        CK(prj::launch_bwd_xd(pl, P, st, 0, nullptr), "inverse x");
+    }
+    for (int it = 1; it <= pl->mixed_iters; it++) {
+        const bool last = (it == pl->mixed_iters);
+        {
+            StageTimer tm(pl, prj::kStResidual, st);
+            CK(prj::launch_plane_mean(pl, P, pl->pbar, st), "plane means");
+            CK(prj::launch_residual(pl, b, P, pl->pbar, r, st), "residual");
+        }
+        {
+            StageTimer tm(pl, prj::kStFwdX, st);
+            CK(prj::launch_fwd_xd(pl, prj::FwdSource::Pressure, r, nullptr, nullptr, nullptr, nullptr, st), "forward x");
+        }
+        if ((rc = run_zsolve_mixed(pl, st))) return rc;
+        if (last) CK(cudaMemsetAsync(pl->stat_buf + 4, 0, 2 * sizeof(double), st), "norm slots");
+        {
+            StageTimer tm(pl, prj::kStBwdX, st);
+            CK(prj::launch_bwd_xd(pl, P, st, 1, last ? pl->stat_buf + 4 : nullptr), "inverse x");
+        }
+    }
+    return PRJ_OK;
+}
 
 // z transforms + Thomas: three kernels (split) or one fused kernel
 int run_zsolve(prj_plan* pl, cudaStream_t st) {
@@ -429,6 +529,7 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if ((rc = make_dif(nz, &pl->zd, &bytes))) return bail(rc);
     if (pl->zd.ok && (rc = make_slot_table(nz, &pl->kz_of_slot, &bytes))) return bail(rc);
     pl->zmode = z_mode(pl->zd.ok && pl->kz_of_slot);
+    pl->kxs = g.nxh;
     pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);
 
     // rows per CTA of the x kernels: fit two ping-pong buffers in ~100 KB
@@ -564,6 +665,7 @@ const char* prj_stage_name(int stage) {
     case prj::kStZfftFwd: return "k_zfft_fwd";
     case prj::kStThomas: return "k_thomas";
     case prj::kStZfftInv: return "k_zfft_inv";
+    case prj::kStResidual: return "k_residual";
     default: return "";
     }
 }
@@ -586,7 +688,10 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
         return fail(PRJ_ERR_ARG, "NULL array or params");
     if (!(params->dt > 0) || !std::isfinite(params->dt)) return fail(PRJ_ERR_ARG, "dt=%g must be finite and positive", params->dt);
     if (mode != PRJ_MODE_FP64 && mode != PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_ARG, "unknown mode %d", mode);
-    if (mode == PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_UNSUPPORTED, "mixed-precision mode not built yet");
+    if (mode == PRJ_MODE_FP32_REFINE && (plan->zmode != 0 || !plan->xd.ok))
+        return fail(PRJ_ERR_UNSUPPORTED, "the mixed-precision path needs in-place plans for nx/2 and nz (radices 2, 3, 4, 5, 8)");
+    if (d_U == d_Uh || d_V == d_Vh || d_W == d_Wh || d_U == d_Vh || d_U == d_Wh || d_V == d_Uh || d_V == d_Wh)
+        return fail(PRJ_ERR_ARG, "output velocity arrays must not alias the predictor arrays");
     DeviceGuard dg(plan->device);
     cudaStream_t st = (cudaStream_t)stream;
     prj::StepScalars sc{};
@@ -594,17 +699,22 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
     sc.inv_dt = 1.0 / params->dt;
     sc.wall[0] = params->wall_U_bot; sc.wall[1] = params->wall_V_bot; sc.wall[2] = params->wall_W_bot;
     sc.wall[3] = params->wall_U_top; sc.wall[4] = params->wall_V_top; sc.wall[5] = params->wall_W_top;
-    {
-        StageTimer tm(plan, prj::kStFwdX, st);
-        CK(prj::launch_fwd_x(plan, prj::FwdSource::Divergence, nullptr, d_Uh, d_Vh, d_Wh, &sc, st), "divergence + forward x");
-    }
-    {
-        const int rz = run_zsolve(plan, st);
-        if (rz) return rz;
-    }
-    {
-        StageTimer tm(plan, prj::kStBwdX, st);
-        CK(prj::launch_bwd_x(plan, d_P, st), "inverse x");
+    if (mode == PRJ_MODE_FP32_REFINE) {
+        const int rm = run_mixed_solve(plan, d_Uh, d_Vh, d_Wh, d_U, d_V, d_P, sc, st);
+        if (rm) return rm;
+    } else {
+        {
+            StageTimer tm(plan, prj::kStFwdX, st);
+            CK(prj::launch_fwd_x(plan, prj::FwdSource::Divergence, nullptr, d_Uh, d_Vh, d_Wh, &sc, st), "divergence + forward x");
+        }
+        {
+            const int rz = run_zsolve(plan, st);
+            if (rz) return rz;
+        }
+        {
+            StageTimer tm(plan, prj::kStBwdX, st);
+            CK(prj::launch_bwd_x(plan, d_P, st), "inverse x");
+        }
     }
     {
         StageTimer tm(plan, prj::kStCorrect, st);
@@ -625,9 +735,15 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
             stats->div_maxabs = h[0];
             stats->p_maxabs = h[1];
             stats->min_pivot = plan->min_pivot;
-            stats->refine_iters = 0;
-            stats->fp64_lines = plan->g.nxh * plan->g.nz;
-            stats->last_update_rel = 0.0;
+            if (mode == PRJ_MODE_FP32_REFINE) {
+                stats->refine_iters = plan->mixed_iters;
+                stats->fp64_lines = plan->kxs_mixed * plan->g.nz;
+                stats->last_update_rel = (h[3] > 0) ? std::sqrt(h[2] / h[3]) : 0.0;
+            } else {
+                stats->refine_iters = 0;
+                stats->fp64_lines = plan->g.nxh * plan->g.nz;
+                stats->last_update_rel = 0.0;
+            }
         }
         if (!std::isfinite(h[0]) || !std::isfinite(h[1])) return fail(PRJ_ERR_NUMERIC, "NaN detected in the projection");
     }

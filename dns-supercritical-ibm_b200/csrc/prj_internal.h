@@ -67,7 +67,7 @@ namespace prj {
 // stage ids of the per-kernel timing record
 enum Stage {
     kStFwdX = 0, kStZSolve = 1, kStBwdX = 2, kStCorrect = 3, kStStats = 4,
-    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kNumStages = 8
+    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kStResidual = 8, kNumStages = 12
 };
 
 struct StageRecord {
@@ -98,6 +98,11 @@ struct prj_plan {
     prj::DifFft zd;               // in-place transform of length nz (z rows)
     int tz_xd = 1;                // rows per CTA of the in-place x-transform kernels
     int* kz_of_slot = nullptr;    // z wavenumber held by each slot of zd's output
+    int kxs = 0;                  // spectral rows kx < kxs stored in FP64 (nxh on the FP64 path)
+    int kxs_mixed = 0;            // FP64 row count of the mixed path
+    int mixed_iters = 2;          // refinement iterations of the mixed path
+    float2* spec32 = nullptr;     // FP32 spectral rows of the mixed path
+    double* pbar = nullptr;       // per-plane means of P (ny) for the mixed-path residual
     int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
 };
 
@@ -127,14 +132,23 @@ cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, c
 cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStream_t st);
 
 // x transforms with the in-place DIF FFT (prj_xfft.cu); used when pl->xd.ok
+// bout: also store the source field (divergence) there; accum: P += result; sq: norms of
+// the update and of the result (accum only)
 cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
-                          const double* Wh, const StepScalars* sc, cudaStream_t st);
-cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st);
+                          const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout = nullptr);
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum = 0, double* sq = nullptr);
 int choose_tz_xd(int m, bool even);
 
 // z direction as separate kernels (prj_zsplit.cu); need pl->zd.ok and pl->kz_of_slot
 cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st);
 cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st);
+// mixed storage (FP64 rows kx < kxs in spec, FP32 rows in spec32)
+cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st);
+cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st);
+// residual r = b - A p of the pinned operator and the per-plane means it needs (prj_mixed.cu)
+cudaError_t launch_plane_mean(const prj_plan* pl, const double* P, double* pbar, cudaStream_t st);
+cudaError_t launch_residual(const prj_plan* pl, const double* B, const double* P, const double* pbar, double* R,
+                            cudaStream_t st);
 
 // stat_buf slots: [0] min pivot (bits), [2] max|div u|, [3] max|P|, [6] device error word
 constexpr int kStatErrSlot = 6;

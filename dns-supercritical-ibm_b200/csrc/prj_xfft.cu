@@ -40,9 +40,25 @@ struct XArgs {
     const double* Wh;
     const double* inv_dy_p;
     double inv_dx, inv_dz, inv_dt, vbot, vtop, scale;
-    double2* X;
+    double2* X;      // FP64 rows kx < kxs: X[(y kxs + kx) nz + z]
+    float2* X32;     // FP32 rows kx >= kxs: X32[(y (nh - kxs) + kx - kxs) nz + z]
+    int kxs;         // nh on the FP64 path
     double* Pout;
+    double* Bout;    // k_fwd_xd: copy of the source field (P layout), or null
+    int accum;       // k_bwd_xd: Pout += result instead of Pout = result
+    double* sq;      // k_bwd_xd with accum: sq[0] += sum(update^2), sq[1] += sum(result^2), or null
 };
+
+__device__ __forceinline__ void spec_store(const XArgs& a, int y, int kx, int z, double2 v) {
+    if (kx < a.kxs) a.X[((size_t)y * a.kxs + kx) * a.nz + z] = v;
+    else a.X32[((size_t)y * (a.nh - a.kxs) + (kx - a.kxs)) * a.nz + z] = make_float2((float)v.x, (float)v.y);
+}
+
+__device__ __forceinline__ double2 spec_load(const XArgs& a, int y, int kx, int z) {
+    if (kx < a.kxs) return a.X[((size_t)y * a.kxs + kx) * a.nz + z];
+    const float2 f = a.X32[((size_t)y * (a.nh - a.kxs) + (kx - a.kxs)) * a.nz + z];
+    return make_double2(f.x, f.y);
+}
 
 // divergence at cell (i, j, k), mod_cfd_subroutines.f90:532-534 (periodic wrap in x and z,
 // V_hat walls from the step parameters); reference operation order, no contraction
@@ -83,7 +99,10 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_fwd_xd(const XArgs a) {
             if (idx < total) {
                 const int r = idx / nx, i = idx - r * nx;
                 const int z = z0 + r;
-                if (z < a.nz) v[u] = (SRC == 0) ? a.P[((size_t)y * a.nz + z) * nx + i] : div_at(a, i, z, y);
+                if (z < a.nz) {
+                    v[u] = (SRC == 0) ? a.P[((size_t)y * a.nz + z) * nx + i] : div_at(a, i, z, y);
+                    if (a.Bout) a.Bout[((size_t)y * a.nz + z) * nx + i] = v[u];
+                }
             }
         }
 #pragma unroll
@@ -128,7 +147,7 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_fwd_xd(const XArgs a) {
         const int z = z0 + r;
         if (z >= a.nz) continue;
         const int slot = (a.even && kx == m) ? m : pos[kx];
-        a.X[((size_t)y * a.nh + kx) * a.nz + z] = A[S(r * a.rs + slot)];
+        spec_store(a, y, kx, z, A[S(r * a.rs + slot)]);
     }
 }
 
@@ -150,7 +169,7 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
             if (idx < total) {
                 const int kx = idx / a.tz, r = idx - kx * a.tz;
                 const int z = z0 + r;
-                if (z < a.nz) v[u] = a.X[((size_t)y * a.nh + kx) * a.nz + z];
+                if (z < a.nz) v[u] = spec_load(a, y, kx, z);
             }
         }
 #pragma unroll
@@ -200,9 +219,11 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
     }
     __syncthreads();
     inplace_rows<+1, false, true>(A, a.tz, a.rs, a.f, a.tw);
-    // row index fastest (conflict-free gathers); each warp still writes whole 32-byte sectors
+    // x fastest: fully coalesced row stores (measured faster here than conflict-free
+    // row-fastest gathers with sector-sized stores)
+    double sq0 = 0.0, sq1 = 0.0;
     for (int idx = tid; idx < a.tz * nx; idx += nthr) {
-        const int i = idx / a.tz, r = idx - i * a.tz;
+        const int r = idx / nx, i = idx - r * nx;
         const int z = z0 + r;
         if (z >= a.nz) continue;
         double v;
@@ -212,7 +233,25 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
         } else {
             v = A[S(r * a.rs + pos[i])].x;
         }
-        a.Pout[((size_t)y * a.nz + z) * nx + i] = v;
+        double* out = a.Pout + ((size_t)y * a.nz + z) * nx + i;
+        if (a.accum) {
+            const double nv = *out + v;
+            sq0 += v * v;
+            sq1 += nv * nv;
+            *out = nv;
+        } else {
+            *out = v;
+        }
+    }
+    if (a.sq) {
+        for (int o = 16; o > 0; o >>= 1) {
+            sq0 += __shfl_xor_sync(0xffffffffu, sq0, o);
+            sq1 += __shfl_xor_sync(0xffffffffu, sq1, o);
+        }
+        if ((tid & 31) == 0) {
+            atomicAdd(a.sq, sq0);
+            atomicAdd(a.sq + 1, sq1);
+        }
     }
 }
 
@@ -226,6 +265,8 @@ XArgs make_args(const prj_plan* pl) {
     a.f = pl->xd.f; a.tw = pl->xd.tw; a.pos = pl->xd.pos; a.post = pl->fx64.post;
     a.inv_dx = 1.0 / g.dx; a.inv_dz = 1.0 / g.dz;
     a.X = pl->spec;
+    a.X32 = pl->spec32;
+    a.kxs = pl->kxs;
     return a;
 }
 
@@ -250,8 +291,9 @@ int choose_tz_xd(int m, bool even) {
 }
 
 cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
-                          const double* Wh, const StepScalars* sc, cudaStream_t st) {
+                          const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout) {
     XArgs a = make_args(pl);
+    a.Bout = bout;
     a.P = P; a.Uh = Uh; a.Vh = Vh; a.Wh = Wh; a.inv_dy_p = pl->t.inv_dy_p;
     if (sc) { a.inv_dt = sc->inv_dt; a.vbot = sc->wall[1]; a.vtop = sc->wall[4]; }
     const size_t smem = smem_bytes(a);
@@ -267,9 +309,11 @@ cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st) {
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq) {
     XArgs a = make_args(pl);
     a.Pout = P;
+    a.accum = accum;
+    a.sq = sq;
     a.scale = 1.0 / ((double)pl->g.nx * (double)pl->g.nz + 0.0);
     const size_t smem = smem_bytes(a);
     cudaError_t e = allow_smem(k_bwd_xd, smem);

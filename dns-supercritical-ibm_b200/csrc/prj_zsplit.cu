@@ -27,28 +27,34 @@ namespace prj {
 namespace {
 
 struct ZfftArgs {
-    int nrow_total;  // ny * nxh rows of length nz
+    int nrow_total;  // rows of length nz in this buffer (ny * rows per plane)
     int nz, rb;      // rows per CTA
     DifDev f;
     const double2* tw;
-    double2* X;
+    void* X;         // double2 (FP64 storage) or float2 (FP32 storage) rows
 };
 
-template <int DIR>
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
+__device__ __forceinline__ void from_d2(double2& o, double2 v) { o = v; }
+__device__ __forceinline__ void from_d2(float2& o, double2 v) { o = make_float2((float)v.x, (float)v.y); }
+
+// T: storage type of the spectrum rows (arithmetic is FP64 in shared memory)
+template <int DIR, typename T>
 __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
     extern __shared__ __align__(16) double2 zs[];
     const int tid = threadIdx.x, nthr = blockDim.x;
     const size_t row0 = (size_t)blockIdx.x * a.rb;
     const int nr = (int)min((size_t)a.rb, (size_t)a.nrow_total - row0);
     const int tot = nr * a.nz;
-    const double2* src = a.X + row0 * a.nz;
+    const T* src = static_cast<const T*>(a.X) + row0 * a.nz;
     constexpr int U = 4;
     for (int base = tid; base < tot; base += U * nthr) {
         double2 v[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const int i = base + u * nthr;
-            if (i < tot) v[u] = src[i];
+            if (i < tot) v[u] = to_d2(src[i]);
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -59,24 +65,27 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
     __syncthreads();
     if (DIR < 0) inplace_rows<-1, false, true>(zs, nr, a.nz, a.f, a.tw);
     else inplace_rows<+1, true, true>(zs, nr, a.nz, a.f, a.tw);
-    double2* dst = a.X + row0 * a.nz;
-    for (int i = tid; i < tot; i += nthr) dst[i] = zs[sidx<true>(i)];
+    T* dst = static_cast<T*>(a.X) + row0 * a.nz;
+    for (int i = tid; i < tot; i += nthr) from_d2(dst[i], zs[sidx<true>(i)]);
 }
 
 struct ThomasArgs {
     int nz, ny, nh, mzp, tiles;  // tiles of kThomasTile slots per kx
+    int nhb, kx0;                // rows per plane in this buffer; its first kx
     const double* bands;         // a, b, c, a00, b00, c00
-    const double* piv;           // D[y][kx][kzs]
+    const double* piv;           // D[y][kx][kzs], kx over all nh rows
     const int* kz_of_slot;       // wavenumber held by each slot
-    double2* X;
+    void* X;                     // T rows [y][kx - kx0][slot]
 };
 
 constexpr int kThomasTile = 128;
 constexpr int kBlock = 8;  // planes loaded together (independent loads in flight)
 
+template <typename T>
 __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
-    const int kx = blockIdx.x / a.tiles;
-    const int slot = (blockIdx.x - kx * a.tiles) * kThomasTile + threadIdx.x;
+    const int kb = blockIdx.x / a.tiles;  // row within this buffer
+    const int kx = a.kx0 + kb;
+    const int slot = (blockIdx.x - kb * a.tiles) * kThomasTile + threadIdx.x;
     if (slot >= a.nz) return;
     const int nz = a.nz, ny = a.ny, nh = a.nh, mzp = a.mzp;
     const int kz = a.kz_of_slot[slot];
@@ -84,9 +93,9 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
     const bool is00 = (kx == 0 && kz == 0);
     const double* A = a.bands + (is00 ? 3 : 0) * ny;
     const double* C = a.bands + (is00 ? 5 : 2) * ny;
-    const size_t rstride = (size_t)nh * nz;  // X: next y plane
-    const size_t pstride = (size_t)nh * mzp;  // D: next y plane
-    double2* x = a.X + (size_t)kx * nz + slot;
+    const size_t rstride = (size_t)a.nhb * nz;  // X: next y plane
+    const size_t pstride = (size_t)nh * mzp;     // D: next y plane
+    T* x = static_cast<T*>(a.X) + (size_t)kb * nz + slot;
     const double* d = a.piv + (size_t)kx * mzp + kzs;
 
     // forward sweep, y ascending
@@ -98,7 +107,7 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
         for (int u = 0; u < kBlock; u++) {
             const int y = y0 + u;
             if (y < ny) {
-                v[u] = x[(size_t)y * rstride];
+                v[u] = to_d2(x[(size_t)y * rstride]);
                 D[u] = d[(size_t)y * pstride];
                 av[u] = A[y];
             }
@@ -116,12 +125,12 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
                     r.y = __ddiv_rn(__dsub_rn(r.y, __dmul_rn(av[u], prev.y)), D[u]);
                 }
                 prev = r;
-                if (y < ny - 1) x[(size_t)y * rstride] = r;
+                if (y < ny - 1) from_d2(x[(size_t)y * rstride], r);
             }
         }
     }
     // backward sweep, y descending; prev holds d'_{ny-1} = x_{ny-1}
-    x[(size_t)(ny - 1) * rstride] = prev;
+    from_d2(x[(size_t)(ny - 1) * rstride], prev);
     for (int y1 = ny - 2; y1 >= 0; y1 -= kBlock) {
         double2 v[kBlock];
         double D[kBlock], cv[kBlock];
@@ -129,7 +138,7 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
         for (int u = 0; u < kBlock; u++) {
             const int y = y1 - u;
             if (y >= 0) {
-                v[u] = x[(size_t)y * rstride];
+                v[u] = to_d2(x[(size_t)y * rstride]);
                 D[u] = d[(size_t)y * pstride];
                 cv[u] = C[y];
             }
@@ -143,7 +152,7 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
                 r.x = __dsub_rn(v[u].x, __dmul_rn(prev.x, c));
                 r.y = __dsub_rn(v[u].y, __dmul_rn(prev.y, c));
                 prev = r;
-                x[(size_t)y * rstride] = r;
+                from_d2(x[(size_t)y * rstride], r);
             }
         }
     }
@@ -157,44 +166,67 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 }  // namespace
 
-// in-place z FFT of every spectral row: dir < 0 forward (natural -> slot order),
-// dir > 0 inverse (slot order -> natural); needs pl->zd.ok
-cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st) {
+// in-place z FFT of every spectral row of one buffer: dir < 0 forward (natural ->
+// slot order), dir > 0 inverse (slot order -> natural); needs pl->zd.ok.
+// `rows_per_plane` rows of T storage per y plane.
+template <typename T>
+cudaError_t launch_zfft_t(const prj_plan* pl, int dir, void* X, int rows_per_plane, cudaStream_t st) {
     const Geometry& g = pl->g;
     ZfftArgs a{};
-    a.nrow_total = g.ny * g.nxh;
+    a.nrow_total = g.ny * rows_per_plane;
     a.nz = g.nz;
     a.f = pl->zd.f;
     a.tw = pl->zd.tw;
-    a.X = pl->spec;
-    const size_t row = (size_t)g.nz * sizeof(double2);
+    a.X = X;
     int rb = 16;
     while (rb > 1 && (size_t)padded_len(rb * g.nz, true) * sizeof(double2) > 48 * 1024) rb /= 2;
     a.rb = rb;
     const size_t smem = (size_t)padded_len(rb * g.nz, true) * sizeof(double2);
-    (void)row;
     const unsigned grid = (unsigned)((a.nrow_total + rb - 1) / rb);
+    if (grid == 0) return cudaSuccess;
     cudaError_t e;
     if (dir < 0) {
-        if ((e = allow_smem(k_zfft<-1>, smem)) != cudaSuccess) return e;
-        k_zfft<-1><<<grid, 256, smem, st>>>(a);
+        if ((e = allow_smem(k_zfft<-1, T>, smem)) != cudaSuccess) return e;
+        k_zfft<-1, T><<<grid, 256, smem, st>>>(a);
     } else {
-        if ((e = allow_smem(k_zfft<+1>, smem)) != cudaSuccess) return e;
-        k_zfft<+1><<<grid, 256, smem, st>>>(a);
+        if ((e = allow_smem(k_zfft<+1, T>, smem)) != cudaSuccess) return e;
+        k_zfft<+1, T><<<grid, 256, smem, st>>>(a);
     }
     return cudaGetLastError();
 }
 
-
-// Thomas sweeps over y for every (kx, slot) line, in place on the slot-ordered spectrum
-cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st) {
+template <typename T>
+cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_plane, cudaStream_t st) {
     const Geometry& g = pl->g;
+    if (rows_per_plane <= 0) return cudaSuccess;
     ThomasArgs t{};
     t.nz = g.nz; t.ny = g.ny; t.nh = g.nxh; t.mzp = g.mzp;
     t.tiles = (g.nz + kThomasTile - 1) / kThomasTile;
-    t.bands = pl->t.bands; t.piv = pl->t.piv; t.kz_of_slot = pl->kz_of_slot; t.X = pl->spec;
-    k_thomas<<<(unsigned)(g.nxh * t.tiles), kThomasTile, 0, st>>>(t);
+    t.nhb = rows_per_plane; t.kx0 = kx0;
+    t.bands = pl->t.bands; t.piv = pl->t.piv; t.kz_of_slot = pl->kz_of_slot; t.X = X;
+    k_thomas<T><<<(unsigned)(rows_per_plane * t.tiles), kThomasTile, 0, st>>>(t);
     return cudaGetLastError();
+}
+
+cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st) {
+    return launch_zfft_t<double2>(pl, dir, pl->spec, pl->g.nxh, st);
+}
+
+cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st) {
+    return launch_thomas_t<double2>(pl, pl->spec, 0, pl->g.nxh, st);
+}
+
+// mixed storage: FP64 rows kx < kxs in pl->spec (kxs rows per plane), FP32 rows in pl->spec32
+cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st) {
+    cudaError_t e = launch_zfft_t<double2>(pl, dir, pl->spec, pl->kxs, st);
+    if (e != cudaSuccess) return e;
+    return launch_zfft_t<float2>(pl, dir, pl->spec32, pl->g.nxh - pl->kxs, st);
+}
+
+cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st) {
+    cudaError_t e = launch_thomas_t<double2>(pl, pl->spec, 0, pl->kxs, st);
+    if (e != cudaSuccess) return e;
+    return launch_thomas_t<float2>(pl, pl->spec32, pl->kxs, pl->g.nxh - pl->kxs, st);
 }
 
 }  // namespace prj

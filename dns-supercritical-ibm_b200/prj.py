@@ -254,7 +254,7 @@ class Plan:
     def stage_times(self):
         """{kernel name: (total ms, launches)} recorded since the last call (synchronises)."""
         L = load_library()
-        n = 8
+        n = 12
         ms = (ctypes.c_double * n)()
         cnt = (ctypes.c_int * n)()
         ns = ctypes.c_int()

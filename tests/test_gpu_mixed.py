@@ -1,0 +1,70 @@
+"""GPU tests of the mixed-precision projection (FP32 spectral storage with FP64
+iterative refinement, PRJ_MODE_FP32_REFINE) against the FP64 path and the oracle.
+
+Tolerance: pressure within 1e-11 relative L2 of the FP64 result, and, with the
+divergence-consistent bands, max|div u| <= 1e-10.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gpu_util import empty_like_dev, from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+TOL_MIXED = 1e-11
+
+
+def run(plan, Uh, Vh, Wh, dt, mode):
+    import torch
+    g = plan.grid
+    hs = (g.nx + 2, g.nz + 2, g.ny + 2)
+    dU, dV, dW = (empty_like_dev(hs) for _ in range(3))
+    dP = empty_like_dev((g.nx, g.nz, g.ny))
+    st = plan.projection_step(to_dev(Uh), to_dev(Vh), to_dev(Wh), dU, dV, dW, dP, dt, mode=mode)
+    torch.cuda.synchronize()
+    return from_dev(dU), from_dev(dV), from_dev(dW), from_dev(dP), st
+
+
+@pytest.mark.parametrize("band_mode", ["consistent", "reference"])
+@pytest.mark.parametrize("shape", [(64, 48, 32), (128, 96, 64), (96, 40, 60)])
+def test_mixed_matches_fp64(cuda_device, oracle, band_mode, shape):
+    import prj
+    import workloads
+    nx, ny, nz = shape
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=3)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, band_mode) as plan:
+        U64, V64, W64, P64, s64 = run(plan, Uh, Vh, Wh, 0.8, prj.MODE_FP64)
+        U32, V32, W32, P32, s32 = run(plan, Uh, Vh, Wh, 0.8, prj.MODE_FP32_REFINE)
+    assert s32["refine_iters"] >= 1 and s32["fp64_lines"] > 0
+    assert rel_l2(P32, P64) <= TOL_MIXED, rel_l2(P32, P64)
+    Uo, Vo, Wo, Po = oracle.projection(Uh, Vh, Wh, dx, dz, 0.8, yu, band_mode)
+    assert rel_l2(P32, Po) <= TOL_MIXED
+    for a, b in ((U32, U64), (V32, V64), (W32, W64)):
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
+    if band_mode == "consistent":
+        assert s32["div_maxabs"] <= 1e-10
+
+
+def test_mixed_full_size(cuda_device):
+    """768 x 384 x 384 channel step: mixed vs FP64 pressure and solenoidality."""
+    import prj
+    import workloads
+    nx, ny, nz = 768, 384, 384
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=1)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        _, _, _, P64, s64 = run(plan, Uh, Vh, Wh, 1.0, prj.MODE_FP64)
+        _, _, _, P32, s32 = run(plan, Uh, Vh, Wh, 1.0, prj.MODE_FP32_REFINE)
+    assert rel_l2(P32, P64) <= TOL_MIXED, rel_l2(P32, P64)
+    assert s32["div_maxabs"] <= 1e-10, s32
+
+
+def test_mixed_rejects_unsupported_lengths(cuda_device):
+    import prj
+    import workloads
+    nx, ny, nz = 14, 6, 7  # nx/2 = 7: no in-place plan
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu) as plan:
+        with pytest.raises(prj.PrjError) as e:
+            run(plan, Uh, Vh, Wh, 1.0, prj.MODE_FP32_REFINE)
+        assert e.value.code == prj.PRJ_ERR_UNSUPPORTED
