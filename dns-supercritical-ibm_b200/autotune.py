@@ -1,0 +1,97 @@
+"""Launch-shape autotuner of the pressure-Poisson engine.
+
+For one grid size it times candidate tunings of a plan -- x-rows per CTA of the
+x transforms, spectral rows per CTA of the z transforms, and split versus fused
+z kernels (prj_tuning, include/projection.h) -- on an in-place FP64 solve with
+CUDA events, keeps the fastest, and caches it in a JSON file keyed by grid size
+and device name (PRJ_AUTOTUNE_CACHE, default ~/.cache/prj_b200/autotune.json).
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import prj
+
+CACHE = os.environ.get("PRJ_AUTOTUNE_CACHE",
+                       os.path.join(os.path.expanduser("~"), ".cache", "prj_b200", "autotune.json"))
+
+
+def _load_cache():
+    try:
+        with open(CACHE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save_cache(d):
+    try:
+        os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+        tmp = CACHE + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, CACHE)
+    except OSError:
+        pass
+
+
+def key(plan) -> str:
+    import torch
+    g = plan.grid
+    return f"{g.nx}x{g.nz}x{g.ny}:{torch.cuda.get_device_name(plan.device)}"
+
+
+def candidates(plan):
+    out = []
+    for z_mode in (0, 1):
+        for x_rows in (2, 4, 8, 16):
+            for z_rows in ((0, 4, 8, 16) if z_mode == 0 else (0,)):
+                out.append(dict(x_rows=x_rows, z_rows=z_rows, z_mode=z_mode))
+    return out
+
+
+def time_solve(plan, P, reps):
+    import torch
+    s = torch.cuda.current_stream(plan.device)
+    plan.poisson_fp64(P, stream=s)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        plan.poisson_fp64(P, stream=s)
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune(plan, reps: int = 5, use_cache: bool = True) -> dict:
+    """Apply the fastest tuning for this plan's grid (cached) and return it with its time."""
+    import torch
+    k = key(plan)
+    cache = _load_cache() if use_cache else {}
+    if k in cache:
+        t = cache[k]
+        plan.set_tuning(t["x_rows"], t["z_rows"], t["z_mode"])
+        return dict(t, cached=True)
+    g = plan.grid
+    P = torch.randn((g.ny, g.nz, g.nx), dtype=torch.float64, device=f"cuda:{plan.device}")
+    best = None
+    default = plan.tuning
+    for c in candidates(plan):
+        try:
+            plan.set_tuning(c["x_rows"], c["z_rows"], c["z_mode"])
+        except prj.PrjError:
+            continue
+        ms = time_solve(plan, P, reps)
+        if best is None or ms < best["ms"]:
+            best = dict(c, ms=ms)
+    if best is None:
+        plan.set_tuning(default["x_rows"], default["z_rows"], default["z_mode"])
+        return dict(default, ms=None, cached=False)
+    plan.set_tuning(best["x_rows"], best["z_rows"], best["z_mode"])
+    if use_cache:
+        cache = _load_cache()
+        cache[k] = best
+        _save_cache(cache)
+    return dict(best, cached=False)

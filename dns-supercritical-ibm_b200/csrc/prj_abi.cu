@@ -184,6 +184,8 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->kz_of_slot);
     dfree(pl->spec32);
     dfree(pl->pbar);
+    dfree(pl->mix_b);
+    dfree(pl->mix_r);
     pl->xd.ok = pl->zd.ok = false;
     dfree(pl->spec);
     dfree(pl->stat_buf);
@@ -298,14 +300,13 @@ int run_zsolve_mixed(prj_plan* pl, cudaStream_t st) {
 }
 
 // FP32-storage solve with FP64 refinement: p = solve(b); repeat mixed_iters times
-// { r = b - A p; p += solve(r) }.  b and r live in the (still unused) output
-// buffers U and V, which the correction overwrites afterwards.
-int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, double* U, double* V,
-                    double* P, const prj::StepScalars& sc, cudaStream_t st) {
+// { r = b - A p; p += solve(r) }.  The right-hand side is the divergence of
+// (Uh, Vh, Wh) when Uh is given, else the incoming P.  b and r are scratch fields
+// of nx nz ny doubles (the projection passes its still unused outputs U and V).
+int run_mixed_core(prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, const prj::StepScalars* sc,
+                   double* b, double* r, double* P, cudaStream_t st) {
     int rc = ensure_mixed(pl);
     if (rc) return rc;
-    double* b = U;
-    double* r = V;
     struct KxsScope {
         prj_plan* pl;
         int saved;
@@ -314,7 +315,10 @@ int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const doub
     } scope(pl);
     {
         StageTimer tm(pl, prj::kStFwdX, st);
-        CK(prj::launch_fwd_xd(pl, prj::FwdSource::Divergence, nullptr, Uh, Vh, Wh, &sc, st, b), "divergence + forward x");
+        if (Uh)
+            CK(prj::launch_fwd_xd(pl, prj::FwdSource::Divergence, nullptr, Uh, Vh, Wh, sc, st, b), "divergence + forward x");
+        else
+            CK(prj::launch_fwd_xd(pl, prj::FwdSource::Pressure, P, nullptr, nullptr, nullptr, nullptr, st, b), "forward x");
     }
     if ((rc = run_zsolve_mixed(pl, st))) return rc;
     {
@@ -340,6 +344,33 @@ int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const doub
         }
     }
     return PRJ_OK;
+}
+
+int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, double* U, double* V,
+                    double* P, const prj::StepScalars& sc, cudaStream_t st) {
+    return run_mixed_core(pl, Uh, Vh, Wh, &sc, U, V, P, st);
+}
+
+int mixed_supported(const prj_plan* pl) {
+    if (pl->zmode != 0 || !pl->xd.ok)
+        return fail(PRJ_ERR_UNSUPPORTED, "the mixed-precision path needs in-place plans for nx/2 and nz (radices 2, 3, 4, 5, 8)");
+    return PRJ_OK;
+}
+
+// Poisson-only mixed solve: plan-owned scratch for b and r
+int run_mixed_poisson(prj_plan* pl, double* P, cudaStream_t st) {
+    int rc = mixed_supported(pl);
+    if (rc) return rc;
+    const size_t n = (size_t)pl->g.nx * pl->g.nz * pl->g.ny;
+    if (!pl->mix_b) {
+        CK(cudaMalloc((void**)&pl->mix_b, n * sizeof(double)), "cudaMalloc(mixed scratch)");
+        pl->device_bytes += n * sizeof(double);
+    }
+    if (!pl->mix_r) {
+        CK(cudaMalloc((void**)&pl->mix_r, n * sizeof(double)), "cudaMalloc(mixed scratch)");
+        pl->device_bytes += n * sizeof(double);
+    }
+    return run_mixed_core(pl, nullptr, nullptr, nullptr, nullptr, pl->mix_b, pl->mix_r, P, st);
 }
 
 // z transforms + Thomas: three kernels (split) or one fused kernel
@@ -399,6 +430,25 @@ int ensure_host_stage(prj_plan* pl, size_t elems) {
     return PRJ_OK;
 }
 
+// A captured batch: one CUDA graph, one branch (own stream during capture) per case.
+struct BatchImpl {
+    int device = 0;
+    int ncases = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace
+
+struct prj_batch : BatchImpl {};
+
+namespace {
+void batch_release(prj_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
 }  // namespace
 
 int prj::record_error(int code, const char* msg) {
@@ -688,8 +738,7 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
         return fail(PRJ_ERR_ARG, "NULL array or params");
     if (!(params->dt > 0) || !std::isfinite(params->dt)) return fail(PRJ_ERR_ARG, "dt=%g must be finite and positive", params->dt);
     if (mode != PRJ_MODE_FP64 && mode != PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_ARG, "unknown mode %d", mode);
-    if (mode == PRJ_MODE_FP32_REFINE && (plan->zmode != 0 || !plan->xd.ok))
-        return fail(PRJ_ERR_UNSUPPORTED, "the mixed-precision path needs in-place plans for nx/2 and nz (radices 2, 3, 4, 5, 8)");
+    if (mode == PRJ_MODE_FP32_REFINE && (rc = mixed_supported(plan))) return rc;
     if (d_U == d_Uh || d_V == d_Vh || d_W == d_Wh || d_U == d_Vh || d_U == d_Wh || d_V == d_Uh || d_V == d_Wh)
         return fail(PRJ_ERR_ARG, "output velocity arrays must not alias the predictor arrays");
     DeviceGuard dg(plan->device);
@@ -786,6 +835,137 @@ int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h
     CK(cudaMemcpy(h_V, dV, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy V");
     CK(cudaMemcpy(h_W, dW, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy W");
     CK(cudaMemcpy(h_P, dP, np * sizeof(double), cudaMemcpyDeviceToHost), "copy P");
+    return PRJ_OK;
+}
+
+int prj_poisson_mixed(prj_plan* plan, double* d_P, void* stream) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!d_P) return fail(PRJ_ERR_ARG, "P is NULL");
+    DeviceGuard dg(plan->device);
+    return run_mixed_poisson(plan, d_P, (cudaStream_t)stream);
+}
+
+int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out) {
+    if (!plan || !out) return fail(PRJ_ERR_ARG, "NULL argument");
+    out->x_rows = plan->tz_xd;
+    out->z_rows = plan->zfft_rows;
+    out->z_mode = plan->zmode;
+    return PRJ_OK;
+}
+
+int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!t) return fail(PRJ_ERR_ARG, "NULL tuning");
+    auto pow2 = [](int v) { return v >= 1 && v <= 16 && (v & (v - 1)) == 0; };
+    if (!pow2(t->x_rows)) return fail(PRJ_ERR_ARG, "x_rows=%d must be a power of two in [1, 16]", t->x_rows);
+    if (t->z_rows != 0 && !pow2(t->z_rows)) return fail(PRJ_ERR_ARG, "z_rows=%d must be 0 or a power of two in [1, 16]", t->z_rows);
+    if (t->z_mode != 0 && t->z_mode != 1) return fail(PRJ_ERR_ARG, "z_mode=%d must be 0 or 1", t->z_mode);
+    if (t->z_mode == 0 && !(plan->zd.ok && plan->kz_of_slot)) return fail(PRJ_ERR_UNSUPPORTED, "no in-place z plan for nz=%d", plan->g.nz);
+    const int rs = plan->fx64.even ? plan->fx64.m + 1 : plan->fx64.m;
+    if ((size_t)prj::padded_len(t->x_rows * rs, true) * sizeof(double2) + (size_t)plan->fx64.m * sizeof(int) > 200 * 1024)
+        return fail(PRJ_ERR_ARG, "x_rows=%d does not fit shared memory for nx=%d", t->x_rows, plan->g.nx);
+    if (t->z_rows && (size_t)prj::padded_len(t->z_rows * plan->g.nz, true) * sizeof(double2) > 200 * 1024)
+        return fail(PRJ_ERR_ARG, "z_rows=%d does not fit shared memory for nz=%d", t->z_rows, plan->g.nz);
+    plan->tz_xd = t->x_rows;
+    plan->zfft_rows = t->z_rows;
+    plan->zmode = t->z_mode;
+    return PRJ_OK;
+}
+
+int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int mode, prj_batch** out) {
+    if (!out) return fail(PRJ_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!plans || !d_P || ncases < 1) return fail(PRJ_ERR_ARG, "need ncases >= 1 plans and arrays");
+    if (mode != PRJ_MODE_FP64 && mode != PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_ARG, "unknown mode %d", mode);
+    const int dev = plans[0] ? plans[0]->device : 0;
+    for (int i = 0; i < ncases; i++) {
+        int rc = check_plan(plans[i]);
+        if (rc) return rc;
+        if (!d_P[i]) return fail(PRJ_ERR_ARG, "array %d is NULL", i);
+        if (plans[i]->device != dev) return fail(PRJ_ERR_ARG, "plans on different devices");
+        for (int j = 0; j < i; j++)
+            if (plans[j] == plans[i]) return fail(PRJ_ERR_ARG, "plan %d appears twice (a plan serves one solve at a time)", i);
+        if (mode == PRJ_MODE_FP32_REFINE && (rc = mixed_supported(plans[i]))) return rc;
+    }
+    DeviceGuard dg(dev);
+    // eager pass: lazy buffers, kernel attributes, and a check that every case runs
+    std::vector<cudaStream_t> streams((size_t)ncases, nullptr);
+    std::vector<cudaEvent_t> joins((size_t)ncases, nullptr);
+    cudaStream_t s0 = nullptr;
+    cudaEvent_t fork = nullptr;
+    auto cleanup = [&]() {
+        for (auto s_ : streams) if (s_) cudaStreamDestroy(s_);
+        for (auto e_ : joins) if (e_) cudaEventDestroy(e_);
+        if (fork) cudaEventDestroy(fork);
+        if (s0) cudaStreamDestroy(s0);
+    };
+    auto bail = [&](int code) { cleanup(); return code; };
+    int rc = PRJ_OK;
+    std::vector<bool> timing((size_t)ncases);
+    for (int i = 0; i < ncases; i++) {
+        timing[i] = plans[i]->timing;
+        plans[i]->timing = false;
+        rc = (mode == PRJ_MODE_FP64) ? run_poisson(plans[i], d_P[i], 0) : run_mixed_poisson(plans[i], d_P[i], 0);
+        if (rc) break;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "batch warm-up");
+    if (rc) {
+        for (int i = 0; i < ncases; i++) plans[i]->timing = timing[i];
+        return bail(rc);
+    }
+    prj_batch* b = new prj_batch();
+    b->device = dev;
+    b->ncases = ncases;
+    e = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    for (int i = 0; i < ncases && e == cudaSuccess; i++) {
+        e = cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+    bool capturing = (e == cudaSuccess);
+    if (e == cudaSuccess) e = cudaEventRecord(fork, s0);
+    for (int i = 0; i < ncases && e == cudaSuccess && !rc; i++) {
+        e = cudaStreamWaitEvent(streams[i], fork, 0);
+        if (e != cudaSuccess) break;
+        rc = (mode == PRJ_MODE_FP64) ? run_poisson(plans[i], d_P[i], streams[i])
+                                     : run_mixed_poisson(plans[i], d_P[i], streams[i]);
+        if (rc) break;
+        e = cudaEventRecord(joins[i], streams[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, joins[i], 0);
+    }
+    if (capturing) {
+        cudaError_t e2 = cudaStreamEndCapture(s0, &b->graph);
+        if (e == cudaSuccess) e = e2;
+    }
+    for (int i = 0; i < ncases; i++) plans[i]->timing = timing[i];
+    if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (rc || e != cudaSuccess) {
+        if (!rc) rc = cuda_fail(e, "batch graph capture");
+        batch_release(b);
+        delete b;
+        return bail(rc);
+    }
+    cleanup();
+    *out = b;
+    return PRJ_OK;
+}
+
+int prj_batch_launch(prj_batch* batch, void* stream) {
+    if (!batch || !batch->exec) return fail(PRJ_ERR_ARG, "batch is NULL or empty");
+    DeviceGuard dg(batch->device);
+    CK(cudaGraphLaunch(batch->exec, (cudaStream_t)stream), "batch graph launch");
+    return PRJ_OK;
+}
+
+int prj_batch_destroy(prj_batch* batch) {
+    if (!batch) return PRJ_OK;
+    DeviceGuard dg(batch->device);
+    batch_release(batch);
+    delete batch;
     return PRJ_OK;
 }
 

@@ -103,6 +103,9 @@ struct prj_plan {
     int mixed_iters = 2;          // refinement iterations of the mixed path
     float2* spec32 = nullptr;     // FP32 spectral rows of the mixed path
     double* pbar = nullptr;       // per-plane means of P (ny) for the mixed-path residual
+    double* mix_b = nullptr;      // Poisson-only mixed solve: copy of the right-hand side
+    double* mix_r = nullptr;      // Poisson-only mixed solve: residual
+    int zfft_rows = 0;            // rows per CTA of the z-transform kernels (0: default rule)
     int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
 };
 

@@ -178,8 +178,9 @@ cudaError_t launch_zfft_t(const prj_plan* pl, int dir, void* X, int rows_per_pla
     a.f = pl->zd.f;
     a.tw = pl->zd.tw;
     a.X = X;
-    int rb = 16;
-    while (rb > 1 && (size_t)padded_len(rb * g.nz, true) * sizeof(double2) > 48 * 1024) rb /= 2;
+    int rb = pl->zfft_rows > 0 ? pl->zfft_rows : 16;
+    const size_t limit = pl->zfft_rows > 0 ? (size_t)200 * 1024 : (size_t)48 * 1024;
+    while (rb > 1 && (size_t)padded_len(rb * g.nz, true) * sizeof(double2) > limit) rb /= 2;
     a.rb = rb;
     const size_t smem = (size_t)padded_len(rb * g.nz, true) * sizeof(double2);
     const unsigned grid = (unsigned)((a.nrow_total + rb - 1) / rb);

@@ -49,7 +49,9 @@ EXPORTS = (
     "prj_plan_device_bytes", "prj_last_error_string", "prj_version",
     "prj_bands_from_yu", "prj_metrics_from_yu",
     "prj_plan_enable_stage_timing", "prj_plan_stage_times", "prj_stage_name",
-    "prj_poisson_fp64_noalloc",
+    "prj_poisson_fp64_noalloc", "prj_poisson_mixed",
+    "prj_batch_create", "prj_batch_launch", "prj_batch_destroy",
+    "prj_plan_get_tuning", "prj_plan_set_tuning",
 )
 
 BANDS_REFERENCE = 0
@@ -66,6 +68,13 @@ class Stats(ctypes.Structure):
     _fields_ = [("div_maxabs", ctypes.c_double), ("p_maxabs", ctypes.c_double),
                 ("min_pivot", ctypes.c_double), ("refine_iters", ctypes.c_int),
                 ("fp64_lines", ctypes.c_int), ("last_update_rel", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("x_rows", ctypes.c_int), ("z_rows", ctypes.c_int), ("z_mode", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -116,6 +125,12 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_stage_times.argtypes = [_vp, _dp, ctypes.POINTER(ctypes.c_int), i, ctypes.POINTER(ctypes.c_int)]
     L.prj_stage_name.argtypes = [i]
     L.prj_poisson_fp64_noalloc.argtypes = [i, i, i, d, d, _dp, _dp, _dp, _dp, _dp, _dp, _vp, _vp]
+    L.prj_poisson_mixed.argtypes = [_vp, _vp, _vp]
+    L.prj_batch_create.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(_vp), i, i, ctypes.POINTER(_vp)]
+    L.prj_batch_launch.argtypes = [_vp, _vp]
+    L.prj_batch_destroy.argtypes = [_vp]
+    L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
+    L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.prj_last_error_string.restype = ctypes.c_char_p
@@ -261,7 +276,26 @@ class Plan:
         _check(L.prj_plan_stage_times(self.handle, ms, cnt, n, ctypes.byref(ns)))
         return {L.prj_stage_name(i).decode(): (ms[i], cnt[i]) for i in range(ns.value) if cnt[i]}
 
+    @property
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(load_library().prj_plan_get_tuning(self.handle, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, x_rows, z_rows=0, z_mode=0):
+        _check(load_library().prj_plan_set_tuning(self.handle, ctypes.byref(Tuning(x_rows, z_rows, z_mode))))
+
     # ---------------------------------------------------------------- solve
+    def poisson_mixed(self, P, stream=None):
+        """In-place Poisson solve with FP32 spectral storage and FP64 refinement (torch CUDA tensor)."""
+        g = self.grid
+        torch = _torch()
+        if not (_is_tensor(P) and P.is_cuda and P.dtype == torch.float64 and P.is_contiguous()
+                and tuple(P.shape) == (g.ny, g.nz, g.nx)):
+            raise ValueError("P must be a contiguous float64 CUDA tensor of shape (ny, nz, nx)")
+        _check(load_library().prj_poisson_mixed(self.handle, ctypes.c_void_p(P.data_ptr()), _stream_ptr(stream)))
+        return P
+
     def poisson_fp64(self, P, stream=None):
         """In-place FP64 solve.  torch CUDA tensor [y, z, x] (async) or numpy [x, z, y] F-order (sync)."""
         g = self.grid
@@ -306,6 +340,43 @@ class Plan:
             _check(L.prj_projection_step_host(self.handle, _p(Uh), _p(Vh), _p(Wh), _p(U), _p(V), _p(W), _p(P),
                                               ctypes.byref(par), mode, sp))
         return st.as_dict() if stats else None
+
+
+class Batch:
+    """Many independent in-place Poisson solves replayed as one CUDA graph launch
+    (prj_batch_create / prj_batch_launch).  Case i solves plans[i] on tensors[i]."""
+
+    def __init__(self, plans, tensors, mode=MODE_FP64):
+        if len(plans) != len(tensors) or not plans:
+            raise ValueError("need one tensor per plan")
+        L = load_library()
+        n = len(plans)
+        hp = (_vp * n)(*[p.handle for p in plans])
+        hd = (_vp * n)(*[ctypes.c_void_p(t.data_ptr()) for t in tensors])
+        h = _vp()
+        _check(L.prj_batch_create(hp, hd, n, mode, ctypes.byref(h)))
+        self._h = h
+        self._keep = (list(plans), list(tensors))  # the graph holds their addresses
+
+    def launch(self, stream=None):
+        _check(load_library().prj_batch_launch(self._h, _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().prj_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ------------------------------------------------------------------------------

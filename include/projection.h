@@ -126,6 +126,45 @@ int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h
                              double* h_U, double* h_V, double* h_W, double* h_P,
                              const prj_step_params* params, int mode, prj_stats* stats);
 
+/*
+ * Poisson solve in place with FP32 spectral storage and FP64 iterative
+ * refinement (the precision scheme of PRJ_MODE_FP32_REFINE): rows of
+ * x-wavenumbers whose tridiagonals are badly conditioned stay FP64, the
+ * residual b - A p of the pinned operator is formed in FP64.  Needs in-place
+ * transform plans (radices 2, 3, 4, 5, 8 for nx/2 and nz).  Asynchronous.
+ */
+int prj_poisson_mixed(prj_plan* plan, double* d_P, void* stream);
+
+/*
+ * Batched solves: one CUDA graph holding every case (case i solves plans[i] in
+ * place on the device array d_P[i], FP64 or PRJ_MODE_FP32_REFINE), the cases
+ * on parallel graph branches, replayed by one graph launch.  The plans must be
+ * distinct (a plan's scratch serves one solve at a time) and outlive the batch;
+ * the arrays are bound at creation.  No counterpart in the reference, which
+ * solves one grid per run.
+ */
+typedef struct prj_batch prj_batch;
+int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int mode, prj_batch** out);
+int prj_batch_launch(prj_batch* batch, void* stream);
+int prj_batch_destroy(prj_batch* batch);
+
+/*
+ * Launch-shape tuning of a plan (read by the autotuner, which times
+ * candidates and caches the winner per grid size):
+ *   x_rows  x-rows per CTA of the x-transform kernels (power of two, 1..16);
+ *   z_rows  spectral rows per CTA of the z-transform kernels (power of two, 1..16);
+ *   z_mode  0 = z FFT / Thomas / inverse z FFT as three kernels, 1 = one fused
+ *           pipelined kernel per x-wavenumber.
+ * prj_plan_set_tuning rejects shapes that do not fit shared memory.
+ */
+typedef struct prj_tuning {
+    int x_rows;
+    int z_rows;
+    int z_mode;
+} prj_tuning;
+int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out);
+int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
+
 /* band modes of prj_bands_from_yu */
 #define PRJ_BANDS_REFERENCE 0   /* the reference's mk_P_abc bands */
 #define PRJ_BANDS_CONSISTENT 1  /* bands of div(grad p) with the divergence/correction metrics */
