@@ -207,6 +207,105 @@ def cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz):
             "sample": f"one full {NX}x{NY}x{NZ} projection step ({dt:.2f} s)"}
 
 
+# ----------------------------------------------------------------------------- extra legs
+def timed_steps(fn, stream, steps):
+    """Sum of CUDA-event durations of `steps` calls of fn() on `stream`."""
+    import torch
+    total = 0.0
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total
+
+
+def run_batched(device, steps, warmup):
+    """64 independent Poisson solves of uneven sizes in one CUDA graph launch: sizes from
+    default_rng(2) (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]),
+    uniform[-1,1] right-hand sides minus their dy-weighted mean; launch shapes from the
+    autotuner.  FP64 and FP32-storage + FP64-refinement graphs."""
+    import numpy as np
+    import torch
+    import autotune
+    import prj
+    import workloads
+    rng = np.random.default_rng(2)
+    specs = []
+    for _ in range(64):
+        nx, nz = (int(v) for v in rng.choice([64, 96, 128, 192, 256], 2))
+        ny = int(rng.choice([48, 64, 96, 128]))
+        specs.append((nx, ny, nz, float(rng.uniform(1.5, 2.5))))
+    plans, rhs = [], []
+    t_tune = time.perf_counter()
+    tuned = {}
+    for i, (nx, ny, nz, beta) in enumerate(specs):
+        yu = workloads.tanh_faces(ny, beta)
+        dx, dz = workloads.channel_spacing(nx, nz)
+        p = prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent"), device=device.index or 0)
+        if (nx, ny, nz) in tuned:
+            p.set_tuning(**tuned[(nx, ny, nz)])
+        else:
+            best = autotune.tune(p, reps=3)
+            tuned[(nx, ny, nz)] = {k: best[k] for k in ("x_rows", "z_rows", "z_mode")}
+        plans.append(p)
+        g = torch.Generator(device=device)
+        g.manual_seed(1000 + i)
+        r = torch.rand((ny, nz, nx), generator=g, dtype=torch.float64, device=device) * 2 - 1
+        w = torch.tensor(np.diff(yu), dtype=torch.float64, device=device).view(-1, 1, 1)
+        r -= (r * w).sum() / (w.sum() * nx * nz)
+        rhs.append(r)
+    t_tune = time.perf_counter() - t_tune
+    pts = sum(nx * ny * nz for nx, ny, nz, _ in specs)
+    out = {"cases": 64, "points": pts, "distinct_sizes": len(tuned), "setup_s": t_tune}
+    stream = torch.cuda.current_stream(device)
+    for name, mode in (("fp64", prj.MODE_FP64), ("mixed", prj.MODE_FP32_REFINE)):
+        if mode == prj.MODE_FP32_REFINE:  # the mixed path runs the split z kernels
+            for p in plans:
+                t = p.tuning
+                if t["z_mode"] != 0:
+                    p.set_tuning(t["x_rows"], 0, 0)
+        work = [r.clone() for r in rhs]
+        with prj.Batch(plans, work, mode=mode) as batch:
+            def reset():
+                for w_, r_ in zip(work, rhs):
+                    w_.copy_(r_)
+            for _ in range(warmup):
+                reset()
+                batch.launch(stream)
+            torch.cuda.synchronize()
+            total = 0.0
+            for _ in range(steps):
+                reset()
+                total += timed_steps(lambda: batch.launch(stream), stream, 1)
+            out[name] = {"gpts_per_s": pts * steps / (total / 1e3) / 1e9, "ms_per_batch": total / steps,
+                         "graph_launches": steps}
+    for p in plans:
+        p.close()
+    return out
+
+
+def run_served(device, seconds, rate, budget):
+    """Open-loop Poisson arrivals (rate per second, default_rng(3)) of projection requests of
+    sizes (128,96,64)/(256,128,128)/(384,192,192)/(768,384,384) with p = 0.4/0.3/0.2/0.1."""
+    import serve
+    arrivals = serve.poisson_arrivals(rate, seconds, seed=3)
+    srv = serve.ProjectionServer(device=device.index or 0, hbm_budget=budget)
+    t0 = time.perf_counter()
+    done = srv.run(arrivals)
+    wall = time.perf_counter() - t0
+    out = serve.summarize(done, seconds)
+    offered = sum(a * b * c for _, (a, b, c) in arrivals) / seconds / 1e9
+    out.update({"rate_hz": rate, "offered_gpts_per_s": offered, "wall_s": wall,
+                "max_inflight": srv.max_inflight, "peak_resident_gb": srv.peak_used / 1e9,
+                "sustained": bool(out["drain_s"] is not None and out["drain_s"] < 0.05 * seconds)})
+    srv.close()
+    return out
+
+
 def main():
     global NX, NY, NZ
     ap = argparse.ArgumentParser()
@@ -218,6 +317,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3, help="0 skips the end-to-end leg")
     ap.add_argument("--grid", default=f"{NX}x{NY}x{NZ}", help="nx x ny x nz (profiling of smaller cases)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the mixed, batched and served legs")
+    ap.add_argument("--served-seconds", type=float, default=30.0)
+    ap.add_argument("--served-rate", type=float, default=2000.0)
+    ap.add_argument("--served-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -330,6 +433,32 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz)
 
+    extra = {}
+    if not args.no_extra:
+        # FP32 spectral storage + FP64 refinement on the same step
+        other = prj.MODE_FP32_REFINE if mode == prj.MODE_FP64 else prj.MODE_FP64
+        P_main = P.clone()
+        for _ in range(args.warmup):
+            plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=other, stats=False, stream=stream)
+        ms_other = timed_steps(lambda: plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=other, stats=False,
+                                                            stream=stream), stream, max(3, args.steps // 4))
+        st_o = plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=other, stats=True, stream=stream)
+        rel = float(torch.linalg.vector_norm(P - P_main) / torch.linalg.vector_norm(P_main))
+        nsteps_o = max(3, args.steps // 4)
+        extra["other_precision"] = {
+            "mode": "mixed" if other == prj.MODE_FP32_REFINE else "fp64",
+            "gpts_per_s": world * NX * NY * NZ * nsteps_o / (ms_other / 1e3) / 1e9, "ms_per_step": ms_other / nsteps_o,
+            "p_rel_l2_vs_this_mode": rel, "div_maxabs": st_o["div_maxabs"], "refine_iters": st_o["refine_iters"],
+            "fp64_lines": st_o["fp64_lines"], "last_update_rel": st_o["last_update_rel"]}
+        del P_main
+    plan.close()
+    del Uh, Vh, Wh, U, V, W, P
+    torch.cuda.empty_cache()
+    if not args.no_extra and world == 1:
+        extra["batched"] = run_batched(device, steps=max(3, args.steps // 4), warmup=args.warmup)
+        torch.cuda.empty_cache()
+        extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
@@ -352,8 +481,8 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
-    plan.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
