@@ -288,6 +288,85 @@ def run_batched(device, steps, warmup):
     return out
 
 
+def fluid_div_maxabs(U, V, W, solid, inv_dy_p, dx, dz, vbot=0.0, vtop=0.0):
+    """max |div u| over the fluid cells of corrected halo'd [y+2, z+2, x+2] fields, in the
+    engine's discrete divergence (periodic x and z halos, wall faces V(0) and V(ny))."""
+    import torch
+    ny = U.shape[0] - 2
+    out = 0.0
+    for j0 in range(0, ny, 64):  # plane blocks bound the temporaries
+        j1 = min(ny, j0 + 64)
+        sl = slice(j0 + 1, j1 + 1)
+        d = (U[sl, 1:-1, 2:] - U[sl, 1:-1, 1:-1]) / dx
+        d += (W[sl, 2:, 1:-1] - W[sl, 1:-1, 1:-1]) / dz
+        v1 = V[j0 + 2:j1 + 2, 1:-1, 1:-1].clone()
+        v0 = V[sl, 1:-1, 1:-1].clone()
+        if j1 == ny:
+            v1[-1] = vtop
+        if j0 == 0:
+            v0[0] = vbot
+        d += (v1 - v0) * inv_dy_p[j0:j1].view(-1, 1, 1)
+        d.masked_fill_(solid[j0:j1], 0.0)
+        out = max(out, float(d.abs().max()))
+    return out
+
+
+def run_rough(device, nx, ny, nz, steps, warmup):
+    """Rough-wall projection: wall-refined faces (uniform below y = 0.1, 1.5% growth per
+    cell), the channel predictor zeroed inside a Gaussian k^-2 height field (peak 0.08,
+    RMS 0.02, default_rng(5), both walls), FP64 and FP32 storage + FP64 refinement."""
+    import numpy as np
+    import torch
+    import prj
+    import workloads
+    yu = workloads.wall_refined_faces(ny)
+    h = workloads.rough_height_field(nx, nz, seed=5)
+    yp = torch.tensor((yu[:-1] + yu[1:]) / 2, dtype=torch.float64, device=device).view(-1, 1, 1)
+    ht = torch.tensor(h.T.copy(), dtype=torch.float64, device=device).unsqueeze(0)  # [1, z, x]
+    solid = (yp < ht) | (yp > 2.0 - ht)                                              # [y, z, x]
+    g = torch.Generator(device=device)
+    g.manual_seed(6)
+    hs = (ny + 2, nz + 2, nx + 2)
+    fields = []
+    for comp in range(3):
+        f = torch.zeros(hs, dtype=torch.float64, device=device)
+        inner = f[1:-1, 1:-1, 1:-1]
+        inner.normal_(0.0, 0.1, generator=g)
+        if comp == 0:
+            inner += 1.5 * (1.0 - (yp - 1.0) ** 2)
+        inner.masked_fill_(solid, 0.0)
+        if comp == 1:
+            f[1] = 0.0
+        fields.append(f)
+    Uh, Vh, Wh = fields
+    U, V, W = (torch.empty_like(Uh) for _ in range(3))
+    P = torch.empty((ny, nz, nx), dtype=torch.float64, device=device)
+    dx, dz = 2 * math.pi / nx, math.pi / nz
+    inv_dy_p = torch.tensor(prj.metrics(yu)[0], dtype=torch.float64, device=device)
+    out = {"grid": f"{nx}x{ny}x{nz}", "solid_fraction": float(solid.float().mean()),
+           "dy_wall": float(yu[1] - yu[0]), "dy_max": float(np.diff(yu).max())}
+    stream = torch.cuda.current_stream(device)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent", device=device.index or 0) as plan:
+        P64 = None
+        for name, mode in (("fp64", prj.MODE_FP64), ("mixed", prj.MODE_FP32_REFINE)):
+            fn = lambda: plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=mode, stats=False, stream=stream)
+            for _ in range(warmup):
+                fn()
+            ms = timed_steps(fn, stream, steps) / steps
+            st = plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=mode, stats=True, stream=stream)
+            rec = {"gpts_per_s": nx * ny * nz / (ms / 1e3) / 1e9, "ms_per_step": ms,
+                   "div_maxabs_all": st["div_maxabs"],
+                   "div_maxabs_fluid": fluid_div_maxabs(U, V, W, solid, inv_dy_p, dx, dz)}
+            if P64 is None:
+                P64 = P.clone()
+            else:
+                rec["p_rel_l2_vs_fp64"] = float(torch.linalg.vector_norm(P - P64) / torch.linalg.vector_norm(P64))
+                rec.update({k: st[k] for k in ("refine_iters", "fp64_lines", "last_update_rel")})
+            out[name] = rec
+        del P64
+    return out
+
+
 def run_served(device, seconds, rate, budget):
     """Open-loop Poisson arrivals (rate per second, default_rng(3)) of projection requests of
     sizes (128,96,64)/(256,128,128)/(384,192,192)/(768,384,384) with p = 0.4/0.3/0.2/0.1."""
@@ -321,6 +400,7 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=30.0)
     ap.add_argument("--served-rate", type=float, default=2000.0)
     ap.add_argument("--served-budget-gb", type=float, default=150.0)
+    ap.add_argument("--rough-grid", default="1536x512x768", help="rough-wall leg nx x ny x nz ('' skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -458,6 +538,11 @@ def main():
         extra["batched"] = run_batched(device, steps=max(3, args.steps // 4), warmup=args.warmup)
         torch.cuda.empty_cache()
         extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
+        torch.cuda.empty_cache()
+        if args.rough_grid:
+            rx, ry, rz = (int(v) for v in args.rough_grid.lower().split("x"))
+            extra["rough_wall"] = run_rough(device, rx, ry, rz, steps=max(3, args.steps // 10), warmup=args.warmup)
+            torch.cuda.empty_cache()
 
     if rank == 0:
         line = {

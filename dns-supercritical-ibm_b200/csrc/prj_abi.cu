@@ -269,7 +269,7 @@ int ensure_mixed(prj_plan* pl) {
     for (int kx = 1; kx < g.nxh; kx++)
         if (std::fabs(ax[kx]) >= tau * bmax) { kxs = kx; break; }
     pl->kxs_mixed = kxs;
-    pl->mixed_iters = (int)env_double("PRJ_MIXED_ITERS", 2);
+    pl->mixed_iters = (int)env_double("PRJ_MIXED_ITERS", 1);  // one pass leaves ~1e-13 (the next update measures 1e-14)
     if (pl->mixed_iters < 0) pl->mixed_iters = 0;
     const size_t n32 = (size_t)(g.nxh - kxs) * g.nz * g.ny;
     if (n32) {

@@ -86,3 +86,61 @@ def projection_inputs(nx: int, ny: int, nz: int, beta: float = 2.0, seed: int = 
 
 def halo_shape(nx, nz, ny):
     return (nx + 2, nz + 2, ny + 2)
+
+
+def rough_height_field(nx: int, nz: int, lx: float = 2 * np.pi, lz: float = np.pi, seed: int = 5,
+                       kmin: float = 2 * np.pi / 0.5, kmax: float = 2 * np.pi / 0.05, peak: float = 0.08,
+                       rms: float = 0.02) -> np.ndarray:
+    """Rough-wall height h(x, z) >= 0 at the cell centres, shape (nx, nz).
+
+    A Gaussian random field g with isotropic power spectrum |k|^-2 for kmin <= |k| <= kmax
+    (zero elsewhere; complex normal Fourier coefficients from default_rng(seed)) is mapped to
+    h = max(0, peak - s (max g - g)), with s found by bisection so that sqrt(mean h^2) = rms.
+    The map fixes both the peak height and the RMS height, and h = 0 marks smooth wall."""
+    rng = np.random.default_rng(seed)
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=lx / nx)
+    kz = 2 * np.pi * np.fft.rfftfreq(nz, d=lz / nz)
+    k = np.hypot(kx[:, None], kz[None, :])
+    amp = np.zeros_like(k)
+    band = (k >= kmin) & (k <= kmax)
+    amp[band] = 1.0 / k[band]
+    coef = amp * (rng.standard_normal(k.shape) + 1j * rng.standard_normal(k.shape))
+    g = np.fft.irfft2(coef, s=(nx, nz))
+    g = (g - g.mean()) / g.std()
+    gap = g.max() - g
+
+    def rms_of(s):
+        return np.sqrt(np.mean(np.maximum(0.0, peak - s * gap) ** 2))
+
+    lo, hi = 0.0, 1.0
+    while rms_of(hi) > rms:
+        hi *= 2.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if rms_of(mid) > rms:
+            lo = mid
+        else:
+            hi = mid
+    return np.maximum(0.0, peak - 0.5 * (lo + hi) * gap)
+
+
+def solid_cells(h: np.ndarray, yu: np.ndarray) -> np.ndarray:
+    """Cells (i, k, j) inside the roughness, shape (nx, nz, ny): cell centre y_p below h on the
+    bottom wall or above 2 - h on the top wall (the same height field on both walls)."""
+    yp = (yu[:-1] + yu[1:]) / 2
+    return (yp[None, None, :] < h[:, :, None]) | (yp[None, None, :] > 2.0 - h[:, :, None])
+
+
+def rough_projection_inputs(nx: int, ny: int, nz: int, seed: int = 5, sigma: float = 0.1):
+    """Projection inputs of the rough-wall channel: wall-refined faces (uniform below
+    y = 0.1, 1.5% growth toward the centre), the channel predictor of projection_inputs
+    (noise from default_rng(seed + 1)), and every velocity component whose cell lies in the
+    roughness (height field from default_rng(seed)) set to zero.
+
+    Returns (Uh, Vh, Wh, yu, dx, dz, solid) with solid[x, z, y] boolean."""
+    yu = wall_refined_faces(ny)
+    Uh, Vh, Wh, yu, dx, dz = projection_inputs(nx, ny, nz, seed=seed + 1, sigma=sigma, yu=yu)
+    solid = solid_cells(rough_height_field(nx, nz, seed=seed), yu)
+    for f in (Uh, Vh, Wh):
+        f[1:-1, 1:-1, 1:-1][solid] = 0.0
+    return Uh, Vh, Wh, yu, dx, dz, solid

@@ -130,8 +130,10 @@ int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h
  * Poisson solve in place with FP32 spectral storage and FP64 iterative
  * refinement (the precision scheme of PRJ_MODE_FP32_REFINE): rows of
  * x-wavenumbers whose tridiagonals are badly conditioned stay FP64, the
- * residual b - A p of the pinned operator is formed in FP64.  Needs in-place
- * transform plans (radices 2, 3, 4, 5, 8 for nx/2 and nz).  Asynchronous.
+ * residual b - A p of the pinned operator is formed in FP64.  One refinement
+ * pass by default (environment variable PRJ_MIXED_ITERS, read at the plan's
+ * first mixed call).  Needs in-place transform plans (radices 2, 3, 4, 5, 8 for
+ * nx/2 and nz).  Asynchronous.
  */
 int prj_poisson_mixed(prj_plan* plan, double* d_P, void* stream);
 
