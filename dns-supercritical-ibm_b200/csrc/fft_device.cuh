@@ -96,6 +96,19 @@ template <int DIR, typename V> __device__ __forceinline__ void dft8(V* a) {
     a[3] = cadd(e3, o3);   a[7] = csub(e3, o3);
 }
 
+// 6-point DFT by the prime-factor map n = (3 n1 + 2 n2) mod 6, k = (3 k1 + 4 k2) mod 6:
+// two 3-point DFTs and three 2-point DFTs, no internal twiddles.
+template <int DIR, typename V>
+__device__ __forceinline__ void dft6(V* a) {
+    V e0 = a[0], e1 = a[2], e2 = a[4];
+    V o0 = a[3], o1 = a[5], o2 = a[1];
+    dft3<DIR>(e0, e1, e2);
+    dft3<DIR>(o0, o1, o2);
+    a[0] = cadd(e0, o0); a[3] = csub(e0, o0);
+    a[4] = cadd(e1, o1); a[1] = csub(e1, o1);
+    a[2] = cadd(e2, o2); a[5] = csub(e2, o2);
+}
+
 // ------------------------------------------------------------ one radix stage
 // i: butterfly index in [0, n/R); k = i mod p.  Inputs src[i + r n/R];
 // outputs dst[(i - k) R + k + r p].

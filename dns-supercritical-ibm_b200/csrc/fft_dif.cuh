@@ -8,9 +8,9 @@
 // buffer.  The result is in digit-reversed order: frequency (or, for the
 // inverse, time) index k sits at slot pos[k]; consumers read through `pos`.
 //
-// Twiddles per stage: tw[j (R-1) + q - 1] = exp(-2 pi i q j / L), j < L/R,
+// Twiddles per stage: tw[(q - 1) L/R + j] = exp(-2 pi i q j / L), j < L/R,
 // 1 <= q < R.  The inverse transform uses the conjugates.  Radices 2, 3, 4, 5
-// and 8 only; other lengths use the out-of-place path of fft_device.cuh.
+// 6 and 8 only; other lengths use the out-of-place path of fft_device.cuh.
 #pragma once
 #include "fft_device.cuh"
 
@@ -66,7 +66,7 @@ __device__ __forceinline__ int sidx(int g) {
 // elements per row buffer of n slots with optional padding
 __host__ __device__ inline int padded_len(int n, bool pad) { return pad ? n + (n >> 3) + 1 : n; }
 
-// One butterfly of radix R on elements g0 + r mm (r < R) of buf.
+// One butterfly of radix R on elements g0 + r mm (r < R) of buf; w = the stage's twiddles.
 // DIT = false: DFT, then twiddles (decimation in frequency);
 // DIT = true: twiddles, then DFT (its transpose).
 template <int DIR, bool DIT, bool PAD, int R, typename V>
@@ -76,16 +76,17 @@ __device__ __forceinline__ void bfly_r(V* __restrict__ buf, int g0, int mm, int 
     for (int r = 0; r < R; r++) a[r] = buf[sidx<PAD>(g0 + r * mm)];
     if (DIT && j) {
 #pragma unroll
-        for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
+        for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[(q - 1) * mm + j]);
     }
     if (R == 2) dft2<DIR>(a[0], a[1]);
     else if (R == 3) dft3<DIR>(a[0], a[1], a[2]);
     else if (R == 4) dft4<DIR>(a[0], a[1], a[2], a[3]);
     else if (R == 5) dft5<DIR>(a[0], a[1], a[2], a[3], a[4]);
+    else if (R == 6) dft6<DIR>(a);
     else dft8<DIR>(a);
     if (!DIT && j) {
 #pragma unroll
-        for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[q - 1]);
+        for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[(q - 1) * mm + j]);
     }
 #pragma unroll
     for (int r = 0; r < R; r++) buf[sidx<PAD>(g0 + r * mm)] = a[r];
@@ -98,6 +99,7 @@ __device__ __forceinline__ void bfly(V* __restrict__ buf, int g0, int mm, int R,
     case 3: bfly_r<DIR, DIT, PAD, 3>(buf, g0, mm, j, w); break;
     case 4: bfly_r<DIR, DIT, PAD, 4>(buf, g0, mm, j, w); break;
     case 5: bfly_r<DIR, DIT, PAD, 5>(buf, g0, mm, j, w); break;
+    case 6: bfly_r<DIR, DIT, PAD, 6>(buf, g0, mm, j, w); break;
     case 8: bfly_r<DIR, DIT, PAD, 8>(buf, g0, mm, j, w); break;
     default:
         // other radices are planned on the out-of-place Stockham path (fft_device.cuh);
@@ -128,7 +130,7 @@ __device__ void inplace_rows(V* buf, int nrows, int rs, const DifDev& f, const V
             const int bi = idx - row * nb;
             const int b = fdiv(bi, dmm);
             const int j = bi - b * mm;
-            bfly<DIR, DIT, PAD>(buf, row * rs + b * L + j, mm, R, j, tws + j * (R - 1));
+            bfly<DIR, DIT, PAD>(buf, row * rs + b * L + j, mm, R, j, tws);
         }
         __syncthreads();
     }

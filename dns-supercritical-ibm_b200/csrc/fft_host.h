@@ -8,12 +8,31 @@
 #include <cstring>
 
 #include "fft_dif.cuh"
+#include "fft_pass.cuh"
 
 namespace prj {
 
-// radix sequence of a length-n transform: 8 first, then 4, 2, 3, 5, then any
-// remaining primes; returns the number of stages or -1
+// radices of the lengths with a compile-time pass plan (fft_pass.cuh); 0 if none
+inline int pass_radices(int n, int* fac, int cap) {
+#define PRJ_PASS_RADICES(N, ...)                                  \
+    if (n == N) {                                                 \
+        const int r[] = {__VA_ARGS__};                            \
+        const int nr = (int)(sizeof(r) / sizeof(r[0]));           \
+        if (nr > cap) return -1;                                  \
+        for (int i = 0; i < nr; i++) fac[i] = r[i];               \
+        return nr;                                                \
+    }
+    PRJ_PASS_PLANS(PRJ_PASS_RADICES)
+#undef PRJ_PASS_RADICES
+    return 0;
+}
+
+// radix sequence of a length-n transform: the pass plan's radices where one
+// exists, else 8 first, then 4, 2, 3, 5, then any remaining primes; returns the
+// number of stages or -1
 inline int fft_factorize(int n, int* fac, int cap) {
+    const int np = pass_radices(n, fac, cap);
+    if (np != 0) return np;
     int nf = 0, m = n;
     auto push = [&](int r) { if (nf < cap) fac[nf] = r; nf++; };
     while (m % 8 == 0 && m != 16) { push(8); m /= 8; }
@@ -27,13 +46,13 @@ inline int fft_factorize(int n, int* fac, int cap) {
     return nf <= cap ? nf : -1;
 }
 
-// true when every radix of n has a hard-coded DIF butterfly (2, 3, 4, 5, 8)
+// true when every radix of n has a hard-coded DIF butterfly (2, 3, 4, 5, 6, 8)
 inline bool dif_supported(int n) {
     int fac[64];
     const int nf = fft_factorize(n, fac, 64);
     if (nf < 0 || nf > kMaxStages) return false;
     for (int s = 0; s < nf; s++)
-        if (!(fac[s] == 2 || fac[s] == 3 || fac[s] == 4 || fac[s] == 5 || fac[s] == 8)) return false;
+        if (!(fac[s] == 2 || fac[s] == 3 || fac[s] == 4 || fac[s] == 5 || fac[s] == 6 || fac[s] == 8)) return false;
     return true;
 }
 
@@ -60,15 +79,16 @@ inline long dif_plan(int n, DifDev* f) {
     return cnt > 0 ? cnt : 1;
 }
 
-// twiddles (forward sign) and positions: pos[k] = slot of index k after the transform
+// twiddles (forward sign; stage s at twoff[s], entry (q-1) mm + j, so the butterflies of
+// consecutive j read consecutive entries) and positions: pos[k] = slot of index k after the transform
 template <typename V>
 inline void dif_fill(const DifDev& f, V* tw, int* pos) {
     const long double two_pi = 6.283185307179586476925286766559005768L;
     long c = 0;
     for (int s = 0; s < f.nst; s++) {
         const int R = f.radix[s], L = f.span[s], mm = L / R;
-        for (int j = 0; j < mm; j++)
-            for (int q = 1; q < R; q++) {
+        for (int q = 1; q < R; q++)
+            for (int j = 0; j < mm; j++) {
                 const long double a = two_pi * (long double)q * j / (long double)L;
                 tw[c].x = (decltype(tw[c].x))cosl(a);
                 tw[c].y = (decltype(tw[c].y))(-sinl(a));

@@ -579,8 +579,14 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if ((rc = make_dif(nz, &pl->zd, &bytes))) return bail(rc);
     if (pl->zd.ok && (rc = make_slot_table(nz, &pl->kz_of_slot, &bytes))) return bail(rc);
     pl->zmode = z_mode(pl->zd.ok && pl->kz_of_slot);
+    {
+        // PRJ_FFT_KERNELS=runtime keeps the runtime-radix kernels for lengths with a pass plan
+        const char* v = getenv("PRJ_FFT_KERNELS");
+        pl->use_pass = !(v && !strcmp(v, "runtime"));
+    }
     pl->kxs = g.nxh;
     pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);
+    pl->tz_xp = prj::choose_tz_xp(pl->fx64.m);
 
     // rows per CTA of the x kernels: fit two ping-pong buffers in ~100 KB
     {
@@ -846,9 +852,15 @@ int prj_poisson_mixed(prj_plan* plan, double* d_P, void* stream) {
     return run_mixed_poisson(plan, d_P, (cudaStream_t)stream);
 }
 
+// true when the x transforms run the pass-plan kernels (even nx, m = nx/2 with a plan)
+bool x_pass_active(const prj_plan* pl) {
+    int fac[8];
+    return pl->use_pass && pl->fx64.even && pl->xd.ok && prj::pass_radices(pl->fx64.m, fac, 8) > 0;
+}
+
 int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out) {
     if (!plan || !out) return fail(PRJ_ERR_ARG, "NULL argument");
-    out->x_rows = plan->tz_xd;
+    out->x_rows = x_pass_active(plan) ? plan->tz_xp : plan->tz_xd;
     out->z_rows = plan->zfft_rows;
     out->z_mode = plan->zmode;
     return PRJ_OK;
@@ -869,6 +881,7 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
     if (t->z_rows && (size_t)prj::padded_len(t->z_rows * plan->g.nz, true) * sizeof(double2) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "z_rows=%d does not fit shared memory for nz=%d", t->z_rows, plan->g.nz);
     plan->tz_xd = t->x_rows;
+    plan->tz_xp = t->x_rows;
     plan->zfft_rows = t->z_rows;
     plan->zmode = t->z_mode;
     return PRJ_OK;

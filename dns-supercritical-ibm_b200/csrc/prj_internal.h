@@ -107,6 +107,8 @@ struct prj_plan {
     double* mix_r = nullptr;      // Poisson-only mixed solve: residual
     int zfft_rows = 0;            // rows per CTA of the z-transform kernels (0: default rule)
     int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
+    bool use_pass = true;         // compile-time pass-plan FFT kernels where the length has one
+    int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
 };
 
 namespace prj {
@@ -141,6 +143,8 @@ cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, co
                           const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout = nullptr);
 cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum = 0, double* sq = nullptr);
 int choose_tz_xd(int m, bool even);
+int choose_tz_xp(int m);                 // rows per CTA of the pass-plan x kernels
+size_t pass_x_smem(int m, int tz);       // their shared memory
 
 // z direction as separate kernels (prj_zsplit.cu); need pl->zd.ok and pl->kz_of_slot
 cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st);

@@ -11,6 +11,7 @@
 // CTAs fit on an SM.  Loads and stores of P and u_hat are one element per
 // thread along x (fully coalesced).
 #include "fft_dif.cuh"
+#include "fft_pass.cuh"
 #include "prj_internal.h"
 
 // minimum resident CTAs per SM requested for the shared-memory FFT kernels
@@ -255,6 +256,182 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pass-plan x kernels (fft_pass.cuh), m = nx/2 with a compile-time plan PL.
+// Row stride m + 1 (odd) keeps the row-fastest split and load phases free of
+// bank conflicts.  nr = rows present in this CTA (the last CTA may hold fewer).
+
+// k_fwd_xp: source (P, or the divergence of u_hat) -> packed complex -> DIF
+// passes -> split X_k, X_{m-k} -> transposed store.  SRC 0 reads P in the first
+// pass; SRC 1 stages the divergence in shared memory first.
+template <int SRC, class PL>
+__global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_fwd_xp(const XArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* A = reinterpret_cast<double2*>(sm);
+    constexpr int m = PL::n, nx = 2 * m, rs = m + 1;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int nr = min(a.tz, a.nz - z0);
+    const double2* tw = a.tw;
+    if (SRC == 1) {
+        // divergence of the x pair (2e, 2e+1) of row z0 + r, as packed complex element e
+        // (the operation order of div_at); rows of the halo'd fields addressed from
+        // per-item row pointers, kUnroll items in flight per thread
+        const size_t hrow = (size_t)nx + 2, hplane = hrow * (size_t)(a.nz + 2);
+        const double idy = a.inv_dy_p[y];
+        const bool wb = (y == 0), wt = (y + 1 == a.ny);
+        const int total = nr * m;
+        for (int base = tid; base < total; base += kUnroll * nthr) {
+            double2 v[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const int idx = base + u * nthr;
+                if (idx < total) {
+                    const int r = idx / m, e = idx - r * m;
+                    const int z = z0 + r, zp = (z + 1 == a.nz) ? 0 : z + 1;
+                    const size_t c0 = (size_t)(y + 1) * hplane + (size_t)(z + 1) * hrow + 1;
+                    const size_t cz = (size_t)(y + 1) * hplane + (size_t)(zp + 1) * hrow + 1;
+                    const int i0 = 2 * e, i1 = i0 + 1, i2 = (i1 + 1 == nx) ? 0 : i1 + 1;
+                    const double u0 = a.Uh[c0 + i0], u1 = a.Uh[c0 + i1], u2 = a.Uh[c0 + i2];
+                    const double w00 = a.Wh[c0 + i0], w01 = a.Wh[c0 + i1];
+                    const double w10 = a.Wh[cz + i0], w11 = a.Wh[cz + i1];
+                    const double v00 = wb ? a.vbot : a.Vh[c0 + i0], v01 = wb ? a.vbot : a.Vh[c0 + i1];
+                    const double v10 = wt ? a.vtop : a.Vh[c0 + hplane + i0];
+                    const double v11 = wt ? a.vtop : a.Vh[c0 + hplane + i1];
+                    double s0 = __dmul_rn(__dsub_rn(u1, u0), a.inv_dx);
+                    s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(w10, w00), a.inv_dz));
+                    s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(v10, v00), idy));
+                    double s1 = __dmul_rn(__dsub_rn(u2, u1), a.inv_dx);
+                    s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(w11, w01), a.inv_dz));
+                    s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(v11, v01), idy));
+                    v[u] = make_double2(__dmul_rn(a.inv_dt, s0), __dmul_rn(a.inv_dt, s1));
+                    if (a.Bout) {
+                        double* b = a.Bout + ((size_t)y * a.nz + z) * nx + i0;
+                        b[0] = v[u].x;
+                        b[1] = v[u].y;
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const int idx = base + u * nthr;
+                if (idx < total) {
+                    const int r = idx / m, e = idx - r * m;
+                    A[sidx<true>(r * rs + e)] = v[u];
+                }
+            }
+        }
+        __syncthreads();
+        dif_passes_shared<-1, PL, 0, PL::P>(A, nr, rs, tw);
+    } else {
+        const double2* src = reinterpret_cast<const double2*>(a.P) + ((size_t)y * a.nz + z0) * m;
+        double2* bout = a.Bout ? reinterpret_cast<double2*>(a.Bout) + ((size_t)y * a.nz + z0) * m : nullptr;
+        dif_first_pass<-1, PL>(A, nr, rs, tw, [&](int r, int e) {
+            const double2 v = src[(size_t)r * m + e];
+            if (bout) bout[(size_t)r * m + e] = v;
+            return v;
+        });
+        __syncthreads();
+        dif_passes_shared<-1, PL, 1, PL::P>(A, nr, rs, tw);
+    }
+    // split: X_k = E_k + W^k O_k, X_{m-k} = conj(E_k) + W^{m-k} conj(O_k); row index fastest
+    constexpr int half = m / 2;
+    for (int idx = tid; idx < nr * (half + 1); idx += nthr) {
+        const int k = idx / nr, r = idx - k * nr;
+        const int base = r * rs;
+        const int z = z0 + r;
+        if (k == 0) {
+            const double2 c = A[sidx<true>(base)];
+            spec_store(a, y, 0, z, make_double2(c.x + c.y, 0.0));
+            spec_store(a, y, m, z, make_double2(c.x - c.y, 0.0));
+        } else {
+            const int kk = m - k;
+            const double2 zk = A[sidx<true>(base + pass_slot<PL>(k))];
+            const double2 zm = cconj(A[sidx<true>(base + pass_slot<PL>(kk))]);
+            const double2 e = cscale(cadd(zk, zm), 0.5);
+            const double2 d = csub(zk, zm);
+            const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
+            spec_store(a, y, k, z, cadd(e, cmul(a.post[k], o)));
+            if (kk != k) spec_store(a, y, kk, z, cadd(cconj(e), cmul(a.post[kk], cconj(o))));
+        }
+    }
+}
+
+// k_bwd_xp: transposed load of X_k, X_{m-k} -> inverse split (scaled) into slot
+// order -> DIT passes -> P rows (x pairs as double2), optionally accumulated.
+template <class PL>
+__global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_bwd_xp(const XArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* A = reinterpret_cast<double2*>(sm);
+    constexpr int m = PL::n, rs = m + 1, half = m / 2;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int nr = min(a.tz, a.nz - z0);
+    const double s = a.scale;
+    const int total = nr * (half + 1);
+    // X_k and X_{m-k} of kUnroll items loaded together (independent loads in flight)
+    for (int base0 = tid; base0 < total; base0 += kUnroll * nthr) {
+        double2 xa[kUnroll], xb[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int idx = base0 + u * nthr;
+            if (idx < total) {
+                const int k = idx / nr, r = idx - k * nr;
+                xa[u] = spec_load(a, y, k, z0 + r);
+                xb[u] = spec_load(a, y, m - k, z0 + r);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int idx = base0 + u * nthr;
+            if (idx >= total) continue;
+            const int k = idx / nr, r = idx - k * nr;
+            const int base = r * rs;
+            if (k == 0) {
+                const double x0 = xa[u].x, xm = xb[u].x;
+                A[sidx<true>(base)] = make_double2((x0 + xm) * s, (x0 - xm) * s);
+            } else {
+                const int kk = m - k;
+                const double2 xk = xa[u], xkk = xb[u];
+                const double2 e1 = cadd(xk, cconj(xkk));
+                const double2 o1 = cmulc(csub(xk, cconj(xkk)), a.post[k]);
+                A[sidx<true>(base + pass_slot<PL>(k))] = cscale(make_double2(e1.x - o1.y, e1.y + o1.x), s);
+                if (kk != k) {
+                    const double2 e2 = cadd(xkk, cconj(xk));
+                    const double2 o2 = cmulc(csub(xkk, cconj(xk)), a.post[kk]);
+                    A[sidx<true>(base + pass_slot<PL>(kk))] = cscale(make_double2(e2.x - o2.y, e2.y + o2.x), s);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    dit_passes_shared<+1, PL, PL::P - 1, 0>(A, nr, rs, a.tw);
+    double2* out = reinterpret_cast<double2*>(a.Pout) + ((size_t)y * a.nz + z0) * m;
+    double sq0 = 0.0, sq1 = 0.0;
+    dit_last_pass<+1, PL>(A, nr, rs, a.tw, [&](int r, int e, double2 v) {
+        double2* o = out + (size_t)r * m + e;
+        if (a.accum) {
+            const double2 old = *o;
+            const double2 nv = make_double2(old.x + v.x, old.y + v.y);
+            sq0 += v.x * v.x + v.y * v.y;
+            sq1 += nv.x * nv.x + nv.y * nv.y;
+            *o = nv;
+        } else {
+            *o = v;
+        }
+    });
+    if (a.sq) {
+        for (int o = 16; o > 0; o >>= 1) {
+            sq0 += __shfl_xor_sync(0xffffffffu, sq0, o);
+            sq1 += __shfl_xor_sync(0xffffffffu, sq1, o);
+        }
+        if ((tid & 31) == 0) {
+            atomicAdd(a.sq, sq0);
+            atomicAdd(a.sq + 1, sq1);
+        }
+    }
+}
+
 XArgs make_args(const prj_plan* pl) {
     const Geometry& g = pl->g;
     XArgs a{};
@@ -282,6 +459,16 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 }  // namespace
 
+// rows per CTA of the pass-plan x kernels: a power of two up to 16 whose padded rows
+// (stride m + 1) fit 28 KB, so that 7-8 CTAs share an SM
+int choose_tz_xp(int m) {
+    int tz = 16;
+    while (tz > 1 && (size_t)padded_len(tz * (m + 1), true) * sizeof(double2) > 28 * 1024) tz /= 2;
+    return tz;
+}
+
+size_t pass_x_smem(int m, int tz) { return (size_t)padded_len(tz * (m + 1), true) * sizeof(double2); }
+
 // rows per CTA of the in-place x kernels: a power of two up to 16 within ~56 KB
 int choose_tz_xd(int m, bool even) {
     const int rs = even ? m + 1 : m;
@@ -290,12 +477,67 @@ int choose_tz_xd(int m, bool even) {
     return tz;
 }
 
+namespace {
+
+inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+size_t pass_smem_bytes(const XArgs& a) { return (size_t)padded_len(a.tz * (a.m + 1), true) * sizeof(double2); }
+
+template <class PL>
+cudaError_t launch_fwd_xp_pl(const XArgs& a, FwdSource src, const dim3& grid, cudaStream_t st) {
+    const size_t smem = pass_smem_bytes(a);
+    cudaError_t e;
+    if (src == FwdSource::Pressure) {
+        if ((e = allow_smem(k_fwd_xp<0, PL>, smem)) != cudaSuccess) return e;
+        k_fwd_xp<0, PL><<<grid, kPassThreads, smem, st>>>(a);
+    } else {
+        if ((e = allow_smem(k_fwd_xp<1, PL>, smem)) != cudaSuccess) return e;
+        k_fwd_xp<1, PL><<<grid, kPassThreads, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <class PL>
+cudaError_t launch_bwd_xp_pl(const XArgs& a, const dim3& grid, cudaStream_t st) {
+    const size_t smem = pass_smem_bytes(a);
+    cudaError_t e = allow_smem(k_bwd_xp<PL>, smem);
+    if (e != cudaSuccess) return e;
+    k_bwd_xp<PL><<<grid, kPassThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// pass-plan x kernels for even nx whose half length has a pass plan built with the
+// same radices; cudaErrorNotSupported otherwise (the caller uses the runtime-radix kernels)
+cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, cudaStream_t st) {
+    if (!pl->use_pass || !a.even) return cudaErrorNotSupported;
+    a.tz = pl->tz_xp;
+    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
+    switch (a.m) {
+#define PRJ_X_CASE(N, ...)                                                          \
+    case N: {                                                                       \
+        using PL = PassList<__VA_ARGS__>;                                           \
+        if (!same_radices<PL>(pl->xd.f)) return cudaErrorNotSupported;              \
+        return fwd ? launch_fwd_xp_pl<PL>(a, src, grid, st) : launch_bwd_xp_pl<PL>(a, grid, st); \
+    }
+        PRJ_PASS_PLANS(PRJ_X_CASE)
+#undef PRJ_X_CASE
+    default:
+        return cudaErrorNotSupported;
+    }
+}
+
+}  // namespace
+
 cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
                           const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout) {
     XArgs a = make_args(pl);
     a.Bout = bout;
     a.P = P; a.Uh = Uh; a.Vh = Vh; a.Wh = Wh; a.inv_dy_p = pl->t.inv_dy_p;
     if (sc) { a.inv_dt = sc->inv_dt; a.vbot = sc->wall[1]; a.vtop = sc->wall[4]; }
+    if (src == FwdSource::Divergence || (aligned16(P) && aligned16(bout))) {
+        const cudaError_t e = launch_xpass(pl, true, src, a, st);
+        if (e != cudaErrorNotSupported) return e;
+    }
     const size_t smem = smem_bytes(a);
     const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
     cudaError_t e;
@@ -315,6 +557,10 @@ cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int ac
     a.accum = accum;
     a.sq = sq;
     a.scale = 1.0 / ((double)pl->g.nx * (double)pl->g.nz + 0.0);
+    if (aligned16(P)) {
+        const cudaError_t e2 = launch_xpass(pl, false, FwdSource::Pressure, a, st);
+        if (e2 != cudaErrorNotSupported) return e2;
+    }
     const size_t smem = smem_bytes(a);
     cudaError_t e = allow_smem(k_bwd_xd, smem);
     if (e != cudaSuccess) return e;

@@ -15,6 +15,7 @@
 // of nx/2+1 CTAs.  The Thomas arithmetic keeps the reference's operation order
 // and rounding (poisson_solver_multigpu.f90:401-419) with pivots D from the
 // plan's table (the pair kz, nz-kz shares one pivot row entry).
+#include "fft_pass.cuh"
 #include "prj_internal.h"
 
 // minimum resident CTAs per SM requested for the shared-memory FFT kernels
@@ -67,6 +68,33 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
     else inplace_rows<+1, true, true>(zs, nr, a.nz, a.f, a.tw);
     T* dst = static_cast<T*>(a.X) + row0 * a.nz;
     for (int i = tid; i < tot; i += nthr) from_d2(dst[i], zs[sidx<true>(i)]);
+}
+
+// Pass-plan z transform (fft_pass.cuh): the first pass reads the rows from global
+// memory, the last writes them back; rb rows per CTA, kPassThreads threads.
+template <int DIR, typename T, class PL>
+__global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_zfft_pass(const ZfftArgs a) {
+    extern __shared__ __align__(16) double2 zp[];
+    constexpr int n = PL::n;
+    const size_t row0 = (size_t)blockIdx.x * a.rb;
+    const int nr = (int)min((size_t)a.rb, (size_t)a.nrow_total - row0);
+    T* X = static_cast<T*>(a.X) + row0 * n;
+    const double2* tw = a.tw;
+    // the forward transform's slot-order rows leave shared memory in whole coalesced
+    // rows (its last pass would store R contiguous elements per thread: half-sector
+    // writes per instruction); the inverse reads them directly (measured faster)
+    const int tot = nr * n;
+    if (DIR < 0) {
+        dif_first_pass<-1, PL>(zp, nr, n, tw, [&](int r, int e) { return to_d2(X[(size_t)r * n + e]); });
+        __syncthreads();
+        dif_passes_shared<-1, PL, 1, PL::P>(zp, nr, n, tw);
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) from_d2(X[i], zp[sidx<true>(i)]);
+    } else {
+        dit_first_pass<+1, PL>(zp, nr, n, [&](int r, int q) { return to_d2(X[(size_t)r * n + q]); });
+        __syncthreads();
+        dit_passes_shared<+1, PL, PL::P - 2, 0>(zp, nr, n, tw);
+        dit_last_pass<+1, PL>(zp, nr, n, tw, [&](int r, int e, double2 v) { from_d2(X[(size_t)r * n + e], v); });
+    }
 }
 
 struct ThomasArgs {
@@ -166,11 +194,63 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 }  // namespace
 
+// rows per CTA of the pass-plan kernels: the requested count, else the largest
+// power of two up to 32 whose padded rows fit 28 KB (7-8 CTAs per SM)
+inline int pass_rows(int n, int requested, size_t limit_req = (size_t)200 * 1024) {
+    int rb = requested > 0 ? requested : 32;
+    const size_t limit = requested > 0 ? limit_req : (size_t)28 * 1024;
+    while (rb > 1 && (size_t)padded_len(rb * n, true) * sizeof(double2) > limit) rb /= 2;
+    return rb;
+}
+
+template <int DIR, typename T, class PL>
+cudaError_t launch_zfft_pass_pl(ZfftArgs a, int rows_req, cudaStream_t st) {
+    a.rb = pass_rows(PL::n, rows_req);
+    const size_t smem = (size_t)padded_len(a.rb * PL::n, true) * sizeof(double2);
+    const unsigned grid = (unsigned)((a.nrow_total + a.rb - 1) / a.rb);
+    if (grid == 0) return cudaSuccess;
+    cudaError_t e = allow_smem(k_zfft_pass<DIR, T, PL>, smem);
+    if (e != cudaSuccess) return e;
+    k_zfft_pass<DIR, T, PL><<<grid, kPassThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// pass-plan z transform of one buffer; cudaErrorNotSupported when nz has no pass
+// plan (or the plan was built with other radices)
+template <typename T>
+cudaError_t launch_zfft_pass(const prj_plan* pl, int dir, void* X, int rows_per_plane, cudaStream_t st) {
+    if (!pl->use_pass) return cudaErrorNotSupported;
+    const Geometry& g = pl->g;
+    ZfftArgs a{};
+    a.nrow_total = g.ny * rows_per_plane;
+    a.nz = g.nz;
+    a.f = pl->zd.f;
+    a.tw = pl->zd.tw;
+    a.X = X;
+    switch (g.nz) {
+#define PRJ_Z_CASE(N, ...)                                                                    \
+    case N: {                                                                                 \
+        using PL = PassList<__VA_ARGS__>;                                                     \
+        if (!same_radices<PL>(pl->zd.f)) return cudaErrorNotSupported;                        \
+        return dir < 0 ? launch_zfft_pass_pl<-1, T, PL>(a, pl->zfft_rows, st)                 \
+                       : launch_zfft_pass_pl<+1, T, PL>(a, pl->zfft_rows, st);                \
+    }
+        PRJ_PASS_PLANS(PRJ_Z_CASE)
+#undef PRJ_Z_CASE
+    default:
+        return cudaErrorNotSupported;
+    }
+}
+
 // in-place z FFT of every spectral row of one buffer: dir < 0 forward (natural ->
 // slot order), dir > 0 inverse (slot order -> natural); needs pl->zd.ok.
 // `rows_per_plane` rows of T storage per y plane.
 template <typename T>
 cudaError_t launch_zfft_t(const prj_plan* pl, int dir, void* X, int rows_per_plane, cudaStream_t st) {
+    {
+        const cudaError_t e = launch_zfft_pass<T>(pl, dir, X, rows_per_plane, st);
+        if (e != cudaErrorNotSupported) return e;
+    }
     const Geometry& g = pl->g;
     ZfftArgs a{};
     a.nrow_total = g.ny * rows_per_plane;
