@@ -192,10 +192,11 @@ __device__ __forceinline__ void dit_last_pass(const V* buf, int nrows, int rs, c
     }
 }
 
-// threads per CTA and minimum resident CTAs per SM of the pass-plan kernels
+// threads per CTA and minimum resident CTAs per SM of the pass-plan kernels (6: 85
+// registers, and 6 CTAs of ~28 KB shared memory per SM; measured best of 4-8)
 constexpr int kPassThreads = 128;
 #ifndef PRJ_PASS_MINB
-#define PRJ_PASS_MINB 8
+#define PRJ_PASS_MINB 6
 #endif
 
 // true when a runtime plan has exactly the radices of PL

@@ -275,46 +275,71 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_fwd_xp(const XA
     const double2* tw = a.tw;
     if (SRC == 1) {
         // divergence of the x pair (2e, 2e+1) of row z0 + r, as packed complex element e
-        // (the operation order of div_at); rows of the halo'd fields addressed from
-        // per-item row pointers, kUnroll items in flight per thread
+        // (the operation order of div_at).  Each field row is read as the aligned pair
+        // (interior 2e+1, 2e+2) -- halo'd positions 2e+2, 2e+3, 16-byte aligned because
+        // the halo'd row length nx + 2 is even -- and interior 2e comes from the lane
+        // holding item e-1 by shuffle (a scalar load where that lane holds another row
+        // or is outside the warp).  The periodic wrap u(nx) = u(0) is a scalar load.
         const size_t hrow = (size_t)nx + 2, hplane = hrow * (size_t)(a.nz + 2);
         const double idy = a.inv_dy_p[y];
         const bool wb = (y == 0), wt = (y + 1 == a.ny);
         const int total = nr * m;
-        for (int base = tid; base < total; base += kUnroll * nthr) {
+        const int lane = tid & 31;
+        const unsigned full = 0xffffffffu;
+        for (int base = tid - lane; base < total; base += kUnroll * nthr) {
             double2 v[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
-                const int idx = base + u * nthr;
-                if (idx < total) {
-                    const int r = idx / m, e = idx - r * m;
-                    const int z = z0 + r, zp = (z + 1 == a.nz) ? 0 : z + 1;
-                    const size_t c0 = (size_t)(y + 1) * hplane + (size_t)(z + 1) * hrow + 1;
-                    const size_t cz = (size_t)(y + 1) * hplane + (size_t)(zp + 1) * hrow + 1;
-                    const int i0 = 2 * e, i1 = i0 + 1, i2 = (i1 + 1 == nx) ? 0 : i1 + 1;
-                    const double u0 = a.Uh[c0 + i0], u1 = a.Uh[c0 + i1], u2 = a.Uh[c0 + i2];
-                    const double w00 = a.Wh[c0 + i0], w01 = a.Wh[c0 + i1];
-                    const double w10 = a.Wh[cz + i0], w11 = a.Wh[cz + i1];
-                    const double v00 = wb ? a.vbot : a.Vh[c0 + i0], v01 = wb ? a.vbot : a.Vh[c0 + i1];
-                    const double v10 = wt ? a.vtop : a.Vh[c0 + hplane + i0];
-                    const double v11 = wt ? a.vtop : a.Vh[c0 + hplane + i1];
-                    double s0 = __dmul_rn(__dsub_rn(u1, u0), a.inv_dx);
-                    s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(w10, w00), a.inv_dz));
-                    s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(v10, v00), idy));
-                    double s1 = __dmul_rn(__dsub_rn(u2, u1), a.inv_dx);
-                    s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(w11, w01), a.inv_dz));
-                    s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(v11, v01), idy));
-                    v[u] = make_double2(__dmul_rn(a.inv_dt, s0), __dmul_rn(a.inv_dt, s1));
-                    if (a.Bout) {
-                        double* b = a.Bout + ((size_t)y * a.nz + z) * nx + i0;
-                        b[0] = v[u].x;
-                        b[1] = v[u].y;
-                    }
+                const int idx = base + u * nthr + lane;
+                const bool in = idx < total;
+                const int r = in ? idx / m : 0, e = in ? idx - r * m : 0;
+                const int z = z0 + r, zp = (z + 1 == a.nz) ? 0 : z + 1;
+                // halo'd offsets of interior x = 0 in the rows (z, y), (z+1, y), (z, y+1)
+                const size_t c0 = (size_t)(y + 1) * hplane + (size_t)(z + 1) * hrow + 1;
+                const size_t cz = (size_t)(y + 1) * hplane + (size_t)(zp + 1) * hrow + 1;
+                const size_t c1 = c0 + hplane;
+                double2 pu = make_double2(0.0, 0.0), pw0 = pu, pw1 = pu, pv0 = pu, pv1 = pu;
+                if (in) {
+                    pu = *reinterpret_cast<const double2*>(a.Uh + c0 + 2 * e + 1);
+                    pw0 = *reinterpret_cast<const double2*>(a.Wh + c0 + 2 * e + 1);
+                    pw1 = *reinterpret_cast<const double2*>(a.Wh + cz + 2 * e + 1);
+                    if (!wb) pv0 = *reinterpret_cast<const double2*>(a.Vh + c0 + 2 * e + 1);
+                    if (!wt) pv1 = *reinterpret_cast<const double2*>(a.Vh + c1 + 2 * e + 1);
+                }
+                // interior 2e: .y of the previous item's pair
+                double u0 = __shfl_up_sync(full, pu.y, 1), w00 = __shfl_up_sync(full, pw0.y, 1);
+                double w10 = __shfl_up_sync(full, pw1.y, 1), v00 = __shfl_up_sync(full, pv0.y, 1);
+                double v10 = __shfl_up_sync(full, pv1.y, 1);
+                if (!in) continue;
+                if (lane == 0 || e == 0) {
+                    u0 = a.Uh[c0 + 2 * e];
+                    w00 = a.Wh[c0 + 2 * e];
+                    w10 = a.Wh[cz + 2 * e];
+                    if (!wb) v00 = a.Vh[c0 + 2 * e];
+                    if (!wt) v10 = a.Vh[c1 + 2 * e];
+                }
+                if (wb) v00 = a.vbot;
+                const double v01 = wb ? a.vbot : pv0.x;
+                if (wt) v10 = a.vtop;
+                const double v11 = wt ? a.vtop : pv1.x;
+                const double u1 = pu.x;
+                const double u2 = (e == m - 1) ? a.Uh[c0] : pu.y;
+                double s0 = __dmul_rn(__dsub_rn(u1, u0), a.inv_dx);
+                s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(w10, w00), a.inv_dz));
+                s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(v10, v00), idy));
+                double s1 = __dmul_rn(__dsub_rn(u2, u1), a.inv_dx);
+                s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(pw1.x, pw0.x), a.inv_dz));
+                s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(v11, v01), idy));
+                v[u] = make_double2(__dmul_rn(a.inv_dt, s0), __dmul_rn(a.inv_dt, s1));
+                if (a.Bout) {
+                    double* b = a.Bout + ((size_t)y * a.nz + z) * nx + 2 * e;
+                    b[0] = v[u].x;
+                    b[1] = v[u].y;
                 }
             }
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
-                const int idx = base + u * nthr;
+                const int idx = base + u * nthr + lane;
                 if (idx < total) {
                     const int r = idx / m, e = idx - r * m;
                     A[sidx<true>(r * rs + e)] = v[u];

@@ -109,11 +109,12 @@ struct ThomasArgs {
 constexpr int kThomasTile = 128;
 constexpr int kBlock = 8;  // planes loaded together (independent loads in flight)
 
+// One line: the CTA's block index `blk` within the buffer a.X (T storage).
 template <typename T>
-__global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
-    const int kb = blockIdx.x / a.tiles;  // row within this buffer
+__device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
+    const int kb = blk / a.tiles;  // row within this buffer
     const int kx = a.kx0 + kb;
-    const int slot = (blockIdx.x - kb * a.tiles) * kThomasTile + threadIdx.x;
+    const int slot = (blk - kb * a.tiles) * kThomasTile + threadIdx.x;
     if (slot >= a.nz) return;
     const int nz = a.nz, ny = a.ny, nh = a.nh, mzp = a.mzp;
     const int kz = a.kz_of_slot[slot];
@@ -184,6 +185,19 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
             }
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
+    thomas_line<T>(a, blockIdx.x);
+}
+
+// mixed storage in one launch: blocks [0, nblk64) solve the FP64 rows (a64), the
+// rest the FP32 rows (a32), so the few FP64 rows overlap the FP32 ones
+__global__ void __launch_bounds__(kThomasTile) k_thomas_mixed(const ThomasArgs a64, const ThomasArgs a32,
+                                                              int nblk64) {
+    if ((int)blockIdx.x < nblk64) thomas_line<double2>(a64, blockIdx.x);
+    else thomas_line<float2>(a32, blockIdx.x - nblk64);
 }
 
 template <typename K>
@@ -276,15 +290,20 @@ cudaError_t launch_zfft_t(const prj_plan* pl, int dir, void* X, int rows_per_pla
     return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_plane, cudaStream_t st) {
+ThomasArgs thomas_args(const prj_plan* pl, void* X, int kx0, int rows_per_plane) {
     const Geometry& g = pl->g;
-    if (rows_per_plane <= 0) return cudaSuccess;
     ThomasArgs t{};
     t.nz = g.nz; t.ny = g.ny; t.nh = g.nxh; t.mzp = g.mzp;
     t.tiles = (g.nz + kThomasTile - 1) / kThomasTile;
     t.nhb = rows_per_plane; t.kx0 = kx0;
     t.bands = pl->t.bands; t.piv = pl->t.piv; t.kz_of_slot = pl->kz_of_slot; t.X = X;
+    return t;
+}
+
+template <typename T>
+cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_plane, cudaStream_t st) {
+    if (rows_per_plane <= 0) return cudaSuccess;
+    const ThomasArgs t = thomas_args(pl, X, kx0, rows_per_plane);
     k_thomas<T><<<(unsigned)(rows_per_plane * t.tiles), kThomasTile, 0, st>>>(t);
     return cudaGetLastError();
 }
@@ -305,9 +324,13 @@ cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st) {
 }
 
 cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st) {
-    cudaError_t e = launch_thomas_t<double2>(pl, pl->spec, 0, pl->kxs, st);
-    if (e != cudaSuccess) return e;
-    return launch_thomas_t<float2>(pl, pl->spec32, pl->kxs, pl->g.nxh - pl->kxs, st);
+    const int rows32 = pl->g.nxh - pl->kxs;
+    if (rows32 <= 0) return launch_thomas_t<double2>(pl, pl->spec, 0, pl->kxs, st);
+    const ThomasArgs a64 = thomas_args(pl, pl->spec, 0, pl->kxs);
+    const ThomasArgs a32 = thomas_args(pl, pl->spec32, pl->kxs, rows32);
+    const int nblk64 = pl->kxs * a64.tiles;
+    k_thomas_mixed<<<(unsigned)(nblk64 + rows32 * a32.tiles), kThomasTile, 0, st>>>(a64, a32, nblk64);
+    return cudaGetLastError();
 }
 
 }  // namespace prj
