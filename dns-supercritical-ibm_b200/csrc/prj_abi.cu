@@ -189,6 +189,7 @@ void free_plan_buffers(prj_plan* pl) {
     pl->xd.ok = pl->zd.ok = false;
     dfree(pl->spec);
     dfree(pl->stat_buf);
+    dfree(pl->vd_pad);
     dfree(pl->host_stage);
     pl->host_stage_elems = 0;
 }
@@ -722,6 +723,7 @@ const char* prj_stage_name(int stage) {
     case prj::kStThomas: return "k_thomas";
     case prj::kStZfftInv: return "k_zfft_inv";
     case prj::kStResidual: return "k_residual";
+    case prj::kStVdRhs: return "k_vd_rhs";
     default: return "";
     }
 }
@@ -790,6 +792,7 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
             stats->div_maxabs = h[0];
             stats->p_maxabs = h[1];
             stats->min_pivot = plan->min_pivot;
+            stats->rho_min = 0.0;
             if (mode == PRJ_MODE_FP32_REFINE) {
                 stats->refine_iters = plan->mixed_iters;
                 stats->fp64_lines = plan->kxs_mixed * plan->g.nz;
@@ -800,6 +803,111 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
                 stats->last_update_rel = 0.0;
             }
         }
+        if (!std::isfinite(h[0]) || !std::isfinite(h[1])) return fail(PRJ_ERR_NUMERIC, "NaN detected in the projection");
+    }
+    return PRJ_OK;
+}
+
+int prj_vd_metric_from_yu(int ny, const double* yu, double* inv_dy_p_pad) {
+    if (ny < 2 || !yu || !inv_dy_p_pad) return fail(PRJ_ERR_ARG, "need ny >= 2 and non-NULL arrays");
+    // yp_pad = [2 yu_0 - yp_0, yp_0 .. yp_{ny-1}, 2 yu_ny - yp_{ny-1}], calc_bands.py:273, :276
+    std::vector<double> yp((size_t)ny + 2);
+    for (int k = 0; k < ny; k++) yp[(size_t)k + 1] = (yu[k] + yu[k + 1]) / 2;
+    yp[0] = 2 * yu[0] - yp[1];
+    yp[(size_t)ny + 1] = 2 * yu[ny] - yp[(size_t)ny];
+    for (int i = 0; i <= ny; i++) inv_dy_p_pad[i] = 1. / (yp[(size_t)i + 1] - yp[(size_t)i]);
+    return PRJ_OK;
+}
+
+int prj_plan_set_vd_metric(prj_plan* plan, const double* inv_dy_p_pad) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!inv_dy_p_pad) return fail(PRJ_ERR_ARG, "inv_dy_p_pad is NULL");
+    for (int i = 0; i <= plan->g.ny; i++)
+        if (!std::isfinite(inv_dy_p_pad[i])) return fail(PRJ_ERR_ARG, "inv_dy_p_pad[%d] is not finite", i);
+    DeviceGuard dg(plan->device);
+    const size_t bytes = (size_t)(plan->g.ny + 1) * sizeof(double);
+    if (!plan->vd_pad) {
+        CK(cudaMalloc((void**)&plan->vd_pad, bytes), "cudaMalloc(inv_dy_p_pad)");
+        plan->device_bytes += bytes;
+    }
+    CK(cudaMemcpy(plan->vd_pad, inv_dy_p_pad, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(inv_dy_p_pad)");
+    return PRJ_OK;
+}
+
+int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_Vh, const double* d_Wh, double* d_U,
+                           double* d_V, double* d_W, double* d_P, const prj_step_params* params,
+                           const prj_vd_fields* vd, int mode, prj_stats* stats, void* stream) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!plan->has_metrics) return fail(PRJ_ERR_STATE, "plan was created without inv_dy_p / dPdy (Poisson-only)");
+    if (!plan->vd_pad) return fail(PRJ_ERR_STATE, "no inv_dy_p_pad: call prj_plan_set_vd_metric first");
+    if (!d_Uh || !d_Vh || !d_Wh || !d_U || !d_V || !d_W || !d_P || !params || !vd)
+        return fail(PRJ_ERR_ARG, "NULL array, params or fields");
+    if (!vd->rho || !vd->P_now || !vd->P_old || !vd->div_now || !vd->P_next)
+        return fail(PRJ_ERR_ARG, "NULL variable-density field");
+    if (!(params->dt > 0) || !std::isfinite(params->dt)) return fail(PRJ_ERR_ARG, "dt=%g must be finite and positive", params->dt);
+    if (mode != PRJ_MODE_FP64 && mode != PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_ARG, "unknown mode %d", mode);
+    if (mode == PRJ_MODE_FP32_REFINE && (rc = mixed_supported(plan))) return rc;
+    {
+        const void* outs[5] = {d_U, d_V, d_W, d_P, vd->P_next};
+        const void* ins[7] = {d_Uh, d_Vh, d_Wh, vd->rho, vd->P_now, vd->P_old, vd->div_now};
+        for (const void* o : outs) {
+            for (const void* in : ins)
+                if (o == in) return fail(PRJ_ERR_ARG, "an output array aliases an input array");
+        }
+        for (int a = 0; a < 5; a++)
+            for (int b = a + 1; b < 5; b++)
+                if (outs[a] == outs[b]) return fail(PRJ_ERR_ARG, "two output arrays alias");
+    }
+    DeviceGuard dg(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    prj::StepScalars sc{};
+    sc.dt = params->dt;
+    sc.inv_dt = 1.0 / params->dt;
+    sc.wall[0] = params->wall_U_bot; sc.wall[1] = params->wall_V_bot; sc.wall[2] = params->wall_W_bot;
+    sc.wall[3] = params->wall_U_top; sc.wall[4] = params->wall_V_top; sc.wall[5] = params->wall_W_top;
+    const prj::VdFields f{vd->rho, vd->P_now, vd->P_old, vd->div_now, vd->P_next};
+    unsigned long long* slot = reinterpret_cast<unsigned long long*>(plan->stat_buf + prj::kStatRhoSlot);
+    {
+        StageTimer tm(plan, prj::kStVdRhs, st);
+        CK(prj::launch_vd_rho_min(plan, vd->rho, slot, st), "rho_min");
+        CK(prj::launch_vd_rhs(plan, d_Uh, d_Vh, d_Wh, f, sc, slot, d_P, st), "variable-density right-hand side");
+    }
+    if (mode == PRJ_MODE_FP32_REFINE) {
+        if ((rc = run_mixed_poisson(plan, d_P, st))) return rc;
+    } else if ((rc = run_poisson(plan, d_P, st))) {
+        return rc;
+    }
+    {
+        StageTimer tm(plan, prj::kStCorrect, st);
+        CK(prj::launch_vd_correction(plan, d_P, d_Uh, d_Vh, d_Wh, f, sc, slot, d_U, d_V, d_W, st),
+           "variable-density correction");
+    }
+    if (stats || params->compute_stats) {
+        {
+            StageTimer tm(plan, prj::kStStats, st);
+            CK(prj::launch_stats(plan, d_U, d_V, d_W, d_P, plan->stat_buf + 2, st), "stats");
+        }
+        double h[6] = {-1, -1, 0, 0, 0, 0};
+        CK(cudaMemcpyAsync(h, plan->stat_buf + 2, 6 * sizeof(double), cudaMemcpyDeviceToHost, st), "stats copy");
+        CK(cudaStreamSynchronize(st), "stats sync");
+        int dev_err = 0;
+        std::memcpy(&dev_err, &h[prj::kStatErrSlot - 2], sizeof(int));
+        if (dev_err) return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
+        unsigned long long ord = 0;
+        std::memcpy(&ord, &h[prj::kStatRhoSlot - 2], sizeof(ord));
+        const double rmin = prj::vd_rho_min_host(ord);
+        if (stats) {
+            stats->div_maxabs = h[0];
+            stats->p_maxabs = h[1];
+            stats->min_pivot = plan->min_pivot;
+            stats->refine_iters = mode == PRJ_MODE_FP32_REFINE ? plan->mixed_iters : 0;
+            stats->fp64_lines = (mode == PRJ_MODE_FP32_REFINE ? plan->kxs_mixed : plan->g.nxh) * plan->g.nz;
+            stats->last_update_rel = (mode == PRJ_MODE_FP32_REFINE && h[3] > 0) ? std::sqrt(h[2] / h[3]) : 0.0;
+            stats->rho_min = rmin;
+        }
+        if (!(rmin > 0)) return fail(PRJ_ERR_NUMERIC, "rho_min=%g must be positive", rmin);
         if (!std::isfinite(h[0]) || !std::isfinite(h[1])) return fail(PRJ_ERR_NUMERIC, "NaN detected in the projection");
     }
     return PRJ_OK;

@@ -5,6 +5,9 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstring>
+
 #include <vector>
 
 #include "fft_device.cuh"
@@ -67,7 +70,7 @@ namespace prj {
 // stage ids of the per-kernel timing record
 enum Stage {
     kStFwdX = 0, kStZSolve = 1, kStBwdX = 2, kStCorrect = 3, kStStats = 4,
-    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kStResidual = 8, kNumStages = 12
+    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kStResidual = 8, kStVdRhs = 9, kNumStages = 12
 };
 
 struct StageRecord {
@@ -109,6 +112,7 @@ struct prj_plan {
     int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
     bool use_pass = true;         // compile-time pass-plan FFT kernels where the length has one
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
+    double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
 };
 
 namespace prj {
@@ -157,8 +161,26 @@ cudaError_t launch_plane_mean(const prj_plan* pl, const double* P, double* pbar,
 cudaError_t launch_residual(const prj_plan* pl, const double* B, const double* P, const double* pbar, double* R,
                             cudaStream_t st);
 
-// stat_buf slots: [0] min pivot (bits), [2] max|div u|, [3] max|P|, [6] device error word
+// stat_buf slots: [0] min pivot (bits), [2] max|div u|, [3] max|P|, [6] device error word,
+// [7] rho_min of the variable-density step (order-preserving integer image)
 constexpr int kStatErrSlot = 6;
+constexpr int kStatRhoSlot = 7;
+
+// variable-density step (prj_vd.cu): halo'd fields supplied by the caller
+struct VdFields {
+    const double* rho;
+    const double* P_now;
+    const double* P_old;
+    const double* div_now;
+    double* P_next;
+};
+cudaError_t launch_vd_rho_min(const prj_plan* pl, const double* rho, unsigned long long* slot, cudaStream_t st);
+cudaError_t launch_vd_rhs(const prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, const VdFields& f,
+                          const StepScalars& sc, const unsigned long long* slot, double* P, cudaStream_t st);
+cudaError_t launch_vd_correction(const prj_plan* pl, const double* P, const double* Uh, const double* Vh,
+                                 const double* Wh, const VdFields& f, const StepScalars& sc,
+                                 const unsigned long long* slot, double* U, double* V, double* W, cudaStream_t st);
+double vd_rho_min_host(unsigned long long o);
 
 // Sets the calling thread's prj_last_error_string() message and returns code.
 int record_error(int code, const char* msg);

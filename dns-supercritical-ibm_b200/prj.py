@@ -52,6 +52,7 @@ EXPORTS = (
     "prj_poisson_fp64_noalloc", "prj_poisson_mixed",
     "prj_batch_create", "prj_batch_launch", "prj_batch_destroy",
     "prj_plan_get_tuning", "prj_plan_set_tuning",
+    "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
 )
 
 BANDS_REFERENCE = 0
@@ -67,7 +68,8 @@ class PrjError(RuntimeError):
 class Stats(ctypes.Structure):
     _fields_ = [("div_maxabs", ctypes.c_double), ("p_maxabs", ctypes.c_double),
                 ("min_pivot", ctypes.c_double), ("refine_iters", ctypes.c_int),
-                ("fp64_lines", ctypes.c_int), ("last_update_rel", ctypes.c_double)]
+                ("fp64_lines", ctypes.c_int), ("last_update_rel", ctypes.c_double),
+                ("rho_min", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -78,6 +80,11 @@ class Tuning(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VdFields(ctypes.Structure):
+    _fields_ = [("rho", ctypes.c_void_p), ("P_now", ctypes.c_void_p), ("P_old", ctypes.c_void_p),
+                ("div_now", ctypes.c_void_p), ("P_next", ctypes.c_void_p)]
 
 
 class StepParams(ctypes.Structure):
@@ -131,6 +138,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_batch_destroy.argtypes = [_vp]
     L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
+    L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
+    L.prj_plan_set_vd_metric.argtypes = [_vp, _dp]
+    L.prj_projection_step_vd.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams),
+                                         ctypes.POINTER(VdFields), i, ctypes.POINTER(Stats), _vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.prj_last_error_string.restype = ctypes.c_char_p
@@ -189,6 +200,14 @@ def bands(yu, mode="reference"):
     return tuple(out)
 
 
+def vd_metric(yu):
+    """inv_dy_p_pad (ny+1) of the variable-density step (prj_vd_metric_from_yu; host-only)."""
+    yu = _arr(yu)
+    out = np.zeros(yu.size)
+    _check(load_library().prj_vd_metric_from_yu(yu.size - 1, _p(yu), _p(out)))
+    return out
+
+
 def metrics(yu):
     """(inv_dy_p, dPdy_lo, dPdy_hi) from the face grid (prj_metrics_from_yu; host-only)."""
     yu = _arr(yu)
@@ -226,7 +245,13 @@ class Plan:
     def from_yu(cls, nx, nz, dx, dz, yu, band_mode="reference", device=0):
         """Build bands and metrics from the face grid ``yu`` (ny+1 values)."""
         yu = np.asarray(yu, dtype=np.float64)
-        return cls(nx, nz, len(yu) - 1, dx, dz, bands(yu, band_mode), metrics(yu), device)
+        plan = cls(nx, nz, len(yu) - 1, dx, dz, bands(yu, band_mode), metrics(yu), device)
+        plan.set_vd_metric(vd_metric(yu))
+        return plan
+
+    def set_vd_metric(self, inv_dy_p_pad):
+        """inv_dy_p_pad (ny+1) for projection_step_vd (prj_plan_set_vd_metric)."""
+        _check(load_library().prj_plan_set_vd_metric(self.handle, _p(_arr(inv_dy_p_pad, self.grid.ny + 1))))
 
     def close(self):
         if getattr(self, "_h", None):
@@ -339,6 +364,30 @@ class Plan:
                 raise ValueError("P must be a Fortran-ordered float64 array of shape (nx, nz, ny)")
             _check(L.prj_projection_step_host(self.handle, _p(Uh), _p(Vh), _p(Wh), _p(U), _p(V), _p(W), _p(P),
                                               ctypes.byref(par), mode, sp))
+        return st.as_dict() if stats else None
+
+
+    def projection_step_vd(self, Uh, Vh, Wh, rho, P_now, P_old, div_now, U, V, W, P, P_next, dt, mode=MODE_FP64,
+                           wall=(0.0,) * 6, stats=True, stream=None):
+        """Variable-density projection (prj_projection_step_vd).  Torch CUDA tensors: halo'd
+        [y+2, z+2, x+2] for Uh..W, rho, P_now, P_old, div_now, P_next; P [y, z, x].  The caller
+        rotates P_old <- P_now <- P_next afterwards.  Returns a Stats dict (or None)."""
+        g = self.grid
+        L = load_library()
+        torch = _torch()
+        hs = (g.ny + 2, g.nz + 2, g.nx + 2)
+        for t in (Uh, Vh, Wh, rho, P_now, P_old, div_now, U, V, W, P_next):
+            if not (_is_tensor(t) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and tuple(t.shape) == hs):
+                raise ValueError(f"halo'd fields must be contiguous float64 CUDA tensors of shape {hs}")
+        if not (P.is_cuda and P.dtype == torch.float64 and P.is_contiguous() and tuple(P.shape) == (g.ny, g.nz, g.nx)):
+            raise ValueError("P must be a contiguous float64 CUDA tensor of shape (ny, nz, nx)")
+        par = StepParams(float(dt), *[float(w) for w in wall], 1 if stats else 0)
+        st = Stats()
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+        f = VdFields(rho.data_ptr(), P_now.data_ptr(), P_old.data_ptr(), div_now.data_ptr(), P_next.data_ptr())
+        _check(L.prj_projection_step_vd(self.handle, ptr(Uh), ptr(Vh), ptr(Wh), ptr(U), ptr(V), ptr(W), ptr(P),
+                                        ctypes.byref(par), ctypes.byref(f), mode,
+                                        ctypes.byref(st) if stats else None, _stream_ptr(stream)))
         return st.as_dict() if stats else None
 
 

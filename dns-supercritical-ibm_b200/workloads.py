@@ -144,3 +144,45 @@ def rough_projection_inputs(nx: int, ny: int, nz: int, seed: int = 5, sigma: flo
     for f in (Uh, Vh, Wh):
         f[1:-1, 1:-1, 1:-1][solid] = 0.0
     return Uh, Vh, Wh, yu, dx, dz, solid
+
+
+def fill_halos(F: np.ndarray) -> np.ndarray:
+    """Fill the halos of a halo'd [x+2, z+2, y+2] field in place: periodic images in x and z,
+    and the wall ghost planes y = -1, ny as copies of y = 0, ny-1 (the P_per rule of
+    mod_cfd_subroutines.f90:1087-1118).  Returns F."""
+    F[0, :, :] = F[-2, :, :]
+    F[-1, :, :] = F[1, :, :]
+    F[:, 0, :] = F[:, -2, :]
+    F[:, -1, :] = F[:, 1, :]
+    F[:, :, 0] = F[:, :, 1]
+    F[:, :, -1] = F[:, :, -2]
+    return F
+
+
+def vd_inputs(nx: int, ny: int, nz: int, seed: int = 4, beta: float = 2.0, rho_const=None):
+    """Inputs of the variable-density projection: the channel predictor of projection_inputs,
+    a density rho(y) = 1 - 0.6 (1 - (y-1)^2) (light core, dense walls) times 1 + N(0, 0.05),
+    pressures P_now, P_old ~ N(0, 0.01) and div_now ~ N(0, 0.01), all halo'd with filled halos
+    (draws from default_rng(seed + 1) after the predictor's default_rng(seed)).  With rho_const
+    the density is that constant.
+
+    Returns (Uh, Vh, Wh, rho, P_now, P_old, div_now, yu, dx, dz)."""
+    Uh, Vh, Wh, yu, dx, dz = projection_inputs(nx, ny, nz, beta=beta, seed=seed)
+    yp = (yu[:-1] + yu[1:]) / 2
+    rng = np.random.default_rng(seed + 1)
+    shape = (nx + 2, nz + 2, ny + 2)
+    rho = np.zeros(shape, order="F")
+    if rho_const is None:
+        rho[1:-1, 1:-1, 1:-1] = (1.0 - 0.6 * (1.0 - (yp[None, None, :] - 1.0) ** 2)) * (
+            1.0 + rng.normal(0.0, 0.05, size=(nx, nz, ny)))
+    else:
+        rho[1:-1, 1:-1, 1:-1] = rho_const
+    P_now = np.zeros(shape, order="F")
+    P_old = np.zeros(shape, order="F")
+    div_now = np.zeros(shape, order="F")
+    P_now[1:-1, 1:-1, 1:-1] = rng.normal(0.0, 0.01, size=(nx, nz, ny))
+    P_old[1:-1, 1:-1, 1:-1] = rng.normal(0.0, 0.01, size=(nx, nz, ny))
+    div_now[1:-1, 1:-1, 1:-1] = rng.normal(0.0, 0.01, size=(nx, nz, ny))
+    for F in (rho, P_now, P_old, div_now):
+        fill_halos(F)
+    return Uh, Vh, Wh, rho, P_now, P_old, div_now, yu, dx, dz

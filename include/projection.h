@@ -57,6 +57,7 @@ typedef struct prj_stats {
     int refine_iters;       /* refinement iterations used (0 for FP64) */
     int fp64_lines;         /* spectral lines solved in FP64 by the mixed path */
     double last_update_rel; /* rel-L2 of the last refinement update (mixed path) */
+    double rho_min;         /* variable-density step: min rho over the interior (MCS:476-486); else 0 */
 } prj_stats;
 
 /* Scalars of one projection step (update_vars / build_vars arguments). */
@@ -136,6 +137,38 @@ int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h
  * nx/2 and nz).  Asynchronous.
  */
 int prj_poisson_mixed(prj_plan* plan, double* d_P, void* stream);
+
+/*
+ * Variable-density projection (the reference's use_incompressible = .false.
+ * branch).  The Poisson operator is the plan's constant-coefficient one; the
+ * right-hand side is MCS:538-573 and the correction MCS:1153-1197 (MCS =
+ * src/mod_cfd_subroutines.f90):
+ *   rho_min = min rho over the interior,
+ *   RHS     = rho_min/dt (div u_hat - div_now) + the density-weighted Laplacian
+ *             of Ps = 2 P_now - P_old,
+ *   u       = u_hat - dt grad(P/rho_min + (avg 1/rho - 1/rho_min) Ps).
+ * rho, P_now, P_old and div_now are device arrays in the halo'd layout with
+ * their halos filled by the caller (periodic x/z images, wall ghost planes),
+ * read as given.  P_next (halo'd, device) receives the new pressure with
+ * periodic halos and wall ghost planes P(-1) = P(0), P(ny) = P(ny-1) (P_per,
+ * MCS:1087-1118): the caller's next P_now.  The reference copies P_now to
+ * P_old and P_per to P_now after each step (MCS:1199-1221); callers of this
+ * function rotate the three pointers instead.  No output may alias an input.
+ * Needs inv_dy_p_pad (ny+1 entries, calc_bands.py:273-276; built by
+ * prj_vd_metric_from_yu) set once per plan with prj_plan_set_vd_metric.
+ */
+typedef struct prj_vd_fields {
+    const double* rho;
+    const double* P_now;
+    const double* P_old;
+    const double* div_now;
+    double* P_next;
+} prj_vd_fields;
+int prj_vd_metric_from_yu(int ny, const double* yu, double* inv_dy_p_pad);
+int prj_plan_set_vd_metric(prj_plan* plan, const double* inv_dy_p_pad);
+int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_Vh, const double* d_Wh,
+                           double* d_U, double* d_V, double* d_W, double* d_P, const prj_step_params* params,
+                           const prj_vd_fields* vd, int mode, prj_stats* stats, void* stream);
 
 /*
  * Batched solves: one CUDA graph holding every case (case i solves plans[i] in

@@ -470,3 +470,158 @@ int orc_projection(int nx, int nz, int ny, double dx, double dz, double dt,
     if (rc) return rc;
     return orc_correction(nx, nz, ny, dx, dz, dt, dPdy_lo, dPdy_hi, P, Uh, Vh, Wh, wall, U, V, W, nthreads);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Variable-density projection (use_incompressible = .false.)                */
+/* ------------------------------------------------------------------------- */
+
+double orc_rho_min(int nx, int nz, int ny, const double* rho, int nthreads) {
+    set_threads(nthreads);
+    double m = 1e20; /* mod_cfd_subroutines.f90:476 */
+#pragma omp parallel for schedule(static) reduction(min : m)
+    for (long jk = 0; jk < (long)nz * ny; jk++) {
+        int j = (int)(jk % nz), k = (int)(jk / nz);
+        for (int i = 0; i < nx; i++) {
+            double r = rho[HIDX(i, j, k)];
+            if (r < m) m = r;
+        }
+    }
+    return m;
+}
+
+int orc_vd_metric_from_yu(int ny, const double* yu, double* inv_dy_p_pad) {
+    if (ny < 2 || !yu || !inv_dy_p_pad) return -1;
+    /* yp_pad = [2 yu_0 - yp_0, yp_0 .. yp_{ny-1}, 2 yu_ny - yp_{ny-1}], calc_bands.py:273, :276 */
+    double* yp_pad = (double*)malloc((size_t)(ny + 2) * sizeof(double));
+    if (!yp_pad) return -3;
+    for (int k = 0; k < ny; k++) yp_pad[k + 1] = (yu[k] + yu[k + 1]) / 2;
+    yp_pad[0] = 2 * yu[0] - yp_pad[1];
+    yp_pad[ny + 1] = 2 * yu[ny] - yp_pad[ny];
+    for (int i = 0; i <= ny; i++) inv_dy_p_pad[i] = 1. / (yp_pad[i + 1] - yp_pad[i]);
+    free(yp_pad);
+    return 0;
+}
+
+/* 2 P_now - P_old at a halo'd index */
+static inline double ps_at(const double* Pn, const double* Po, size_t h) { return 2 * Pn[h] - Po[h]; }
+
+/* 1 - rho_min (0.5/rho_a + 0.5/rho_b) */
+static inline double rho_w(double rho_min, double ra, double rb) { return 1.0 - rho_min * (0.5 / ra + 0.5 / rb); }
+
+int orc_vd_rhs(int nx, int nz, int ny, double dx, double dz, double dt,
+               const double* inv_dy_p, const double* inv_dy_p_pad,
+               const double* Uh, const double* Vh, const double* Wh, double vbot, double vtop,
+               const double* rho, const double* P_now, const double* P_old, const double* div_now,
+               double rho_min, double* P, int nthreads) {
+    if (nx < 1 || nz < 1 || ny < 2 || !inv_dy_p || !inv_dy_p_pad || !Uh || !Vh || !Wh || !rho || !P_now ||
+        !P_old || !div_now || !P)
+        return -1;
+    set_threads(nthreads);
+    const double inv_dx = 1.0 / dx, inv_dz = 1.0 / dz, inv_dtmax = 1.0 / dt;
+    const double inv_dx2 = inv_dx * inv_dx, inv_dz2 = inv_dz * inv_dz;
+#pragma omp parallel for schedule(static)
+    for (long jk = 0; jk < (long)nz * ny; jk++) {
+        int j = (int)(jk % nz), k = (int)(jk / nz);
+        int jp = (j + 1 == nz) ? 0 : j + 1;
+        for (int i = 0; i < nx; i++) {
+            int ip = (i + 1 == nx) ? 0 : i + 1;
+            const size_t h = HIDX(i, j, k);
+            double vp = vh_face(nx, nz, Vh, i, j, k + 1, ny, vbot, vtop);
+            double v0 = vh_face(nx, nz, Vh, i, j, k, ny, vbot, vtop);
+            /* the stencil of P_now, P_old and rho reads the caller's halos, MCS:543-556 */
+            double Ps_00 = ps_at(P_now, P_old, h);
+            double Ps_xp = ps_at(P_now, P_old, HIDX(i + 1, j, k)), Ps_xm = ps_at(P_now, P_old, HIDX(i - 1, j, k));
+            double Ps_zp = ps_at(P_now, P_old, HIDX(i, j + 1, k)), Ps_zm = ps_at(P_now, P_old, HIDX(i, j - 1, k));
+            double Ps_yp = ps_at(P_now, P_old, HIDX(i, j, k + 1)), Ps_ym = ps_at(P_now, P_old, HIDX(i, j, k - 1));
+            double r0 = rho[h];
+            double rho_xp = rho_w(rho_min, rho[HIDX(i + 1, j, k)], r0), rho_xm = rho_w(rho_min, rho[HIDX(i - 1, j, k)], r0);
+            double rho_zp = rho_w(rho_min, rho[HIDX(i, j + 1, k)], r0), rho_zm = rho_w(rho_min, rho[HIDX(i, j - 1, k)], r0);
+            double rho_yp = rho_w(rho_min, rho[HIDX(i, j, k + 1)], r0), rho_ym = rho_w(rho_min, rho[HIDX(i, j, k - 1)], r0);
+            /* MCS:558-564 */
+            double dv = ((Uh[HIDX(ip, j, k)] - Uh[h]) * inv_dx + (Wh[HIDX(i, jp, k)] - Wh[h]) * inv_dz +
+                         (vp - v0) * inv_dy_p[k]);
+            P[PIDX(i, j, k)] = inv_dtmax * dv * rho_min - inv_dtmax * rho_min * div_now[h] +
+                               ((rho_xp * (Ps_xp - Ps_00) - rho_xm * (Ps_00 - Ps_xm)) * inv_dx2 +
+                                (rho_zp * (Ps_zp - Ps_00) - rho_zm * (Ps_00 - Ps_zm)) * inv_dz2 +
+                                (rho_yp * (Ps_yp - Ps_00) * inv_dy_p_pad[k + 1] -
+                                 rho_ym * (Ps_00 - Ps_ym) * inv_dy_p_pad[k]) * inv_dy_p[k]);
+        }
+    }
+    return 0;
+}
+
+int orc_vd_correction(int nx, int nz, int ny, double dx, double dz, double dt,
+                      const double* dPdy_lo, const double* dPdy_hi, const double* P,
+                      const double* Uh, const double* Vh, const double* Wh, const double* wall,
+                      const double* rho, const double* P_now, const double* P_old, double rho_min,
+                      double* U, double* V, double* W, double* P_next, int nthreads) {
+    if (nx < 1 || nz < 1 || ny < 2 || !dPdy_lo || !dPdy_hi || !P || !Uh || !Vh || !Wh || !wall || !rho ||
+        !P_now || !P_old || !U || !V || !W || !P_next)
+        return -1;
+    set_threads(nthreads);
+    const double inv_dx = 1.0 / dx, inv_dz = 1.0 / dz, dtmax = dt;
+    const double inv_rho_min = 1.0 / rho_min;
+    const int kmin_Vhat = 1;
+    /* P_per: P with periodic x/z halos and the wall ghost planes P(-1) = P(0),
+     * P(ny) = P(ny-1), MCS:1087-1118; it becomes P_next (the caller's next P_now) */
+#pragma omp parallel for schedule(static)
+    for (long jk = 0; jk < (long)(nz + 2) * (ny + 2); jk++) {
+        int j = (int)(jk % (nz + 2)) - 1, k = (int)(jk / (nz + 2)) - 1;
+        int js = (j < 0) ? nz - 1 : (j == nz ? 0 : j);
+        int ks = (k < 0) ? 0 : (k == ny ? ny - 1 : k);
+        for (int i = -1; i <= nx; i++) {
+            int is = (i < 0) ? nx - 1 : (i == nx ? 0 : i);
+            P_next[HIDX(i, j, k)] = P[PIDX(is, js, ks)];
+        }
+    }
+    /* MCS:1153-1197 */
+#pragma omp parallel for schedule(static)
+    for (long jk = 0; jk < (long)nz * ny; jk++) {
+        int j = (int)(jk % nz), k = (int)(jk / nz);
+        for (int i = 0; i < nx; i++) {
+            const size_t h = HIDX(i, j, k);
+            double inv_rho_now, P_fwd, P_bwd;
+            size_t hm = HIDX(i - 1, j, k);
+            inv_rho_now = 0.5 / rho[h] + 0.5 / rho[hm];
+            P_fwd = P_next[h] * inv_rho_min + (inv_rho_now - inv_rho_min) * (2 * P_now[h] - P_old[h]);
+            P_bwd = P_next[hm] * inv_rho_min + (inv_rho_now - inv_rho_min) * (2 * P_now[hm] - P_old[hm]);
+            U[h] = Uh[h] - dtmax * (P_fwd - P_bwd) * inv_dx;
+            hm = HIDX(i, j - 1, k);
+            inv_rho_now = 0.5 / rho[h] + 0.5 / rho[hm];
+            P_fwd = P_next[h] * inv_rho_min + (inv_rho_now - inv_rho_min) * (2 * P_now[h] - P_old[h]);
+            P_bwd = P_next[hm] * inv_rho_min + (inv_rho_now - inv_rho_min) * (2 * P_now[hm] - P_old[hm]);
+            W[h] = Wh[h] - dtmax * (P_fwd - P_bwd) * inv_dz;
+            if (k >= kmin_Vhat) {
+                hm = HIDX(i, j, k - 1);
+                inv_rho_now = 0.5 / rho[h] + 0.5 / rho[hm];
+                P_fwd = P_next[h] * inv_rho_min + (inv_rho_now - inv_rho_min) * (2 * P_now[h] - P_old[h]);
+                P_bwd = P_next[hm] * inv_rho_min + (inv_rho_now - inv_rho_min) * (2 * P_now[hm] - P_old[hm]);
+                V[h] = Vh[h] - dtmax * (dPdy_hi[k] * P_fwd + dPdy_lo[k] * P_bwd);
+            }
+        }
+    }
+    fill_halos(nx, nz, ny, U, -1, wall[0], wall[3]);
+    fill_halos(nx, nz, ny, V, 0, wall[1], wall[4]);
+    fill_halos(nx, nz, ny, W, -1, wall[2], wall[5]);
+    return 0;
+}
+
+int orc_projection_vd(int nx, int nz, int ny, double dx, double dz, double dt,
+                      const double* a, const double* b, const double* c,
+                      const double* a00, const double* b00, const double* c00,
+                      const double* inv_dy_p, const double* dPdy_lo, const double* dPdy_hi,
+                      const double* inv_dy_p_pad, const double* Uh, const double* Vh, const double* Wh,
+                      const double* wall, const double* rho, const double* P_now, const double* P_old,
+                      const double* div_now, double* U, double* V, double* W, double* P, double* P_next,
+                      double* rho_min_out, int nthreads) {
+    if (!wall || !rho) return -1;
+    const double rho_min = orc_rho_min(nx, nz, ny, rho, nthreads);
+    if (rho_min_out) *rho_min_out = rho_min;
+    int rc = orc_vd_rhs(nx, nz, ny, dx, dz, dt, inv_dy_p, inv_dy_p_pad, Uh, Vh, Wh, wall[1], wall[4], rho, P_now,
+                        P_old, div_now, rho_min, P, nthreads);
+    if (rc) return rc;
+    rc = orc_poisson(nx, nz, ny, dx, dz, a, b, c, a00, b00, c00, P, NULL, nthreads);
+    if (rc) return rc;
+    return orc_vd_correction(nx, nz, ny, dx, dz, dt, dPdy_lo, dPdy_hi, P, Uh, Vh, Wh, wall, rho, P_now, P_old,
+                             rho_min, U, V, W, P_next, nthreads);
+}

@@ -97,6 +97,39 @@ int orc_projection(int nx, int nz, int ny, double dx, double dz, double dt,
 int orc_r2hc(int n, const double* x, double* hc);
 int orc_hc2r(int n, const double* hc, double* x);
 
+/* Variable-density pressure splitting (use_incompressible = .false.).
+ *   orc_rho_min            min of rho over the interior, mod_cfd_subroutines.f90:476-486
+ *   orc_vd_metric_from_yu  inv_dy_p_pad (ny+1 entries), calc_bands.py:273, :276
+ *   orc_vd_rhs             RHS of the constant-coefficient Poisson equation, MCS:538-573:
+ *                          rho_min/dt (div u_hat - div_now) + the density-weighted
+ *                          Laplacian of Ps = 2 P_now - P_old (caller-filled halos of rho,
+ *                          P_now, P_old are read as given)
+ *   orc_vd_correction      u = u_hat - dt grad(P/rho_min + (1/rho - 1/rho_min) Ps),
+ *                          MCS:1153-1197, with the boundary fill :1223-1243; P_next
+ *                          receives P_per (MCS:1087-1118), the caller's next P_now
+ *   orc_projection_vd      the three in sequence around orc_poisson
+ * rho, P_now, P_old, div_now, P_next are halo'd. */
+double orc_rho_min(int nx, int nz, int ny, const double* rho, int nthreads);
+int orc_vd_metric_from_yu(int ny, const double* yu, double* inv_dy_p_pad);
+int orc_vd_rhs(int nx, int nz, int ny, double dx, double dz, double dt,
+               const double* inv_dy_p, const double* inv_dy_p_pad,
+               const double* Uh, const double* Vh, const double* Wh, double vbot, double vtop,
+               const double* rho, const double* P_now, const double* P_old, const double* div_now,
+               double rho_min, double* P, int nthreads);
+int orc_vd_correction(int nx, int nz, int ny, double dx, double dz, double dt,
+                      const double* dPdy_lo, const double* dPdy_hi, const double* P,
+                      const double* Uh, const double* Vh, const double* Wh, const double* wall,
+                      const double* rho, const double* P_now, const double* P_old, double rho_min,
+                      double* U, double* V, double* W, double* P_next, int nthreads);
+int orc_projection_vd(int nx, int nz, int ny, double dx, double dz, double dt,
+                      const double* a, const double* b, const double* c,
+                      const double* a00, const double* b00, const double* c00,
+                      const double* inv_dy_p, const double* dPdy_lo, const double* dPdy_hi,
+                      const double* inv_dy_p_pad, const double* Uh, const double* Vh, const double* Wh,
+                      const double* wall, const double* rho, const double* P_now, const double* P_old,
+                      const double* div_now, double* U, double* V, double* W, double* P, double* P_next,
+                      double* rho_min_out, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

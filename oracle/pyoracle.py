@@ -186,6 +186,12 @@ class COracle:
         L.orc_bands_from_yu.argtypes = [i, _dp, i, _dp, _dp, _dp, _dp, _dp, _dp]
         L.orc_metrics_from_yu.argtypes = [i, _dp, _dp, _dp, _dp]
         L.orc_mk_P_abc.argtypes = [i, _dp, i, _dp, _dp, _dp]
+        L.orc_rho_min.argtypes = [i, i, i, _dp, i]
+        L.orc_rho_min.restype = d
+        L.orc_vd_metric_from_yu.argtypes = [i, _dp, _dp]
+        L.orc_vd_rhs.argtypes = [i, i, i, d, d, d, _dp, _dp, _dp, _dp, _dp, d, d, _dp, _dp, _dp, _dp, d, _dp, i]
+        L.orc_vd_correction.argtypes = [i, i, i, d, d, d, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, d,
+                                        _dp, _dp, _dp, _dp, i]
 
     def poisson(self, rhs, dx, dz, bands6, nthreads=0):
         """Returns (P, min_pivot); rhs [x, z, y] is not modified."""
@@ -235,6 +241,44 @@ class COracle:
         P, _ = self.poisson(P, dx, dz, b6, nthreads)
         U, V, W = self.correction(P, Uh, Vh, Wh, dx, dz, dt, lo, hi, wall, nthreads)
         return U, V, W, P
+
+    # ------------------------------------------------ variable-density projection
+    def vd_metric(self, yu):
+        """inv_dy_p_pad (ny+1) from the faces (calc_bands.py:273, :276)."""
+        yu = np.ascontiguousarray(yu, dtype=np.float64)
+        out = np.zeros(len(yu))
+        assert self.lib.orc_vd_metric_from_yu(len(yu) - 1, _ptr(yu), _ptr(out)) == 0
+        return out
+
+    def rho_min(self, rho, nthreads=0):
+        nx, nz, ny = rho.shape[0] - 2, rho.shape[1] - 2, rho.shape[2] - 2
+        return self.lib.orc_rho_min(nx, nz, ny, _ptr(np.asfortranarray(rho)), nthreads)
+
+    def projection_vd(self, Uh, Vh, Wh, rho, P_now, P_old, div_now, dx, dz, dt, yu, band_mode="reference",
+                      wall=(0.0,) * 6, nthreads=0):
+        """Variable-density step (MCS:538-573, Poisson, MCS:1153-1197); returns
+        (U, V, W, P, P_next, rho_min)."""
+        nx, nz, ny = Uh.shape[0] - 2, Uh.shape[1] - 2, Uh.shape[2] - 2
+        b6 = bands(yu, band_mode)
+        idy, lo, hi = (np.ascontiguousarray(v) for v in metrics(yu))
+        pad = self.vd_metric(yu)
+        rmin = self.rho_min(rho, nthreads)
+        F = [np.asfortranarray(a, dtype=np.float64) for a in (Uh, Vh, Wh, rho, P_now, P_old, div_now)]
+        P = np.zeros((nx, nz, ny), order="F")
+        rc = self.lib.orc_vd_rhs(nx, nz, ny, dx, dz, dt, _ptr(idy), _ptr(pad), _ptr(F[0]), _ptr(F[1]), _ptr(F[2]),
+                                 wall[1], wall[4], _ptr(F[3]), _ptr(F[4]), _ptr(F[5]), _ptr(F[6]), rmin, _ptr(P),
+                                 nthreads)
+        if rc:
+            raise RuntimeError(f"orc_vd_rhs failed: {rc}")
+        P, _ = self.poisson(P, dx, dz, b6, nthreads)
+        U, V, W, P_next = (np.zeros_like(F[0], order="F") for _ in range(4))
+        w = np.ascontiguousarray(wall, dtype=np.float64)
+        rc = self.lib.orc_vd_correction(nx, nz, ny, dx, dz, dt, _ptr(lo), _ptr(hi), _ptr(P), _ptr(F[0]), _ptr(F[1]),
+                                        _ptr(F[2]), _ptr(w), _ptr(F[3]), _ptr(F[4]), _ptr(F[5]), rmin, _ptr(U),
+                                        _ptr(V), _ptr(W), _ptr(P_next), nthreads)
+        if rc:
+            raise RuntimeError(f"orc_vd_correction failed: {rc}")
+        return U, V, W, P, P_next, rmin
 
     def r2hc(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
