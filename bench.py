@@ -367,6 +367,55 @@ def run_rough(device, nx, ny, nz, steps, warmup):
     return out
 
 
+def run_vd(device, nx, ny, nz, steps, warmup):
+    """Variable-density step (rho_min splitting) on the channel case: the predictor of the
+    main workload, rho(y) = 1 - 0.6 (1 - (y-1)^2) times 1 + N(0, 0.05), P_now, P_old and
+    div_now ~ N(0, 0.01), halos filled periodically / by wall ghost copies; FP64."""
+    import torch
+    import prj
+    Uh, Vh, Wh, yu = device_inputs(nx, ny, nz, seed=11, device=device)
+    yp = torch.tensor((yu[:-1] + yu[1:]) / 2, dtype=torch.float64, device=device).view(-1, 1, 1)
+    g = torch.Generator(device=device)
+    g.manual_seed(12)
+    hs = (ny + 2, nz + 2, nx + 2)
+
+    def halo(f):  # periodic x/z images, wall ghost planes copied from the first/last plane
+        f[:, :, 0] = f[:, :, -2]
+        f[:, :, -1] = f[:, :, 1]
+        f[:, 0, :] = f[:, -2, :]
+        f[:, -1, :] = f[:, 1, :]
+        f[0] = f[1]
+        f[-1] = f[-2]
+        return f
+
+    rho = torch.zeros(hs, dtype=torch.float64, device=device)
+    rho[1:-1, 1:-1, 1:-1].normal_(1.0, 0.05, generator=g).mul_(1.0 - 0.6 * (1.0 - (yp - 1.0) ** 2))
+    extra = []
+    for _ in range(3):
+        f = torch.zeros(hs, dtype=torch.float64, device=device)
+        f[1:-1, 1:-1, 1:-1].normal_(0.0, 0.01, generator=g)
+        extra.append(halo(f))
+    halo(rho)
+    Pn, Po, div = extra
+    U, V, W, Pnext = (torch.empty(hs, dtype=torch.float64, device=device) for _ in range(4))
+    P = torch.empty((ny, nz, nx), dtype=torch.float64, device=device)
+    dx, dz = 2 * math.pi / nx, math.pi / nz
+    stream = torch.cuda.current_stream(device)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent", device=device.index or 0) as plan:
+        fn = lambda: plan.projection_step_vd(Uh, Vh, Wh, rho, Pn, Po, div, U, V, W, P, Pnext, 1.0, stats=False,
+                                             stream=stream)
+        for _ in range(warmup):
+            fn()
+        plan.enable_stage_timing(True)
+        ms = timed_steps(fn, stream, steps) / steps
+        plan.enable_stage_timing(False)
+        stages = plan.stage_times()
+        st = plan.projection_step_vd(Uh, Vh, Wh, rho, Pn, Po, div, U, V, W, P, Pnext, 1.0, stream=stream)
+    return {"grid": f"{nx}x{ny}x{nz}", "gpts_per_s": nx * ny * nz / (ms / 1e3) / 1e9, "ms_per_step": ms,
+            "div_maxabs": st["div_maxabs"], "rho_min": st["rho_min"],
+            "stages_ms_per_launch": {k: v[0] / v[1] for k, v in stages.items()}}
+
+
 def run_served(device, seconds, rate, budget):
     """Open-loop Poisson arrivals (rate per second, default_rng(3)) of projection requests of
     sizes (128,96,64)/(256,128,128)/(384,192,192)/(768,384,384) with p = 0.4/0.3/0.2/0.1."""
@@ -538,6 +587,8 @@ def main():
         extra["batched"] = run_batched(device, steps=max(3, args.steps // 4), warmup=args.warmup)
         torch.cuda.empty_cache()
         extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
+        torch.cuda.empty_cache()
+        extra["variable_density"] = run_vd(device, NX, NY, NZ, steps=max(3, args.steps // 4), warmup=args.warmup)
         torch.cuda.empty_cache()
         if args.rough_grid:
             rx, ry, rz = (int(v) for v in args.rough_grid.lower().split("x"))
