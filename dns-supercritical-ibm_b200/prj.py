@@ -53,6 +53,8 @@ EXPORTS = (
     "prj_batch_create", "prj_batch_launch", "prj_batch_destroy",
     "prj_plan_get_tuning", "prj_plan_set_tuning",
     "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
+    "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
+    "prj_field_write_device",
 )
 
 BANDS_REFERENCE = 0
@@ -139,6 +141,12 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
+    cp, ip = ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)
+    L.prj_field_read_header.argtypes = [cp, ip, ip, ip]
+    L.prj_field_read.argtypes = [cp, i, i, i, _dp, i]
+    L.prj_field_write.argtypes = [cp, i, i, i, _dp, i]
+    L.prj_field_read_device.argtypes = [cp, i, i, i, _vp, i, i]
+    L.prj_field_write_device.argtypes = [cp, i, i, i, _vp, i, i]
     L.prj_plan_set_vd_metric.argtypes = [_vp, _dp]
     L.prj_projection_step_vd.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams),
                                          ctypes.POINTER(VdFields), i, ctypes.POINTER(Stats), _vp]
@@ -389,6 +397,60 @@ class Plan:
                                         ctypes.byref(par), ctypes.byref(f), mode,
                                         ctypes.byref(st) if stats else None, _stream_ptr(stream)))
         return st.as_dict() if stats else None
+
+
+# ----------------------------------------------------------------- field files
+def field_header(path):
+    """(nx, nz, ny) of a field file (prj_field_read_header)."""
+    v = [ctypes.c_int() for _ in range(3)]
+    _check(load_library().prj_field_read_header(os.fsencode(path), *[ctypes.byref(x) for x in v]))
+    return tuple(x.value for x in v)
+
+
+def _field_dims(a, halo):
+    if _is_tensor(a):
+        ny, nz, nx = a.shape
+    else:
+        nx, nz, ny = a.shape
+    return (nx - 2, nz - 2, ny - 2) if halo else (nx, nz, ny)
+
+
+def write_field(path, a, halo=False):
+    """Write a field in the reference's file format (src/mod_io.f90: int32 nx, nz, ny + float64
+    interior, x fastest).  a: numpy Fortran-ordered [x, z, y] or a contiguous torch CUDA tensor
+    [y, z, x]; halo=True for halo'd arrays (interior written)."""
+    L = load_library()
+    nx, nz, ny = _field_dims(a, halo)
+    if _is_tensor(a):
+        if not (a.is_cuda and a.is_contiguous() and str(a.dtype) == "torch.float64"):
+            raise ValueError("tensor fields must be contiguous float64 CUDA tensors")
+        _check(L.prj_field_write_device(os.fsencode(path), nx, nz, ny, ctypes.c_void_p(a.data_ptr()), int(halo),
+                                        a.device.index or 0))
+    else:
+        if not (a.dtype == np.float64 and a.flags.f_contiguous):
+            raise ValueError("numpy fields must be Fortran-ordered float64 arrays")
+        _check(L.prj_field_write(os.fsencode(path), nx, nz, ny, _p(a), int(halo)))
+
+
+def read_field(path, out=None, halo=False):
+    """Read a field file into `out` (same conventions as write_field) or, when out is None, into
+    a new numpy Fortran-ordered (nx, nz, ny) array.  A grid differing from out's raises PrjError."""
+    L = load_library()
+    if out is None:
+        nx, nz, ny = field_header(path)
+        out = np.empty((nx, nz, ny), order="F")
+        halo = False
+    nx, nz, ny = _field_dims(out, halo)
+    if _is_tensor(out):
+        if not (out.is_cuda and out.is_contiguous() and str(out.dtype) == "torch.float64"):
+            raise ValueError("tensor fields must be contiguous float64 CUDA tensors")
+        _check(L.prj_field_read_device(os.fsencode(path), nx, nz, ny, ctypes.c_void_p(out.data_ptr()), int(halo),
+                                       out.device.index or 0))
+    else:
+        if not (out.dtype == np.float64 and out.flags.f_contiguous):
+            raise ValueError("numpy fields must be Fortran-ordered float64 arrays")
+        _check(L.prj_field_read(os.fsencode(path), nx, nz, ny, _p(out), int(halo)))
+    return out
 
 
 class Batch:

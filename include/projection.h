@@ -171,6 +171,24 @@ int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_V
                            const prj_vd_fields* vd, int mode, prj_stats* stats, void* stream);
 
 /*
+ * Field files of the reference (src/mod_io.f90:7-149, cfd_read_arr /
+ * cfd_write_arr: array_ini_*.dat, end/array_end_*.dat): stream-unformatted,
+ * three 4-byte integers nx, nz, ny, then the nx*nz*ny interior values as
+ * float64, x fastest, then z, then y.  `halo` = 0: the array is (nx, nz, ny);
+ * halo = 1: it is halo'd (nx+2, nz+2, ny+2) and only its interior is read or
+ * written (halos untouched).  Reads fail with PRJ_ERR_ARG when the file's grid
+ * differs from (nx, nz, ny) (the reference stops there, mod_io.f90:27-33).
+ * The device forms stage y-plane chunks through pinned host memory and overlap
+ * the file transfer with the copies; they first wait for the device's pending
+ * work and return when the transfer is complete.
+ */
+int prj_field_read_header(const char* path, int* nx, int* nz, int* ny);
+int prj_field_read(const char* path, int nx, int nz, int ny, double* h_dst, int halo);
+int prj_field_write(const char* path, int nx, int nz, int ny, const double* h_src, int halo);
+int prj_field_read_device(const char* path, int nx, int nz, int ny, double* d_dst, int halo, int device);
+int prj_field_write_device(const char* path, int nx, int nz, int ny, const double* d_src, int halo, int device);
+
+/*
  * Batched solves: one CUDA graph holding every case (case i solves plans[i] in
  * place on the device array d_P[i], FP64 or PRJ_MODE_FP32_REFINE), the cases
  * on parallel graph branches, replayed by one graph launch.  The plans must be
