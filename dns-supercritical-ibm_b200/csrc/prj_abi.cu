@@ -584,6 +584,10 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
         // PRJ_FFT_KERNELS=runtime keeps the runtime-radix kernels for lengths with a pass plan
         const char* v = getenv("PRJ_FFT_KERNELS");
         pl->use_pass = !(v && !strcmp(v, "runtime"));
+        // PRJ_X_STAGED=128|256 selects the staged persistent x-forward kernel for the
+        // divergence source with that many threads per CTA (measured slower; off by default)
+        const char* xs = getenv("PRJ_X_STAGED");
+        pl->x_staged = xs ? atoi(xs) : 0;
     }
     pl->kxs = g.nxh;
     pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);

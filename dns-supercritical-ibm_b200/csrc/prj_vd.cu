@@ -73,10 +73,12 @@ struct VdArgs {
 __device__ __forceinline__ double ps(const VdArgs& a, size_t h) {
     return __dsub_rn(__dmul_rn(2.0, a.Pn[h]), a.Po[h]);
 }
-// 1 - rho_min (0.5/rho_nbr + 0.5/rho_c)
-__device__ __forceinline__ double rho_w(double rmin, double rn, double rc) {
-    return __dsub_rn(1.0, __dmul_rn(rmin, __dadd_rn(__ddiv_rn(0.5, rn), __ddiv_rn(0.5, rc))));
+// 1 - rho_min (0.5/rho_nbr + 0.5/rho_c), given hn = 0.5/rho_nbr and hc = 0.5/rho_c (each
+// quotient computed once per point: the same correctly rounded value the reference forms)
+__device__ __forceinline__ double rho_w(double rmin, double hn, double hc) {
+    return __dsub_rn(1.0, __dmul_rn(rmin, __dadd_rn(hn, hc)));
 }
+__device__ __forceinline__ double half_inv(double r) { return __ddiv_rn(0.5, r); }
 
 // RHS of the constant-coefficient Poisson equation, one CTA per (y, z) row
 __global__ void __launch_bounds__(128) k_vd_rhs(const VdArgs a) {
@@ -97,13 +99,14 @@ __global__ void __launch_bounds__(128) k_vd_rhs(const VdArgs a) {
         const size_t hzp = hix(nx, nz, i, j + 1, k), hzm = hix(nx, nz, i, j - 1, k);
         const size_t hyp = hix(nx, nz, i, j, k + 1), hym = hix(nx, nz, i, j, k - 1);
         const double p00 = ps(a, h);
-        const double r0 = a.rho[h];
-        const double X = __dsub_rn(__dmul_rn(rho_w(rmin, a.rho[hxp], r0), __dsub_rn(ps(a, hxp), p00)),
-                                   __dmul_rn(rho_w(rmin, a.rho[hxm], r0), __dsub_rn(p00, ps(a, hxm))));
-        const double Z = __dsub_rn(__dmul_rn(rho_w(rmin, a.rho[hzp], r0), __dsub_rn(ps(a, hzp), p00)),
-                                   __dmul_rn(rho_w(rmin, a.rho[hzm], r0), __dsub_rn(p00, ps(a, hzm))));
-        const double Y = __dsub_rn(__dmul_rn(__dmul_rn(rho_w(rmin, a.rho[hyp], r0), __dsub_rn(ps(a, hyp), p00)), padp),
-                                   __dmul_rn(__dmul_rn(rho_w(rmin, a.rho[hym], r0), __dsub_rn(p00, ps(a, hym))), padm));
+        const double h0 = half_inv(a.rho[h]);
+        const double X = __dsub_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hxp]), h0), __dsub_rn(ps(a, hxp), p00)),
+                                   __dmul_rn(rho_w(rmin, half_inv(a.rho[hxm]), h0), __dsub_rn(p00, ps(a, hxm))));
+        const double Z = __dsub_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hzp]), h0), __dsub_rn(ps(a, hzp), p00)),
+                                   __dmul_rn(rho_w(rmin, half_inv(a.rho[hzm]), h0), __dsub_rn(p00, ps(a, hzm))));
+        const double Y =
+            __dsub_rn(__dmul_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hyp]), h0), __dsub_rn(ps(a, hyp), p00)), padp),
+                      __dmul_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hym]), h0), __dsub_rn(p00, ps(a, hym))), padm));
         const double L = __dadd_rn(__dadd_rn(__dmul_rn(X, a.inv_dx2), __dmul_rn(Z, a.inv_dz2)), __dmul_rn(Y, idy));
         const double t1 = __dmul_rn(__dmul_rn(a.inv_dt, dv), rmin);
         const double t2 = __dmul_rn(__dmul_rn(a.inv_dt, rmin), a.div_now[h]);
