@@ -77,11 +77,22 @@ __device__ __forceinline__ int pass_slot(int k) {
     }
 }
 
-// a[q] *= w^(q j) from the stage table w[(q - 1) mm + j]
+// a[q] *= w1^q with w1 = exp(-+2 pi i j / L) the first row of the stage table
+// (w[j]); the powers come from a product tree of depth <= 3 (about 3 ulp), so a
+// butterfly loads one twiddle instead of R-1 (the loads were the larger share of
+// the L1 traffic of these kernels)
 template <int DIR, int R, int MM, typename V>
 __device__ __forceinline__ void apply_twiddles(V* a, const V* __restrict__ w, int j) {
+    V p[R];
+    p[1] = w[j];
+    if constexpr (R > 2) p[2] = cmul(p[1], p[1]);
+    if constexpr (R > 3) p[3] = cmul(p[1], p[2]);
+    if constexpr (R > 4) p[4] = cmul(p[2], p[2]);
+    if constexpr (R > 5) p[5] = cmul(p[2], p[3]);
+    if constexpr (R > 6) p[6] = cmul(p[3], p[3]);
+    if constexpr (R > 7) p[7] = cmul(p[3], p[4]);
 #pragma unroll
-    for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], w[(q - 1) * MM + j]);
+    for (int q = 1; q < R; q++) a[q] = twiddle<DIR>(a[q], p[q]);
 }
 
 // One pass s of nrows rows held in shared memory (row stride rs, padded slots):
