@@ -54,7 +54,7 @@ EXPORTS = (
     "prj_plan_get_tuning", "prj_plan_set_tuning",
     "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
     "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
-    "prj_field_write_device",
+    "prj_field_write_device", "prj_rough_force", "prj_ibm_interp",
 )
 
 BANDS_REFERENCE = 0
@@ -87,6 +87,10 @@ class Tuning(ctypes.Structure):
 class VdFields(ctypes.Structure):
     _fields_ = [("rho", ctypes.c_void_p), ("P_now", ctypes.c_void_p), ("P_old", ctypes.c_void_p),
                 ("div_now", ctypes.c_void_p), ("P_next", ctypes.c_void_p)]
+
+
+class RoughInds(ctypes.Structure):
+    _fields_ = [(f"{c}_{w}", ctypes.c_void_p) for c in "UVW" for w in ("bot", "top")]
 
 
 class StepParams(ctypes.Structure):
@@ -141,6 +145,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
+    L.prj_rough_force.argtypes = [i, i, i, _vp, _vp, _vp, ctypes.POINTER(RoughInds), ctypes.POINTER(StepParams), _vp]
+    ll = ctypes.c_longlong
+    L.prj_ibm_interp.argtypes = [_vp, ll, i, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp, _vp, _vp, _vp]
     cp, ip = ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)
     L.prj_field_read_header.argtypes = [cp, ip, ip, ip]
     L.prj_field_read.argtypes = [cp, i, i, i, _dp, i]
@@ -397,6 +404,38 @@ class Plan:
                                         ctypes.byref(par), ctypes.byref(f), mode,
                                         ctypes.byref(st) if stats else None, _stream_ptr(stream)))
         return st.as_dict() if stats else None
+
+
+# ----------------------------------------------------------------- IBM forcing
+def rough_force(Uh, Vh, Wh, inds, wall=(0.0,) * 6, stream=None):
+    """ibm_part_2 forcing in place (prj_rough_force).  Uh, Vh, Wh: halo'd torch CUDA tensors
+    [y+2, z+2, x+2]; inds: dict with keys U_bot, U_top, V_bot, V_top, W_bot, W_top of contiguous
+    int32 CUDA tensors [nz, nx] (column (i, j) at [j, i])."""
+    torch = _torch()
+    ny, nz, nx = (d - 2 for d in Uh.shape)
+    keys = [f"{c}_{w}" for c in "UVW" for w in ("bot", "top")]
+    for k in keys:
+        t = inds[k]
+        if not (t.is_cuda and t.dtype == torch.int32 and t.is_contiguous() and tuple(t.shape) == (nz, nx)):
+            raise ValueError(f"{k} must be a contiguous int32 CUDA tensor of shape {(nz, nx)}")
+    ri = RoughInds(*[inds[k].data_ptr() for k in keys])
+    par = StepParams(1.0, *[float(w) for w in wall], 0)
+    _check(load_library().prj_rough_force(nx, nz, ny, ctypes.c_void_p(Uh.data_ptr()), ctypes.c_void_p(Vh.data_ptr()),
+                                          ctypes.c_void_p(Wh.data_ptr()), ctypes.byref(ri), ctypes.byref(par),
+                                          _stream_ptr(stream)))
+
+
+def ibm_interp(A, pos, src1, src2, c0, c1, c2, dst=None, src=None, stream=None):
+    """Interpolated forcing points in place on torch CUDA tensor A (prj_ibm_interp):
+    A[pos] = c1 A[src1] + c2 A[src2] + c0 (sources read first), then A[dst] = A[src].
+    Offsets are int64 CUDA tensors into A's flat storage; coefficients float64 CUDA tensors."""
+    torch = _torch()
+    n = int(pos.numel())
+    ncopy = int(dst.numel()) if dst is not None else 0
+    scratch = torch.empty(2 * n + 1, dtype=torch.float64, device=A.device)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
+    _check(load_library().prj_ibm_interp(vp(A), A.numel(), n, vp(pos), vp(src1), vp(src2), vp(c0), vp(c1), vp(c2),
+                                         ncopy, vp(dst), vp(src), vp(scratch), _stream_ptr(stream)))
 
 
 # ----------------------------------------------------------------- field files

@@ -171,6 +171,38 @@ int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_V
                            const prj_vd_fields* vd, int mode, prj_stats* stats, void* stream);
 
 /*
+ * Immersed-boundary forcing of the predictor before the projection (rough-wall
+ * runs, src/mod_cfd_subroutines.f90:411-426), in place on the halo'd device
+ * fields.
+ *
+ * prj_rough_force: ibm_part_2 (src/ibm_setup/mod_cfd_ibm.f90:47-131).  For each
+ * column (i, j) (index c = i + nx j of the int32 device arrays): cells
+ * k = 0..bot[c] take the bottom wall value, k = top[c]..ny-1 the top one (v:
+ * k = top[c]..ny, up to the top wall face).  bot = -1 / top = ny force nothing.
+ *
+ * prj_ibm_interp: the interpolated forcing points of diezdecomp_ibm_exec on one
+ * rank (src/diezdecomp_api_ibm.f90:374-424) for one field A of `len` elements:
+ * A[pos_i] = c1_i A[src1_i] + c2_i A[src2_i] + c0_i for i < n, every source read
+ * before any point is written, then A[dst_j] = A[src_j] for j < ncopy.  Offsets
+ * are elements of the halo'd array.  d_scratch holds 2 n + 1 doubles.  An offset
+ * outside [0, len) is skipped and reported as PRJ_ERR_ARG; the call synchronises
+ * `stream`.
+ */
+typedef struct prj_rough_inds {
+    const int* U_bot;
+    const int* U_top;
+    const int* V_bot;
+    const int* V_top;
+    const int* W_bot;
+    const int* W_top;
+} prj_rough_inds;
+int prj_rough_force(int nx, int nz, int ny, double* d_Uh, double* d_Vh, double* d_Wh, const prj_rough_inds* inds,
+                    const prj_step_params* walls, void* stream);
+int prj_ibm_interp(double* d_A, long long len, int n, const long long* d_pos, const long long* d_src1,
+                   const long long* d_src2, const double* d_c0, const double* d_c1, const double* d_c2, int ncopy,
+                   const long long* d_dst, const long long* d_src, double* d_scratch, void* stream);
+
+/*
  * Field files of the reference (src/mod_io.f90:7-149, cfd_read_arr /
  * cfd_write_arr: array_ini_*.dat, end/array_end_*.dat): stream-unformatted,
  * three 4-byte integers nx, nz, ny, then the nx*nz*ny interior values as

@@ -306,3 +306,34 @@ class COracle:
         out = [np.zeros(ny) for _ in range(3)]
         assert self.lib.orc_metrics_from_yu(ny, _ptr(yu), *[_ptr(v) for v in out]) == 0
         return tuple(out)
+
+
+# --------------------------------------------------------------------- IBM forcing
+def rough_force(Uh, Vh, Wh, inds, wall=(0.0,) * 6):
+    """ibm_part_2 (src/ibm_setup/mod_cfd_ibm.f90:64-116) on halo'd [x+2, z+2, y+2] copies:
+    column (i, j): k = 0..bot take the bottom wall value, k = top..ny-1 (v: ..ny) the top one.
+    inds[name] is an (nx, nz) integer array.  Returns the forced (U, V, W)."""
+    out = [np.array(a, order="F", copy=True) for a in (Uh, Vh, Wh)]
+    ny = Uh.shape[2] - 2
+    for F, c, lo, hi, kmax in ((out[0], "U", wall[0], wall[3], ny - 1), (out[1], "V", wall[1], wall[4], ny),
+                               (out[2], "W", wall[2], wall[5], ny - 1)):
+        bot, top = inds[f"{c}_bot"], inds[f"{c}_top"]
+        nx, nz = bot.shape
+        for i in range(nx):
+            for j in range(nz):
+                for k in range(0, bot[i, j] + 1):
+                    F[i + 1, j + 1, k + 1] = lo
+                for k in range(top[i, j], kmax + 1):
+                    F[i + 1, j + 1, k + 1] = hi
+    return tuple(out)
+
+
+def ibm_interp(A, pos, src1, src2, c0, c1, c2, dst=(), src=()):
+    """diezdecomp_ibm_exec on one rank (src/diezdecomp_api_ibm.f90:374-424) on the flat Fortran
+    storage of A: sources gathered first, A[pos] = (c1 A[src1] + c2 A[src2]) + c0, then copies."""
+    flat = np.array(A, order="F", copy=True).reshape(-1, order="F")
+    g1, g2 = flat[np.asarray(src1)], flat[np.asarray(src2)]
+    flat[np.asarray(pos)] = (np.asarray(c1) * g1 + np.asarray(c2) * g2) + np.asarray(c0)
+    for d, s_ in zip(dst, src):
+        flat[d] = flat[s_]
+    return flat.reshape(A.shape, order="F")
