@@ -223,7 +223,7 @@ def timed_steps(fn, stream, steps):
     return total
 
 
-def run_batched(device, steps, warmup):
+def run_batched(device, steps, warmup, rank=0, world=1, dist=None):
     """64 independent Poisson solves of uneven sizes in one CUDA graph launch: sizes from
     default_rng(2) (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]),
     uniform[-1,1] right-hand sides minus their dy-weighted mean; launch shapes from the
@@ -233,12 +233,17 @@ def run_batched(device, steps, warmup):
     import autotune
     import prj
     import workloads
+    import sharding
     rng = np.random.default_rng(2)
-    specs = []
+    specs_all = []
     for _ in range(64):
         nx, nz = (int(v) for v in rng.choice([64, 96, 128, 192, 256], 2))
         ny = int(rng.choice([48, 64, 96, 128]))
-        specs.append((nx, ny, nz, float(rng.uniform(1.5, 2.5))))
+        specs_all.append((nx, ny, nz, float(rng.uniform(1.5, 2.5))))
+    # the 64 cases are split over the ranks by size (no data-path collective)
+    mine = sharding.partition_cases([a * b * c for a, b, c, _ in specs_all], world)[rank]
+    specs = [specs_all[i] for i in mine]
+    seeds = [1000 + i for i in mine]
     plans, rhs = [], []
     t_tune = time.perf_counter()
     tuned = {}
@@ -253,14 +258,15 @@ def run_batched(device, steps, warmup):
             tuned[(nx, ny, nz)] = {k: best[k] for k in ("x_rows", "z_rows", "z_mode")}
         plans.append(p)
         g = torch.Generator(device=device)
-        g.manual_seed(1000 + i)
+        g.manual_seed(seeds[i])
         r = torch.rand((ny, nz, nx), generator=g, dtype=torch.float64, device=device) * 2 - 1
         w = torch.tensor(np.diff(yu), dtype=torch.float64, device=device).view(-1, 1, 1)
         r -= (r * w).sum() / (w.sum() * nx * nz)
         rhs.append(r)
     t_tune = time.perf_counter() - t_tune
-    pts = sum(nx * ny * nz for nx, ny, nz, _ in specs)
-    out = {"cases": 64, "points": pts, "distinct_sizes": len(tuned), "setup_s": t_tune}
+    pts = sum(nx * ny * nz for nx, ny, nz, _ in specs_all)
+    out = {"cases": 64, "points": pts, "distinct_sizes": len(tuned), "setup_s": t_tune,
+           "sharding": f"{world} rank(s), cases partitioned by size"}
     stream = torch.cuda.current_stream(device)
     for name, mode in (("fp64", prj.MODE_FP64), ("mixed", prj.MODE_FP32_REFINE)):
         if mode == prj.MODE_FP32_REFINE:  # the mixed path runs the split z kernels
@@ -281,6 +287,9 @@ def run_batched(device, steps, warmup):
             for _ in range(steps):
                 reset()
                 total += timed_steps(lambda: batch.launch(stream), stream, 1)
+            if dist is not None:
+                dist.barrier()
+            total = sharding.max_over_ranks(total, dist, device)
             out[name] = {"gpts_per_s": pts * steps / (total / 1e3) / 1e9, "ms_per_batch": total / steps,
                          "graph_launches": steps}
     for p in plans:
@@ -464,6 +473,7 @@ def main():
     import numpy as np
     import torch
     import prj
+    import sharding
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
@@ -510,11 +520,8 @@ def main():
     plan.enable_stage_timing(False)
     ms = e0.elapsed_time(e1)
     stages = plan.stage_times()
-    t = torch.tensor([ms], dtype=torch.float64, device=device)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * NX * NY * NZ * args.steps / (ms_max / 1e3) / 1e9
+    ms_max = sharding.max_over_ranks(ms, dist, device)
+    value = sharding.job_throughput(NX * NY * NZ, args.steps, world, ms_max)
 
     # accuracy record of the same step (outside the timed region)
     st = step(stats=True)
@@ -537,11 +544,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             plan.projection_step(pUh, pVh, pWh, pU, pV, pW, pP, 1.0, mode=mode, stats=False)
-        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-        te = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-        if dist is not None:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_s = float(te.item())
+        e2e_s = sharding.max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, dist, device)
         nh = (NX + 2) * (NZ + 2) * (NY + 2)
         e2e = {"value": world * NX * NY * NZ / e2e_s / 1e9, "unit": "Gpts/s", "h2d_bytes_per_step": 3 * 8 * nh,
                "d2h_bytes_per_step": 3 * 8 * nh + 8 * NX * NY * NZ, "ms_per_step": 1e3 * e2e_s,
@@ -571,6 +574,7 @@ def main():
             plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=other, stats=False, stream=stream)
         ms_other = timed_steps(lambda: plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=other, stats=False,
                                                             stream=stream), stream, max(3, args.steps // 4))
+        ms_other = sharding.max_over_ranks(ms_other, dist, device)
         st_o = plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=other, stats=True, stream=stream)
         rel = float(torch.linalg.vector_norm(P - P_main) / torch.linalg.vector_norm(P_main))
         nsteps_o = max(3, args.steps // 4)
@@ -583,9 +587,11 @@ def main():
     plan.close()
     del Uh, Vh, Wh, U, V, W, P
     torch.cuda.empty_cache()
-    if not args.no_extra and world == 1:
-        extra["batched"] = run_batched(device, steps=max(3, args.steps // 4), warmup=args.warmup)
+    if not args.no_extra:
+        extra["batched"] = run_batched(device, steps=max(3, args.steps // 4), warmup=args.warmup, rank=rank,
+                                       world=world, dist=dist)
         torch.cuda.empty_cache()
+    if not args.no_extra and world == 1:
         extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
         torch.cuda.empty_cache()
         extra["variable_density"] = run_vd(device, NX, NY, NZ, steps=max(3, args.steps // 4), warmup=args.warmup)
