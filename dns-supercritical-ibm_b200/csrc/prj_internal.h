@@ -115,12 +115,21 @@ struct prj_plan {
                                   // 0 off, else its threads per CTA (128 or 256)
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
     double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
+    int overlap_chunks = 0;       // y chunks of the overlapped projection schedule (0: sequential)
+    cudaStream_t ov_st[2] = {nullptr, nullptr};  // its two helper streams (created on first use)
+    std::vector<cudaEvent_t> ov_ev;              // its events
 };
 
 namespace prj {
 
 // Kernel launchers (prj_kernels.cu).  All are asynchronous on `st`.
 enum class FwdSource { Pressure, Divergence };
+
+// a range of y planes [y0, y1) of one launch; y1 < 0 means up to ny
+struct YRange {
+    int y0 = 0, y1 = -1;
+    YRange resolved(int ny) const { return YRange{y0, y1 < 0 ? ny : y1}; }
+};
 
 struct StepScalars {
     double dt, inv_dt;
@@ -130,10 +139,14 @@ struct StepScalars {
 cudaError_t launch_fwd_x(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
                          const double* Wh, const StepScalars* sc, cudaStream_t st);
 cudaError_t launch_zsolve(const prj_plan* pl, cudaStream_t st);
+// divergence + forward x over a y range (the in-place x kernels)
+inline cudaError_t launch_fwd_x_range(const prj_plan* pl, const double* Uh, const double* Vh, const double* Wh,
+                                      const StepScalars* sc, cudaStream_t st, YRange yr);
 cudaError_t launch_bwd_x(const prj_plan* pl, double* P, cudaStream_t st);
+// kh: halo'd plane range [kh0, kh1) of 0 .. ny+1 (planes -1 .. ny); default all
 cudaError_t launch_correction(const prj_plan* pl, const double* P, const double* Uh, const double* Vh,
                               const double* Wh, double* U, double* V, double* W, const StepScalars& sc,
-                              cudaStream_t st);
+                              cudaStream_t st, YRange kh = YRange{});
 cudaError_t launch_build_pivots(const prj_plan* pl, cudaStream_t st);
 cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, const double* W, const double* P,
                          double* out2, cudaStream_t st);
@@ -146,14 +159,20 @@ cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStrea
 // bout: also store the source field (divergence) there; accum: P += result; sq: norms of
 // the update and of the result (accum only)
 cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
-                          const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout = nullptr);
-cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum = 0, double* sq = nullptr);
+                          const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout = nullptr,
+                          YRange yr = YRange{});
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum = 0, double* sq = nullptr,
+                          YRange yr = YRange{});
+inline cudaError_t launch_fwd_x_range(const prj_plan* pl, const double* Uh, const double* Vh, const double* Wh,
+                                      const StepScalars* sc, cudaStream_t st, YRange yr) {
+    return launch_fwd_xd(pl, FwdSource::Divergence, nullptr, Uh, Vh, Wh, sc, st, nullptr, yr);
+}
 int choose_tz_xd(int m, bool even);
 int choose_tz_xp(int m);                 // rows per CTA of the pass-plan x kernels
 size_t pass_x_smem(int m, int tz);       // their shared memory
 
 // z direction as separate kernels (prj_zsplit.cu); need pl->zd.ok and pl->kz_of_slot
-cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st);
+cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st, YRange yr = YRange{});
 cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st);
 // mixed storage (FP64 rows kx < kxs in spec, FP32 rows in spec32)
 cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st);

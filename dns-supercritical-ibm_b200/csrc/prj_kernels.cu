@@ -315,6 +315,7 @@ struct CorrArgs {
     double* W;
     double dt, inv_dx, inv_dz;
     double wall[6];
+    int kh0;  // first halo'd plane of this launch (grid.x planes from kh0)
 };
 
 // u = u_hat - dt grad P on the whole halo'd box (mod_cfd_subroutines.f90:1124-1152);
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(128) k_correct(const CorrArgs a) {
     // one block per halo'd x-row (jh, kh): no index division, coalesced along x
     const int nx = a.nx, nz = a.nz, ny = a.ny;
     const int jh = blockIdx.y;
-    const int k = (int)blockIdx.x - 1;
+    const int k = (int)blockIdx.x + a.kh0 - 1;
     const size_t rowh = (size_t)(nx + 2) * ((size_t)jh + (size_t)(nz + 2) * (size_t)(k + 1));
     if (k < 0 || k == ny) {
         const double u = k < 0 ? a.wall[0] : a.wall[3];
@@ -484,15 +485,18 @@ cudaError_t launch_build_pivots(const prj_plan* pl, cudaStream_t st) {
 
 cudaError_t launch_correction(const prj_plan* pl, const double* P, const double* Uh, const double* Vh,
                               const double* Wh, double* U, double* V, double* W, const StepScalars& sc,
-                              cudaStream_t st) {
+                              cudaStream_t st, YRange kh) {
     const Geometry& g = pl->g;
+    kh = kh.resolved(g.ny + 2);
     CorrArgs a{};
+    a.kh0 = kh.y0;
     a.nx = g.nx; a.nz = g.nz; a.ny = g.ny;
     a.P = P; a.Uh = Uh; a.Vh = Vh; a.Wh = Wh; a.lo = pl->t.dpdy_lo; a.hi = pl->t.dpdy_hi;
     a.U = U; a.V = V; a.W = W;
     a.dt = sc.dt; a.inv_dx = 1.0 / g.dx; a.inv_dz = 1.0 / g.dz;
     for (int i = 0; i < 6; i++) a.wall[i] = sc.wall[i];
-    const dim3 grid((unsigned)(g.ny + 2), (unsigned)(g.nz + 2));
+    if (kh.y1 <= kh.y0) return cudaSuccess;
+    const dim3 grid((unsigned)(kh.y1 - kh.y0), (unsigned)(g.nz + 2));
     k_correct<<<grid, 128, 0, st>>>(a);
     return cudaGetLastError();
 }

@@ -45,6 +45,7 @@ struct XArgs {
     double2* X;      // FP64 rows kx < kxs: X[(y kxs + kx) nz + z]
     float2* X32;     // FP32 rows kx >= kxs: X32[(y (nh - kxs) + kx - kxs) nz + z]
     int kxs;         // nh on the FP64 path
+    int y0;          // first y plane of this launch (grid.y planes from y0)
     double* Pout;
     double* Bout;    // k_fwd_xd: copy of the source field (P layout), or null
     int accum;       // k_bwd_xd: Pout += result instead of Pout = result
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_fwd_xd(const XArgs a) {
     double2* A = reinterpret_cast<double2*>(sm);
     int* pos = reinterpret_cast<int*>(sm + (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2));
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
     const int m = a.m, nx = a.nx;
     for (int i = tid; i < m; i += nthr) pos[i] = a.pos[i];
     // kUnroll elements per thread per batch: their loads are independent and in flight together
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
     double2* A = reinterpret_cast<double2*>(sm);
     int* pos = reinterpret_cast<int*>(sm + (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2));
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
     const int m = a.m, nx = a.nx;
     for (int i = tid; i < m; i += nthr) pos[i] = a.pos[i];
     const int total = a.nh * a.tz;
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_fwd_xp(const XA
     double2* A = reinterpret_cast<double2*>(sm);
     constexpr int m = PL::n, nx = 2 * m, rs = m + 1;
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
     const int nr = min(a.tz, a.nz - z0);
     const double2* tw = a.tw;
     if (SRC == 1) {
@@ -516,7 +517,7 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_bwd_xp(const XA
     double2* A = reinterpret_cast<double2*>(sm);
     constexpr int m = PL::n, rs = m + 1, half = m / 2;
     const int tid = threadIdx.x, nthr = blockDim.x;
-    const int y = blockIdx.y, z0 = blockIdx.x * a.tz;
+    const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
     const int nr = min(a.tz, a.nz - z0);
     const double s = a.scale;
     const int total = nr * (half + 1);
@@ -706,10 +707,10 @@ cudaError_t launch_fwd_xs_pl(const XArgs& a, int* err, int nt, cudaStream_t st) 
 
 // pass-plan x kernels for even nx whose half length has a pass plan built with the
 // same radices; cudaErrorNotSupported otherwise (the caller uses the runtime-radix kernels)
-cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, cudaStream_t st) {
+cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, int ny_launch, cudaStream_t st) {
     if (!pl->use_pass || !a.even) return cudaErrorNotSupported;
-    if (fwd && src == FwdSource::Divergence && pl->x_staged && aligned16(a.Uh) && aligned16(a.Vh) &&
-        aligned16(a.Wh)) {
+    if (fwd && src == FwdSource::Divergence && pl->x_staged && a.y0 == 0 && ny_launch == pl->g.ny &&
+        aligned16(a.Uh) && aligned16(a.Vh) && aligned16(a.Wh)) {
         int* err = reinterpret_cast<int*>(pl->stat_buf + kStatErrSlot);
         switch (a.m) {
 #define PRJ_XS_CASE(N, ...)                                                   \
@@ -727,7 +728,7 @@ cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, c
         }
     }
     a.tz = pl->tz_xp;
-    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
+    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, ny_launch);
     switch (a.m) {
 #define PRJ_X_CASE(N, ...)                                                          \
     case N: {                                                                       \
@@ -745,17 +746,19 @@ cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, c
 }  // namespace
 
 cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
-                          const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout) {
+                          const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout, YRange yr) {
     XArgs a = make_args(pl);
+    yr = yr.resolved(pl->g.ny);
+    a.y0 = yr.y0;
     a.Bout = bout;
     a.P = P; a.Uh = Uh; a.Vh = Vh; a.Wh = Wh; a.inv_dy_p = pl->t.inv_dy_p;
     if (sc) { a.inv_dt = sc->inv_dt; a.vbot = sc->wall[1]; a.vtop = sc->wall[4]; }
     if (src == FwdSource::Divergence || (aligned16(P) && aligned16(bout))) {
-        const cudaError_t e = launch_xpass(pl, true, src, a, st);
+        const cudaError_t e = launch_xpass(pl, true, src, a, yr.y1 - yr.y0, st);
         if (e != cudaErrorNotSupported) return e;
     }
     const size_t smem = smem_bytes(a);
-    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
+    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, yr.y1 - yr.y0);
     cudaError_t e;
     if (src == FwdSource::Pressure) {
         if ((e = allow_smem(k_fwd_xd<0>, smem)) != cudaSuccess) return e;
@@ -767,20 +770,22 @@ cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq) {
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq, YRange yr) {
     XArgs a = make_args(pl);
+    yr = yr.resolved(pl->g.ny);
+    a.y0 = yr.y0;
     a.Pout = P;
     a.accum = accum;
     a.sq = sq;
     a.scale = 1.0 / ((double)pl->g.nx * (double)pl->g.nz + 0.0);
     if (aligned16(P)) {
-        const cudaError_t e2 = launch_xpass(pl, false, FwdSource::Pressure, a, st);
+        const cudaError_t e2 = launch_xpass(pl, false, FwdSource::Pressure, a, yr.y1 - yr.y0, st);
         if (e2 != cudaErrorNotSupported) return e2;
     }
     const size_t smem = smem_bytes(a);
     cudaError_t e = allow_smem(k_bwd_xd, smem);
     if (e != cudaSuccess) return e;
-    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, pl->g.ny);
+    const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, yr.y1 - yr.y0);
     k_bwd_xd<<<grid, 256, smem, st>>>(a);
     return cudaGetLastError();
 }

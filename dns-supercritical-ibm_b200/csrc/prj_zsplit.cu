@@ -232,11 +232,11 @@ cudaError_t launch_zfft_pass_pl(ZfftArgs a, int rows_req, cudaStream_t st) {
 // pass-plan z transform of one buffer; cudaErrorNotSupported when nz has no pass
 // plan (or the plan was built with other radices)
 template <typename T>
-cudaError_t launch_zfft_pass(const prj_plan* pl, int dir, void* X, int rows_per_plane, cudaStream_t st) {
+cudaError_t launch_zfft_pass(const prj_plan* pl, int dir, void* X, int rows_per_plane, cudaStream_t st, int nplanes = -1) {
     if (!pl->use_pass) return cudaErrorNotSupported;
     const Geometry& g = pl->g;
     ZfftArgs a{};
-    a.nrow_total = g.ny * rows_per_plane;
+    a.nrow_total = (nplanes < 0 ? g.ny : nplanes) * rows_per_plane;
     a.nz = g.nz;
     a.f = pl->zd.f;
     a.tw = pl->zd.tw;
@@ -308,8 +308,12 @@ cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_p
     return cudaGetLastError();
 }
 
-cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st) {
-    return launch_zfft_t<double2>(pl, dir, pl->spec, pl->g.nxh, st);
+cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st, YRange yr) {
+    yr = yr.resolved(pl->g.ny);
+    if (yr.y0 == 0 && yr.y1 == pl->g.ny) return launch_zfft_t<double2>(pl, dir, pl->spec, pl->g.nxh, st);
+    // a y range: the pass-plan kernel only (the overlapped schedule requires it)
+    double2* X = pl->spec + (size_t)yr.y0 * pl->g.nxh * pl->g.nz;
+    return launch_zfft_pass<double2>(pl, dir, X, pl->g.nxh, st, yr.y1 - yr.y0);
 }
 
 cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st) {

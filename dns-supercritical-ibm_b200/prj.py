@@ -54,7 +54,7 @@ EXPORTS = (
     "prj_plan_get_tuning", "prj_plan_set_tuning",
     "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
     "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
-    "prj_field_write_device", "prj_rough_force", "prj_ibm_interp",
+    "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
 )
 
 BANDS_REFERENCE = 0
@@ -145,6 +145,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
+    L.prj_plan_schedule.argtypes = [_vp, i, ctypes.POINTER(i), ctypes.POINTER(i)]
     L.prj_rough_force.argtypes = [i, i, i, _vp, _vp, _vp, ctypes.POINTER(RoughInds), ctypes.POINTER(StepParams), _vp]
     ll = ctypes.c_longlong
     L.prj_ibm_interp.argtypes = [_vp, ll, i, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp, _vp, _vp, _vp]
@@ -263,6 +264,19 @@ class Plan:
         plan = cls(nx, nz, len(yu) - 1, dx, dz, bands(yu, band_mode), metrics(yu), device)
         plan.set_vd_metric(vd_metric(yu))
         return plan
+
+    def schedule(self, mode=MODE_FP64):
+        """(kernel launches per projection step, overlapped y chunks) (prj_plan_schedule)."""
+        n, c = ctypes.c_int(), ctypes.c_int()
+        _check(load_library().prj_plan_schedule(self.handle, mode, ctypes.byref(n), ctypes.byref(c)))
+        return n.value, c.value
+
+    def launches_per_step(self, mode=MODE_FP64):
+        return self.schedule(mode)[0]
+
+    @property
+    def overlap_chunks(self):
+        return self.schedule(MODE_FP64)[1]
 
     def set_vd_metric(self, inv_dy_p_pad):
         """inv_dy_p_pad (ny+1) for projection_step_vd (prj_plan_set_vd_metric)."""

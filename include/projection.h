@@ -250,6 +250,15 @@ typedef struct prj_tuning {
 int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out);
 int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
 
+/* Kernel launches one prj_projection_step of `mode` issues with the plan's current
+ * configuration (statistics excluded), and the number of y chunks of the overlapped
+ * FP64 schedule (0 when the kernels run one after another).  The overlapped
+ * schedule (environment variable PRJ_OVERLAP_CHUNKS, default 0 = off) splits the planes
+ * into chunks and overlaps the x transform, z transforms and correction of
+ * neighbouring chunks on three streams forked from and joined back into the
+ * caller's stream; stage timing switches it off. */
+int prj_plan_schedule(const prj_plan* plan, int mode, int* launches, int* chunks);
+
 /* band modes of prj_bands_from_yu */
 #define PRJ_BANDS_REFERENCE 0   /* the reference's mk_P_abc bands */
 #define PRJ_BANDS_CONSISTENT 1  /* bands of div(grad p) with the divergence/correction metrics */
