@@ -590,6 +590,10 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
         // PRJ_FFT_KERNELS=runtime keeps the runtime-radix kernels for lengths with a pass plan
         const char* v = getenv("PRJ_FFT_KERNELS");
         pl->use_pass = !(v && !strcmp(v, "runtime"));
+        // PRJ_THOMAS_ASYNC: -1 (default) streams the mixed-storage Thomas only, 0 never,
+        // 1..4 always with ring shape 4x4, 8x2, 2x8, 8x3 (planes x stages)
+        const char* ta = getenv("PRJ_THOMAS_ASYNC");
+        pl->thomas_async = ta ? atoi(ta) : -1;
         // PRJ_OVERLAP_CHUNKS: y chunks of the overlapped projection schedule; off by default
         // (measured on B200 at 768x384x384: 4.16 ms sequential, 4.18 / 4.27 / 4.35 ms with
         // 2 / 4 / 8 chunks -- every kernel already fills the GPU)

@@ -111,6 +111,8 @@ struct prj_plan {
     int zfft_rows = 0;            // rows per CTA of the z-transform kernels (0: default rule)
     int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
     bool use_pass = true;         // compile-time pass-plan FFT kernels where the length has one
+    int thomas_async = -1;        // Thomas lines streamed through a cp.async shared-memory ring:
+                                  // -1 for the mixed storage only, 0 never, 1..4 always (ring shape)
     int x_staged = 0;             // divergence rows staged by bulk copies (persistent x-forward kernel):
                                   // 0 off, else its threads per CTA (128 or 256)
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels

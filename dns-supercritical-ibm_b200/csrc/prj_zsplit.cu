@@ -187,9 +187,169 @@ __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same line solve with the planes streamed through a ring of NS shared-memory
+// stages of B planes by cp.async (global -> shared, no register staging): while a
+// thread computes block b it already has blocks b+1 .. b+NS-1 in flight, so the
+// sequential recurrence no longer waits on one memory round trip per block.  Each
+// thread copies exactly the elements it consumes (its own line), so a thread only
+// waits for its own copy groups and no CTA barrier is needed.  Arithmetic and
+// order are those of thomas_line, so the results are bit-identical.
+__device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    if (bytes == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T, int B, int NS>
+__device__ __forceinline__ void thomas_line_async(const ThomasArgs& a, int blk, unsigned char* sm) {
+    const int kb = blk / a.tiles;
+    const int kx = a.kx0 + kb;
+    const int slot = (blk - kb * a.tiles) * kThomasTile + threadIdx.x;
+    if (slot >= a.nz) return;  // a thread leaves only its own copy groups behind: none issued
+    const int nz = a.nz, ny = a.ny, nh = a.nh, mzp = a.mzp, tid = threadIdx.x;
+    const int kz = a.kz_of_slot[slot];
+    const int kzs = kz <= nz - kz ? kz : nz - kz;
+    const bool is00 = (kx == 0 && kz == 0);
+    const double* A = a.bands + (is00 ? 3 : 0) * ny;
+    const double* C = a.bands + (is00 ? 5 : 2) * ny;
+    const size_t rstride = (size_t)a.nhb * nz;
+    const size_t pstride = (size_t)nh * mzp;
+    T* x = static_cast<T*>(a.X) + (size_t)kb * nz + slot;
+    const double* d = a.piv + (size_t)kx * mzp + kzs;
+    T* Xs = reinterpret_cast<T*>(sm);                                        // [NS][B][tile]
+    double* Ds = reinterpret_cast<double*>(sm + (size_t)NS * B * kThomasTile * sizeof(T));  // [NS][B][tile]
+    auto xs = [&](int st, int u) -> T& { return Xs[((size_t)st * B + u) * kThomasTile + tid]; };
+    auto ds = [&](int st, int u) -> double& { return Ds[((size_t)st * B + u) * kThomasTile + tid]; };
+    const int nb = (ny + B - 1) / B;
+
+    // forward sweep, y ascending: block b = planes b B .. b B + B - 1
+    auto issue_f = [&](int b) {
+        if (b < nb) {
+            const int st = b % NS;
+            for (int u = 0; u < B; u++) {
+                const int y = b * B + u;
+                if (y < ny) {
+                    cp_async(&xs(st, u), x + (size_t)y * rstride, (int)sizeof(T));
+                    cp_async(&ds(st, u), d + (size_t)y * pstride, 8);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int b = 0; b < NS - 1; b++) issue_f(b);
+    double2 prev = make_double2(0.0, 0.0);
+    for (int b = 0; b < nb; b++) {
+        issue_f(b + NS - 1);
+        cp_async_wait<NS - 1>();
+        const int st = b % NS;
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int y = b * B + u;
+            if (y < ny) {
+                double2 r = to_d2(xs(st, u));
+                const double D = ds(st, u);
+                if (y == 0) {
+                    r.x = __ddiv_rn(r.x, D);
+                    r.y = __ddiv_rn(r.y, D);
+                } else {
+                    const double av = A[y];
+                    r.x = __ddiv_rn(__dsub_rn(r.x, __dmul_rn(av, prev.x)), D);
+                    r.y = __ddiv_rn(__dsub_rn(r.y, __dmul_rn(av, prev.y)), D);
+                }
+                prev = r;
+                if (y < ny - 1) from_d2(x[(size_t)y * rstride], r);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    // the backward sweep reads what this thread just stored: complete those stores first
+    __threadfence();
+    from_d2(x[(size_t)(ny - 1) * rstride], prev);
+    // backward sweep, y descending from ny-2: block b = planes ny-2 - b B - u
+    const int nbb = (ny - 1 + B - 1) / B;
+    auto issue_b = [&](int b) {
+        if (b < nbb) {
+            const int st = b % NS;
+            for (int u = 0; u < B; u++) {
+                const int y = ny - 2 - b * B - u;
+                if (y >= 0) {
+                    cp_async(&xs(st, u), x + (size_t)y * rstride, (int)sizeof(T));
+                    cp_async(&ds(st, u), d + (size_t)y * pstride, 8);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int b = 0; b < NS - 1; b++) issue_b(b);
+    for (int b = 0; b < nbb; b++) {
+        issue_b(b + NS - 1);
+        cp_async_wait<NS - 1>();
+        const int st = b % NS;
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int y = ny - 2 - b * B - u;
+            if (y >= 0) {
+                const double c = __ddiv_rn(C[y], ds(st, u));
+                const double2 v = to_d2(xs(st, u));
+                double2 r;
+                r.x = __dsub_rn(v.x, __dmul_rn(prev.x, c));
+                r.y = __dsub_rn(v.y, __dmul_rn(prev.y, c));
+                prev = r;
+                from_d2(x[(size_t)y * rstride], r);
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// ring shape (planes per stage B x stages NS) of the streamed kernel
+template <typename T, int B, int NS>
+constexpr size_t thomas_async_smem() {
+    return (size_t)NS * B * kThomasTile * (sizeof(T) + sizeof(double));
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThomasTile) k_thomas(const ThomasArgs a) {
     thomas_line<T>(a, blockIdx.x);
+}
+
+template <typename T, int B, int NS>
+__global__ void __launch_bounds__(kThomasTile) k_thomas_async(const ThomasArgs a) {
+    extern __shared__ __align__(16) unsigned char tsm[];
+    thomas_line_async<T, B, NS>(a, blockIdx.x, tsm);
+}
+
+template <int B, int NS>
+__global__ void __launch_bounds__(kThomasTile) k_thomas_mixed_async(const ThomasArgs a64, const ThomasArgs a32,
+                                                                    int nblk64) {
+    extern __shared__ __align__(16) unsigned char tsm[];
+    if ((int)blockIdx.x < nblk64) thomas_line_async<double2, B, NS>(a64, blockIdx.x, tsm);
+    else thomas_line_async<float2, B, NS>(a32, blockIdx.x - nblk64, tsm);
+}
+
+template <typename T, int B, int NS>
+cudaError_t launch_thomas_async(const ThomasArgs& t, unsigned grid, cudaStream_t st) {
+    constexpr size_t smem = thomas_async_smem<T, B, NS>();
+    const cudaError_t e = allow_smem(k_thomas_async<T, B, NS>, smem);
+    if (e != cudaSuccess) return e;
+    k_thomas_async<T, B, NS><<<grid, kThomasTile, smem, st>>>(t);
+    return cudaGetLastError();
+}
+
+template <int B, int NS>
+cudaError_t launch_thomas_mixed_async(const ThomasArgs& a64, const ThomasArgs& a32, int nblk64, unsigned grid,
+                                      cudaStream_t st) {
+    constexpr size_t smem = thomas_async_smem<double2, B, NS>();
+    const cudaError_t e = allow_smem(k_thomas_mixed_async<B, NS>, smem);
+    if (e != cudaSuccess) return e;
+    k_thomas_mixed_async<B, NS><<<grid, kThomasTile, smem, st>>>(a64, a32, nblk64);
+    return cudaGetLastError();
 }
 
 // mixed storage in one launch: blocks [0, nblk64) solve the FP64 rows (a64), the
@@ -304,7 +464,15 @@ template <typename T>
 cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_plane, cudaStream_t st) {
     if (rows_per_plane <= 0) return cudaSuccess;
     const ThomasArgs t = thomas_args(pl, X, kx0, rows_per_plane);
-    k_thomas<T><<<(unsigned)(rows_per_plane * t.tiles), kThomasTile, 0, st>>>(t);
+    const unsigned grid = (unsigned)(rows_per_plane * t.tiles);
+    switch (pl->thomas_async > 0 ? pl->thomas_async : 0) {
+    case 1: return launch_thomas_async<T, 4, 4>(t, grid, st);
+    case 2: return launch_thomas_async<T, 8, 2>(t, grid, st);
+    case 3: return launch_thomas_async<T, 2, 8>(t, grid, st);
+    case 4: return launch_thomas_async<T, 8, 3>(t, grid, st);
+    default: break;
+    }
+    k_thomas<T><<<grid, kThomasTile, 0, st>>>(t);
     return cudaGetLastError();
 }
 
@@ -333,7 +501,17 @@ cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st) {
     const ThomasArgs a64 = thomas_args(pl, pl->spec, 0, pl->kxs);
     const ThomasArgs a32 = thomas_args(pl, pl->spec32, pl->kxs, rows32);
     const int nblk64 = pl->kxs * a64.tiles;
-    k_thomas_mixed<<<(unsigned)(nblk64 + rows32 * a32.tiles), kThomasTile, 0, st>>>(a64, a32, nblk64);
+    const unsigned grid = (unsigned)(nblk64 + rows32 * a32.tiles);
+    // the mixed storage streams by default (measured 0.69 ms against 1.10 ms per solve at
+    // 768x384x384); PRJ_THOMAS_ASYNC=0 keeps the register-prefetch kernel
+    switch (pl->thomas_async) {
+    case 0: break;
+    case 2: return launch_thomas_mixed_async<8, 2>(a64, a32, nblk64, grid, st);
+    case 3: return launch_thomas_mixed_async<2, 8>(a64, a32, nblk64, grid, st);
+    case 4: return launch_thomas_mixed_async<8, 3>(a64, a32, nblk64, grid, st);
+    default: return launch_thomas_mixed_async<4, 4>(a64, a32, nblk64, grid, st);
+    }
+    k_thomas_mixed<<<grid, kThomasTile, 0, st>>>(a64, a32, nblk64);
     return cudaGetLastError();
 }
 

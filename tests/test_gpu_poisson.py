@@ -161,3 +161,25 @@ def test_residual_at_large_size(cuda_device):
         res = float(torch.linalg.vector_norm(Lp - r) / torch.linalg.vector_norm(r))
     # round-off of the stencil itself is ~ eps * (4/dx^2) |p| / |b|
     assert res < 1e-10, res
+
+
+@pytest.mark.parametrize("shape", [(64, 48, 32), (96, 130, 40), (128, 384, 64)])
+def test_streamed_thomas_is_bitwise_register_thomas(cuda_device, monkeypatch, shape):
+    """The cp.async-streamed Thomas kernel keeps the operation order of the register-prefetch
+    kernel: FP64 solves and FP32-storage solves agree bit for bit (ny not a multiple of the
+    4-plane blocks included)."""
+    import prj
+    import workloads
+    nx, ny, nz = shape
+    rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=12)
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("PRJ_THOMAS_ASYNC", flag)
+        with prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent")) as plan:
+            t = to_dev(rhs)
+            plan.poisson_fp64(t)
+            t2 = to_dev(rhs)
+            plan.poisson_mixed(t2)
+            out[flag] = (from_dev(t), from_dev(t2))
+    for a, b in zip(out["0"], out["1"]):
+        np.testing.assert_array_equal(a, b)
