@@ -184,6 +184,7 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->kz_of_slot);
     dfree(pl->spec32);
     dfree(pl->pbar);
+    dfree(pl->psum);
     dfree(pl->mix_b);
     dfree(pl->mix_r);
     pl->xd.ok = pl->zd.ok = false;
@@ -306,6 +307,36 @@ int run_zsolve_mixed(prj_plan* pl, cudaStream_t st) {
     return PRJ_OK;
 }
 
+// inverse x transform that also leaves per-tile sums of P for the next plane means
+// (pass-plan kernel); falls back to the plain transform (psum_valid = false)
+cudaError_t bwd_with_sums(prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq) {
+    // capacity for the current tiling (x_rows may change it); allocated outside any capture
+    // because the batched graphs run every case once before capturing
+    const size_t need = (size_t)pl->g.ny * prj::bwd_tiles_per_plane(pl);
+    if (pl->psum_elems < need) {
+        dfree(pl->psum);
+        pl->psum = nullptr;
+        pl->device_bytes -= pl->psum_elems * sizeof(double);
+        pl->psum_elems = 0;
+        const cudaError_t e = cudaMalloc((void**)&pl->psum, need * sizeof(double));
+        if (e != cudaSuccess) {
+            pl->psum = nullptr;
+            return e;
+        }
+        pl->psum_elems = need;
+        pl->device_bytes += need * sizeof(double);
+    }
+    if (pl->psum) {
+        const cudaError_t e = prj::launch_bwd_xd(pl, P, st, accum, sq, prj::YRange{}, pl->psum);
+        if (e != cudaErrorNotSupported) {
+            pl->psum_valid = (e == cudaSuccess);
+            return e;
+        }
+    }
+    pl->psum_valid = false;
+    return prj::launch_bwd_xd(pl, P, st, accum, sq);
+}
+
 // FP32-storage solve with FP64 refinement: p = solve(b); repeat mixed_iters times
 // { r = b - A p; p += solve(r) }.  The right-hand side is the divergence of
 // (Uh, Vh, Wh) when Uh is given, else the incoming P.  b and r are scratch fields
@@ -330,13 +361,17 @@ int run_mixed_core(prj_plan* pl, const double* Uh, const double* Vh, const doubl
     if ((rc = run_zsolve_mixed(pl, st))) return rc;
     {
         StageTimer tm(pl, prj::kStBwdX, st);
-        CK(prj::launch_bwd_xd(pl, P, st, 0, nullptr), "inverse x");
+        CK(bwd_with_sums(pl, P, st, 0, nullptr), "inverse x");
     }
     for (int it = 1; it <= pl->mixed_iters; it++) {
         const bool last = (it == pl->mixed_iters);
         {
             StageTimer tm(pl, prj::kStResidual, st);
-            CK(prj::launch_plane_mean(pl, P, pl->pbar, st), "plane means");
+            if (pl->psum_valid)
+                CK(prj::launch_plane_mean_partials(pl, pl->psum, prj::bwd_tiles_per_plane(pl), pl->pbar, st),
+                   "plane means");
+            else
+                CK(prj::launch_plane_mean(pl, P, pl->pbar, st), "plane means");
             CK(prj::launch_residual(pl, b, P, pl->pbar, r, st), "residual");
         }
         {
@@ -347,7 +382,7 @@ int run_mixed_core(prj_plan* pl, const double* Uh, const double* Vh, const doubl
         if (last) CK(cudaMemsetAsync(pl->stat_buf + 4, 0, 2 * sizeof(double), st), "norm slots");
         {
             StageTimer tm(pl, prj::kStBwdX, st);
-            CK(prj::launch_bwd_xd(pl, P, st, 1, last ? pl->stat_buf + 4 : nullptr), "inverse x");
+            CK(bwd_with_sums(pl, P, st, 1, last ? pl->stat_buf + 4 : nullptr), "inverse x");
         }
     }
     return PRJ_OK;

@@ -106,6 +106,9 @@ struct prj_plan {
     int mixed_iters = 2;          // refinement iterations of the mixed path
     float2* spec32 = nullptr;     // FP32 spectral rows of the mixed path
     double* pbar = nullptr;       // per-plane means of P (ny) for the mixed-path residual
+    double* psum = nullptr;       // per-CTA partial sums of P from the inverse x kernel (ny x tiles)
+    size_t psum_elems = 0;
+    bool psum_valid = false;      // psum holds the sums of the P last written by the inverse x kernel
     double* mix_b = nullptr;      // Poisson-only mixed solve: copy of the right-hand side
     double* mix_r = nullptr;      // Poisson-only mixed solve: residual
     int zfft_rows = 0;            // rows per CTA of the z-transform kernels (0: default rule)
@@ -163,8 +166,11 @@ cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStrea
 cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, const double* Uh, const double* Vh,
                           const double* Wh, const StepScalars* sc, cudaStream_t st, double* bout = nullptr,
                           YRange yr = YRange{});
+// psum: per-CTA sums of the written P, [y][tile] (pass-plan kernel only; otherwise
+// cudaErrorNotSupported and nothing launched)
 cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum = 0, double* sq = nullptr,
-                          YRange yr = YRange{});
+                          YRange yr = YRange{}, double* psum = nullptr);
+int bwd_tiles_per_plane(const prj_plan* pl);
 inline cudaError_t launch_fwd_x_range(const prj_plan* pl, const double* Uh, const double* Vh, const double* Wh,
                                       const StepScalars* sc, cudaStream_t st, YRange yr) {
     return launch_fwd_xd(pl, FwdSource::Divergence, nullptr, Uh, Vh, Wh, sc, st, nullptr, yr);
@@ -181,6 +187,9 @@ cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st);
 cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st);
 // residual r = b - A p of the pinned operator and the per-plane means it needs (prj_mixed.cu)
 cudaError_t launch_plane_mean(const prj_plan* pl, const double* P, double* pbar, cudaStream_t st);
+// plane means from the inverse x kernel's partial sums ([ny][tiles])
+cudaError_t launch_plane_mean_partials(const prj_plan* pl, const double* psum, int tiles, double* pbar,
+                                       cudaStream_t st);
 cudaError_t launch_residual(const prj_plan* pl, const double* B, const double* P, const double* pbar, double* R,
                             cudaStream_t st);
 

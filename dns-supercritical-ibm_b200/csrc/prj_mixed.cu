@@ -33,6 +33,15 @@ __global__ void __launch_bounds__(256) k_plane_mean(int nx, int nz, const double
     if (threadIdx.x == 0) pm[k] = red[0] / (double)n;
 }
 
+// pm[k] = (sum of the inverse x kernel's tile sums of plane k, in tile order) / (nx nz)
+__global__ void k_plane_mean_partials(int ny, int tiles, double inv_n, const double* __restrict__ ps, double* pm) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ny) return;
+    double s = 0.0;
+    for (int t = 0; t < tiles; t++) s += ps[(size_t)k * tiles + t];
+    pm[k] = s * inv_n;
+}
+
 struct ResArgs {
     int nx, nz, ny;
     double idx2, idz2;
@@ -75,6 +84,14 @@ __global__ void __launch_bounds__(128) k_residual(const ResArgs a) {
 
 cudaError_t launch_plane_mean(const prj_plan* pl, const double* P, double* pbar, cudaStream_t st) {
     k_plane_mean<<<pl->g.ny, 256, 0, st>>>(pl->g.nx, pl->g.nz, P, pbar);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plane_mean_partials(const prj_plan* pl, const double* psum, int tiles, double* pbar,
+                                       cudaStream_t st) {
+    const int ny = pl->g.ny;
+    k_plane_mean_partials<<<(ny + 127) / 128, 128, 0, st>>>(ny, tiles, 1.0 / ((double)pl->g.nx * pl->g.nz), psum,
+                                                          pbar);
     return cudaGetLastError();
 }
 

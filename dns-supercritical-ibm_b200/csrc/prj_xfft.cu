@@ -46,6 +46,7 @@ struct XArgs {
     float2* X32;     // FP32 rows kx >= kxs: X32[(y (nh - kxs) + kx - kxs) nz + z]
     int kxs;         // nh on the FP64 path
     int y0;          // first y plane of this launch (grid.y planes from y0)
+    double* psum;    // k_bwd_xp: per-CTA sums of the written P values, [y][blockIdx.x], or null
     double* Pout;
     double* Bout;    // k_fwd_xd: copy of the source field (P layout), or null
     int accum;       // k_bwd_xd: Pout += result instead of Pout = result
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_bwd_xp(const XA
     __syncthreads();
     dit_passes_shared<+1, PL, PL::P - 1, 0>(A, nr, rs, a.tw);
     double2* out = reinterpret_cast<double2*>(a.Pout) + ((size_t)y * a.nz + z0) * m;
-    double sq0 = 0.0, sq1 = 0.0;
+    double sq0 = 0.0, sq1 = 0.0, ps = 0.0;
     dit_last_pass<+1, PL>(A, nr, rs, a.tw, [&](int r, int e, double2 v) {
         double2* o = out + (size_t)r * m + e;
         if (a.accum) {
@@ -567,11 +568,25 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_bwd_xp(const XA
             const double2 nv = make_double2(old.x + v.x, old.y + v.y);
             sq0 += v.x * v.x + v.y * v.y;
             sq1 += nv.x * nv.x + nv.y * nv.y;
+            ps += nv.x + nv.y;
             *o = nv;
         } else {
+            ps += v.x + v.y;
             *o = v;
         }
     });
+    if (a.psum) {
+        // the tile's sum in a fixed order (per thread, then warp butterfly, then warps in order)
+        __shared__ double wsum[kPassThreads / 32];
+        for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
+        if ((tid & 31) == 0) wsum[tid >> 5] = ps;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < nthr / 32; w++) t += wsum[w];
+            a.psum[(size_t)y * gridDim.x + blockIdx.x] = t;
+        }
+    }
     if (a.sq) {
         for (int o = 16; o > 0; o >>= 1) {
             sq0 += __shfl_xor_sync(0xffffffffu, sq0, o);
@@ -610,6 +625,9 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 }
 
 }  // namespace
+
+// CTAs per y plane of the pass-plan inverse x kernel (the width of its partial sums)
+int bwd_tiles_per_plane(const prj_plan* pl) { return (pl->g.nz + pl->tz_xp - 1) / pl->tz_xp; }
 
 // rows per CTA of the pass-plan x kernels: a power of two up to 16 whose padded rows
 // (stride m + 1) fit 28 KB, so that 7-8 CTAs share an SM
@@ -770,8 +788,10 @@ cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq, YRange yr) {
+cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq, YRange yr,
+                          double* psum) {
     XArgs a = make_args(pl);
+    a.psum = psum;
     yr = yr.resolved(pl->g.ny);
     a.y0 = yr.y0;
     a.Pout = P;
@@ -782,6 +802,7 @@ cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int ac
         const cudaError_t e2 = launch_xpass(pl, false, FwdSource::Pressure, a, yr.y1 - yr.y0, st);
         if (e2 != cudaErrorNotSupported) return e2;
     }
+    if (psum) return cudaErrorNotSupported;  // partial sums come from the pass-plan kernel only
     const size_t smem = smem_bytes(a);
     cudaError_t e = allow_smem(k_bwd_xd, smem);
     if (e != cudaSuccess) return e;
