@@ -191,6 +191,18 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->spec);
     dfree(pl->stat_buf);
     dfree(pl->vd_pad);
+    for (cudaStream_t& hs : pl->hp_st) {
+        if (hs) cudaStreamSynchronize(hs);
+    }
+    for (double*& hb : pl->hp_stage) dfree(hb);
+    for (cudaEvent_t& he : pl->hp_ev) {
+        if (he) cudaEventDestroy(he);
+        he = nullptr;
+    }
+    for (cudaStream_t& hs : pl->hp_st) {
+        if (hs) cudaStreamDestroy(hs);
+        hs = nullptr;
+    }
     for (cudaEvent_t e : pl->ov_ev) cudaEventDestroy(e);
     pl->ov_ev.clear();
     for (cudaStream_t& s : pl->ov_st) {
@@ -1082,6 +1094,69 @@ int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h
     CK(cudaMemcpy(h_V, dV, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy V");
     CK(cudaMemcpy(h_W, dW, nh * sizeof(double), cudaMemcpyDeviceToHost), "copy W");
     CK(cudaMemcpy(h_P, dP, np * sizeof(double), cudaMemcpyDeviceToHost), "copy P");
+    return PRJ_OK;
+}
+
+int prj_projection_step_host_async(prj_plan* plan, const double* h_Uh, const double* h_Vh, const double* h_Wh,
+                                   double* h_U, double* h_V, double* h_W, double* h_P,
+                                   const prj_step_params* params, int mode) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    if (!h_Uh || !h_Vh || !h_Wh || !h_U || !h_V || !h_W || !h_P || !params) return fail(PRJ_ERR_ARG, "NULL argument");
+    DeviceGuard dg(plan->device);
+    const prj::Geometry& g = plan->g;
+    const size_t nh = (size_t)(g.nx + 2) * (g.nz + 2) * (g.ny + 2);
+    const size_t np = (size_t)g.nx * g.nz * g.ny;
+    const size_t elems = 6 * nh + np;
+    if (plan->hp_elems < elems) {
+        for (cudaStream_t hs : plan->hp_st)
+            if (hs) CK(cudaStreamSynchronize(hs), "pipeline drain");
+        for (double*& hb : plan->hp_stage) {
+            dfree(hb);
+            CK(cudaMalloc((void**)&hb, elems * sizeof(double)), "cudaMalloc(pipeline staging)");
+        }
+        plan->hp_elems = elems;
+    }
+    for (cudaStream_t& hs : plan->hp_st)
+        if (!hs) CK(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking), "pipeline stream");
+    for (cudaEvent_t& he : plan->hp_ev)
+        if (!he) CK(cudaEventCreateWithFlags(&he, cudaEventDisableTiming), "pipeline event");
+    const int k = (int)(plan->hp_n & 1);
+    cudaStream_t sin = plan->hp_st[0], scmp = plan->hp_st[1], sout = plan->hp_st[2];
+    cudaEvent_t in_done = plan->hp_ev[k], cmp_done = plan->hp_ev[2 + k], out_done = plan->hp_ev[4 + k];
+    double* d = plan->hp_stage[k];
+    double *dUh = d, *dVh = d + nh, *dWh = d + 2 * nh, *dU = d + 3 * nh, *dV = d + 4 * nh, *dW = d + 5 * nh,
+           *dP = d + 6 * nh;
+    // copy-in: the slot's inputs are free once its previous solve is done
+    CK(cudaStreamWaitEvent(sin, cmp_done, 0), "pipeline order");
+    CK(cudaMemcpyAsync(dUh, h_Uh, nh * sizeof(double), cudaMemcpyHostToDevice, sin), "copy Uh");
+    CK(cudaMemcpyAsync(dVh, h_Vh, nh * sizeof(double), cudaMemcpyHostToDevice, sin), "copy Vh");
+    CK(cudaMemcpyAsync(dWh, h_Wh, nh * sizeof(double), cudaMemcpyHostToDevice, sin), "copy Wh");
+    CK(cudaEventRecord(in_done, sin), "pipeline event");
+    // solve: after the inputs, and after the slot's previous outputs were read out
+    CK(cudaStreamWaitEvent(scmp, in_done, 0), "pipeline order");
+    CK(cudaStreamWaitEvent(scmp, out_done, 0), "pipeline order");
+    prj_step_params p = *params;
+    p.compute_stats = 0;
+    if ((rc = prj_projection_step(plan, dUh, dVh, dWh, dU, dV, dW, dP, &p, mode, nullptr, scmp))) return rc;
+    CK(cudaEventRecord(cmp_done, scmp), "pipeline event");
+    // copy-out
+    CK(cudaStreamWaitEvent(sout, cmp_done, 0), "pipeline order");
+    CK(cudaMemcpyAsync(h_U, dU, nh * sizeof(double), cudaMemcpyDeviceToHost, sout), "copy U");
+    CK(cudaMemcpyAsync(h_V, dV, nh * sizeof(double), cudaMemcpyDeviceToHost, sout), "copy V");
+    CK(cudaMemcpyAsync(h_W, dW, nh * sizeof(double), cudaMemcpyDeviceToHost, sout), "copy W");
+    CK(cudaMemcpyAsync(h_P, dP, np * sizeof(double), cudaMemcpyDeviceToHost, sout), "copy P");
+    CK(cudaEventRecord(out_done, sout), "pipeline event");
+    plan->hp_n++;
+    return PRJ_OK;
+}
+
+int prj_host_async_wait(prj_plan* plan) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    DeviceGuard dg(plan->device);
+    for (cudaStream_t hs : plan->hp_st)
+        if (hs) CK(cudaStreamSynchronize(hs), "pipeline wait");
     return PRJ_OK;
 }
 

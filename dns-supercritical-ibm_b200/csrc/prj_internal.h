@@ -86,6 +86,12 @@ struct prj_plan {
     std::vector<cudaEvent_t> event_pool;     // reusable events
     double* host_stage = nullptr;            // device staging of the host-buffer entry points
     size_t host_stage_elems = 0;
+    // pipelined host-buffer steps: two staging slots, copy-in / compute / copy-out streams
+    double* hp_stage[2] = {nullptr, nullptr};
+    size_t hp_elems = 0;
+    cudaStream_t hp_st[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t hp_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // in[2], cmp[2], out[2]
+    long long hp_n = 0;
     unsigned flags = 0;
     bool has_metrics = false;
     prj::Geometry g{};

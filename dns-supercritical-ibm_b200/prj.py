@@ -55,6 +55,7 @@ EXPORTS = (
     "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
     "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
     "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
+    "prj_projection_step_host_async", "prj_host_async_wait",
 )
 
 BANDS_REFERENCE = 0
@@ -146,6 +147,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
     L.prj_plan_schedule.argtypes = [_vp, i, ctypes.POINTER(i), ctypes.POINTER(i)]
+    L.prj_projection_step_host_async.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.POINTER(StepParams), i]
+    L.prj_host_async_wait.argtypes = [_vp]
     L.prj_rough_force.argtypes = [i, i, i, _vp, _vp, _vp, ctypes.POINTER(RoughInds), ctypes.POINTER(StepParams), _vp]
     ll = ctypes.c_longlong
     L.prj_ibm_interp.argtypes = [_vp, ll, i, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp, _vp, _vp, _vp]
@@ -264,6 +267,24 @@ class Plan:
         plan = cls(nx, nz, len(yu) - 1, dx, dz, bands(yu, band_mode), metrics(yu), device)
         plan.set_vd_metric(vd_metric(yu))
         return plan
+
+    def projection_step_host_async(self, Uh, Vh, Wh, U, V, W, P, dt, mode=MODE_FP64, wall=(0.0,) * 6):
+        """Enqueue one pipelined host-buffer step (prj_projection_step_host_async); numpy
+        Fortran-ordered arrays as for projection_step, ideally in pinned memory.  Call
+        host_async_wait() before reading the outputs or reusing the buffers."""
+        g = self.grid
+        hs = (g.nx + 2, g.nz + 2, g.ny + 2)
+        for a in (Uh, Vh, Wh, U, V, W):
+            if not (a.dtype == np.float64 and a.flags.f_contiguous and a.shape == hs):
+                raise ValueError(f"halo'd fields must be Fortran-ordered float64 arrays of shape {hs}")
+        if not (P.dtype == np.float64 and P.flags.f_contiguous and P.shape == (g.nx, g.nz, g.ny)):
+            raise ValueError("P must be a Fortran-ordered float64 array of shape (nx, nz, ny)")
+        par = StepParams(float(dt), *[float(w) for w in wall], 0)
+        _check(load_library().prj_projection_step_host_async(self.handle, _p(Uh), _p(Vh), _p(Wh), _p(U), _p(V),
+                                                             _p(W), _p(P), ctypes.byref(par), mode))
+
+    def host_async_wait(self):
+        _check(load_library().prj_host_async_wait(self.handle))
 
     def schedule(self, mode=MODE_FP64):
         """(kernel launches per projection step, overlapped y chunks) (prj_plan_schedule)."""

@@ -128,6 +128,21 @@ int prj_projection_step_host(prj_plan* plan, const double* h_Uh, const double* h
                              const prj_step_params* params, int mode, prj_stats* stats);
 
 /*
+ * Pipelined form of prj_projection_step_host for a sequence of steps from host
+ * memory: the call only enqueues (no statistics) and returns.  Two device staging
+ * slots alternate, and the copy-in, the solve and the copy-out run on three
+ * plan-owned streams ordered by events, so the device-to-host copy of one step
+ * overlaps the host-to-device copy of the next on the two copy engines.  The host
+ * buffers of a step must stay valid and untouched until prj_host_async_wait
+ * returns (or, for the inputs, until two later steps were enqueued); use pinned
+ * host memory, as pageable memory makes the copies synchronous.
+ */
+int prj_projection_step_host_async(prj_plan* plan, const double* h_Uh, const double* h_Vh, const double* h_Wh,
+                                   double* h_U, double* h_V, double* h_W, double* h_P,
+                                   const prj_step_params* params, int mode);
+int prj_host_async_wait(prj_plan* plan);
+
+/*
  * Poisson solve in place with FP32 spectral storage and FP64 iterative
  * refinement (the precision scheme of PRJ_MODE_FP32_REFINE): rows of
  * x-wavenumbers whose tridiagonals are badly conditioned stay FP64, the

@@ -136,3 +136,32 @@ def test_overlapped_schedule_is_bitwise_sequential(cuda_device, monkeypatch, chu
             outs.append(run_engine(plan, Uh, Vh, Wh, 0.9, wall))
     for a, b in zip(outs[0][:4], outs[1][:4]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_pipelined_host_steps_match_sync(cuda_device):
+    """Three pipelined host-buffer steps (alternating staging slots) give the synchronous call's
+    outputs bit for bit."""
+    import prj
+    import torch
+    import workloads
+    nx, ny, nz = 64, 48, 32
+    cases = [workloads.projection_inputs(nx, ny, nz, seed=s) for s in (21, 22, 23)]
+    yu, dx, dz = cases[0][3:]
+    pin = lambda shape: torch.empty(tuple(reversed(shape)), dtype=torch.float64).pin_memory().numpy().T
+    hs = (nx + 2, nz + 2, ny + 2)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        ins, outs = [], []
+        for Uh, Vh, Wh, *_ in cases:
+            bufs = [pin(hs) for _ in range(3)]
+            for b, a in zip(bufs, (Uh, Vh, Wh)):
+                b[...] = a
+            ins.append(bufs)
+            outs.append([pin(hs) for _ in range(3)] + [pin((nx, nz, ny))])
+        for i, o in zip(ins, outs):
+            plan.projection_step_host_async(*i, *o, 0.8)
+        plan.host_async_wait()
+        for (Uh, Vh, Wh, *_), o in zip(cases, outs):
+            want = [np.zeros(hs, order="F") for _ in range(3)] + [np.zeros((nx, nz, ny), order="F")]
+            plan.projection_step(Uh, Vh, Wh, *want, 0.8, stats=False)
+            for a, b in zip(o, want):
+                np.testing.assert_array_equal(a, b)
