@@ -191,6 +191,7 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->spec);
     dfree(pl->stat_buf);
     dfree(pl->vd_pad);
+    dfree(pl->vd_ih);
     for (cudaStream_t& hs : pl->hp_st) {
         if (hs) cudaStreamSynchronize(hs);
     }
@@ -1014,9 +1015,15 @@ int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_V
     sc.wall[3] = params->wall_U_top; sc.wall[4] = params->wall_V_top; sc.wall[5] = params->wall_W_top;
     const prj::VdFields f{vd->rho, vd->P_now, vd->P_old, vd->div_now, vd->P_next};
     unsigned long long* slot = reinterpret_cast<unsigned long long*>(plan->stat_buf + prj::kStatRhoSlot);
+    if (!plan->vd_ih) {
+        const size_t nh = (size_t)(plan->g.nx + 2) * (plan->g.nz + 2) * (plan->g.ny + 2);
+        CK(cudaMalloc((void**)&plan->vd_ih, nh * sizeof(double)), "cudaMalloc(0.5 / rho)");
+        plan->device_bytes += nh * sizeof(double);
+    }
     {
         StageTimer tm(plan, prj::kStVdRhs, st);
         CK(prj::launch_vd_rho_min(plan, vd->rho, slot, st), "rho_min");
+        CK(prj::launch_vd_half_inv(plan, vd->rho, plan->vd_ih, st), "0.5 / rho");
         CK(prj::launch_vd_rhs(plan, d_Uh, d_Vh, d_Wh, f, sc, slot, d_P, st), "variable-density right-hand side");
     }
     if (mode == PRJ_MODE_FP32_REFINE) {

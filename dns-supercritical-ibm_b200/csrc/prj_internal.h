@@ -126,6 +126,7 @@ struct prj_plan {
                                   // 0 off, else its threads per CTA (128 or 256)
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
     double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
+    double* vd_ih = nullptr;      // 0.5 / rho (halo'd) of the variable-density step (scratch)
     int overlap_chunks = 0;       // y chunks of the overlapped projection schedule (0: sequential)
     cudaStream_t ov_st[2] = {nullptr, nullptr};  // its two helper streams (created on first use)
     std::vector<cudaEvent_t> ov_ev;              // its events
@@ -213,6 +214,7 @@ struct VdFields {
     double* P_next;
 };
 cudaError_t launch_vd_rho_min(const prj_plan* pl, const double* rho, unsigned long long* slot, cudaStream_t st);
+cudaError_t launch_vd_half_inv(const prj_plan* pl, const double* rho, double* ih, cudaStream_t st);
 cudaError_t launch_vd_rhs(const prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, const VdFields& f,
                           const StepScalars& sc, const unsigned long long* slot, double* P, cudaStream_t st);
 cudaError_t launch_vd_correction(const prj_plan* pl, const double* P, const double* Uh, const double* Vh,

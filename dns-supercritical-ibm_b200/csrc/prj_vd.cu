@@ -46,12 +46,20 @@ __global__ void k_rho_min(int nx, int nz, int ny, const double* __restrict__ rho
     if ((threadIdx.x & 31) == 0) atomicMin(out, ord_of(m));
 }
 
+// ih = 0.5 / rho on the whole halo'd box (the quotient both stencils form for every
+// neighbour; computed once, the same correctly rounded values)
+__global__ void k_half_inv(size_t n, const double* __restrict__ rho, double* __restrict__ ih) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        ih[i] = __ddiv_rn(0.5, rho[i]);
+}
+
 struct VdArgs {
     int nx, nz, ny;
     const double* Uh;
     const double* Vh;
     const double* Wh;
     const double* rho;
+    const double* ih;       // 0.5 / rho (halo'd)
     const double* Pn;
     const double* Po;
     const double* div_now;
@@ -78,7 +86,6 @@ __device__ __forceinline__ double ps(const VdArgs& a, size_t h) {
 __device__ __forceinline__ double rho_w(double rmin, double hn, double hc) {
     return __dsub_rn(1.0, __dmul_rn(rmin, __dadd_rn(hn, hc)));
 }
-__device__ __forceinline__ double half_inv(double r) { return __ddiv_rn(0.5, r); }
 
 // RHS of the constant-coefficient Poisson equation, one CTA per (y, z) row
 __global__ void __launch_bounds__(128) k_vd_rhs(const VdArgs a) {
@@ -99,14 +106,14 @@ __global__ void __launch_bounds__(128) k_vd_rhs(const VdArgs a) {
         const size_t hzp = hix(nx, nz, i, j + 1, k), hzm = hix(nx, nz, i, j - 1, k);
         const size_t hyp = hix(nx, nz, i, j, k + 1), hym = hix(nx, nz, i, j, k - 1);
         const double p00 = ps(a, h);
-        const double h0 = half_inv(a.rho[h]);
-        const double X = __dsub_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hxp]), h0), __dsub_rn(ps(a, hxp), p00)),
-                                   __dmul_rn(rho_w(rmin, half_inv(a.rho[hxm]), h0), __dsub_rn(p00, ps(a, hxm))));
-        const double Z = __dsub_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hzp]), h0), __dsub_rn(ps(a, hzp), p00)),
-                                   __dmul_rn(rho_w(rmin, half_inv(a.rho[hzm]), h0), __dsub_rn(p00, ps(a, hzm))));
+        const double h0 = a.ih[h];
+        const double X = __dsub_rn(__dmul_rn(rho_w(rmin, a.ih[hxp], h0), __dsub_rn(ps(a, hxp), p00)),
+                                   __dmul_rn(rho_w(rmin, a.ih[hxm], h0), __dsub_rn(p00, ps(a, hxm))));
+        const double Z = __dsub_rn(__dmul_rn(rho_w(rmin, a.ih[hzp], h0), __dsub_rn(ps(a, hzp), p00)),
+                                   __dmul_rn(rho_w(rmin, a.ih[hzm], h0), __dsub_rn(p00, ps(a, hzm))));
         const double Y =
-            __dsub_rn(__dmul_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hyp]), h0), __dsub_rn(ps(a, hyp), p00)), padp),
-                      __dmul_rn(__dmul_rn(rho_w(rmin, half_inv(a.rho[hym]), h0), __dsub_rn(p00, ps(a, hym))), padm));
+            __dsub_rn(__dmul_rn(__dmul_rn(rho_w(rmin, a.ih[hyp], h0), __dsub_rn(ps(a, hyp), p00)), padp),
+                      __dmul_rn(__dmul_rn(rho_w(rmin, a.ih[hym], h0), __dsub_rn(p00, ps(a, hym))), padm));
         const double L = __dadd_rn(__dadd_rn(__dmul_rn(X, a.inv_dx2), __dmul_rn(Z, a.inv_dz2)), __dmul_rn(Y, idy));
         const double t1 = __dmul_rn(__dmul_rn(a.inv_dt, dv), rmin);
         const double t2 = __dmul_rn(__dmul_rn(a.inv_dt, rmin), a.div_now[h]);
@@ -154,15 +161,15 @@ __global__ void __launch_bounds__(128) k_vd_correct(const VdArgs a) {
         const int im = iw == 0 ? nx - 1 : iw - 1;
         const size_t h = hix(nx, nz, iw, jw, k);
         const double p0 = Pc[iw];
-        const double r0 = __ddiv_rn(0.5, a.rho[h]);
+        const double r0 = a.ih[h];
         // x face (MCS:1158-1164): neighbours at iw - 1 in the caller's halo'd arrays
         size_t hm = hix(nx, nz, iw - 1, jw, k);
-        double irn = __dadd_rn(r0, __ddiv_rn(0.5, a.rho[hm]));
+        double irn = __dadd_rn(r0, a.ih[hm]);
         double pf = pmix(a, p0, h, irn, irm), pb = pmix(a, Pc[im], hm, irn, irm);
         const double u = __dsub_rn(a.Uh[h], __dmul_rn(__dmul_rn(a.dt, __dsub_rn(pf, pb)), a.inv_dx));
         // z face (:1168-1175)
         hm = hix(nx, nz, iw, jw - 1, k);
-        irn = __dadd_rn(r0, __ddiv_rn(0.5, a.rho[hm]));
+        irn = __dadd_rn(r0, a.ih[hm]);
         pf = pmix(a, p0, h, irn, irm);
         pb = pmix(a, Pjm[iw], hm, irn, irm);
         const double w = __dsub_rn(a.Wh[h], __dmul_rn(__dmul_rn(a.dt, __dsub_rn(pf, pb)), a.inv_dz));
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(128) k_vd_correct(const VdArgs a) {
         double v = a.wall[1];
         if (k > 0) {
             hm = hix(nx, nz, iw, jw, k - 1);
-            irn = __dadd_rn(r0, __ddiv_rn(0.5, a.rho[hm]));
+            irn = __dadd_rn(r0, a.ih[hm]);
             pf = pmix(a, p0, h, irn, irm);
             pb = pmix(a, Pkm[iw], hm, irn, irm);
             v = __dsub_rn(a.Vh[h], __dmul_rn(a.dt, __dadd_rn(__dmul_rn(hi, pf), __dmul_rn(lo, pb))));
@@ -194,11 +201,19 @@ cudaError_t launch_vd_rho_min(const prj_plan* pl, const double* rho, unsigned lo
     return cudaGetLastError();
 }
 
+cudaError_t launch_vd_half_inv(const prj_plan* pl, const double* rho, double* ih, cudaStream_t st) {
+    const Geometry& g = pl->g;
+    const size_t n = (size_t)(g.nx + 2) * (g.nz + 2) * (g.ny + 2);
+    const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+    k_half_inv<<<blocks, 256, 0, st>>>(n, rho, ih);
+    return cudaGetLastError();
+}
+
 static VdArgs vd_args(const prj_plan* pl, const VdFields& f, const StepScalars& sc, const unsigned long long* slot) {
     const Geometry& g = pl->g;
     VdArgs a{};
     a.nx = g.nx; a.nz = g.nz; a.ny = g.ny;
-    a.rho = f.rho; a.Pn = f.P_now; a.Po = f.P_old; a.div_now = f.div_now;
+    a.rho = f.rho; a.ih = pl->vd_ih; a.Pn = f.P_now; a.Po = f.P_old; a.div_now = f.div_now;
     a.inv_dy_p = pl->t.inv_dy_p; a.pad = pl->vd_pad; a.rho_min = slot;
     a.lo = pl->t.dpdy_lo; a.hi = pl->t.dpdy_hi;
     a.dt = sc.dt; a.inv_dt = sc.inv_dt;
