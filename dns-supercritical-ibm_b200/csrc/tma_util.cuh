@@ -46,11 +46,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
-// Wait for completion of the phase with parity `phase`; false after the budget.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+// Wait for completion of the phase with parity `phase`; false after `budget` cycles.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase,
+                                                  long long budget = kWaitBudgetCycles) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, phase)) {
-        if (clock64() - t0 > kWaitBudgetCycles) return false;
+        if (clock64() - t0 > budget) return false;
     }
     return true;
 }

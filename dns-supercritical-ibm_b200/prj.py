@@ -55,7 +55,7 @@ EXPORTS = (
     "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
     "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
     "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
-    "prj_projection_step_host_async", "prj_host_async_wait",
+    "prj_projection_step_host_async", "prj_host_async_wait", "prj_selftest_wait_timeout",
 )
 
 BANDS_REFERENCE = 0
@@ -149,6 +149,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_schedule.argtypes = [_vp, i, ctypes.POINTER(i), ctypes.POINTER(i)]
     L.prj_projection_step_host_async.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.POINTER(StepParams), i]
     L.prj_host_async_wait.argtypes = [_vp]
+    L.prj_selftest_wait_timeout.argtypes = [i, ctypes.c_longlong]
     L.prj_rough_force.argtypes = [i, i, i, _vp, _vp, _vp, ctypes.POINTER(RoughInds), ctypes.POINTER(StepParams), _vp]
     ll = ctypes.c_longlong
     L.prj_ibm_interp.argtypes = [_vp, ll, i, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp, _vp, _vp, _vp]

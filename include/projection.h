@@ -265,6 +265,13 @@ typedef struct prj_tuning {
 int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out);
 int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
 
+/* Diagnostic of the bounded device-side waits of the pipelined kernels: one
+ * kernel waits, for at most budget_cycles SM clock cycles, on an mbarrier that
+ * nothing arrives on, gives up, and reports it.  Returns PRJ_ERR_TIMEOUT when the
+ * wait gave up as designed (the context stays usable), PRJ_OK if it unexpectedly
+ * completed.  No fault, trap or unbounded wait is involved. */
+int prj_selftest_wait_timeout(int device, long long budget_cycles);
+
 /* Kernel launches one prj_projection_step of `mode` issues with the plan's current
  * configuration (statistics excluded), and the number of y chunks of the overlapped
  * FP64 schedule (0 when the kernels run one after another).  The overlapped
