@@ -44,9 +44,11 @@ def key(plan) -> str:
 
 def candidates(plan):
     out = []
-    for z_mode in (0, 1):
+    for z_mode in (0, 1, 3):
         for x_rows in (2, 4, 8, 16):
             for z_rows in ((0, 4, 8, 16) if z_mode == 0 else (0,)):
+                if z_mode == 3 and x_rows not in (4, 8):
+                    continue
                 out.append(dict(x_rows=x_rows, z_rows=z_rows, z_mode=z_mode))
     return out
 

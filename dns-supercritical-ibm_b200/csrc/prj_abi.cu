@@ -158,12 +158,18 @@ int make_slot_table(int n, int** d_out, size_t* bytes) {
     return PRJ_OK;
 }
 
-// z-direction kernel choice: PRJ_ZSOLVE=split|fused|basic (split needs the in-place plan)
-int z_mode(bool split_ok) {
+// z-direction kernel choice: PRJ_ZSOLVE=split|fused|basic|line (split and line need the
+// in-place plan).  By default the per-wavenumber kernel when there are at least two x
+// wavenumbers (its CTAs) per SM, else the split kernels: measured on B200, the
+// per-wavenumber kernel took 1.35 / 1.50 / 7.87 ms against 1.40 / 1.60 / 8.67 ms for
+// nx/2+1 = 385 / 513 / 769, but 0.39 / 0.57 ms against 0.26 / 0.44 ms for 193 / 257.
+int z_mode(bool split_ok, bool line_pref) {
     const char* v = getenv("PRJ_ZSOLVE");
     if (v && !strcmp(v, "fused")) return 1;
     if (v && !strcmp(v, "basic")) return 2;
-    return split_ok ? 0 : 1;
+    if (v && !strcmp(v, "line")) return split_ok ? 3 : 1;
+    if (v && !strcmp(v, "split")) return split_ok ? 0 : 1;
+    return split_ok ? (line_pref ? 3 : 0) : 1;
 }
 
 void free_plan_buffers(prj_plan* pl) {
@@ -407,7 +413,7 @@ int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const doub
 }
 
 int mixed_supported(const prj_plan* pl) {
-    if (pl->zmode != 0 || !pl->xd.ok)
+    if ((pl->zmode != 0 && pl->zmode != 3) || !pl->xd.ok)
         return fail(PRJ_ERR_UNSUPPORTED, "the mixed-precision path needs in-place plans for nx/2 and nz (radices 2, 3, 4, 5, 8)");
     return PRJ_OK;
 }
@@ -430,7 +436,15 @@ int run_mixed_poisson(prj_plan* pl, double* P, cudaStream_t st) {
 
 // z transforms + Thomas: three kernels (split) or one fused kernel
 int run_zsolve(prj_plan* pl, cudaStream_t st) {
-    if (pl->zmode == 0) {
+    if (pl->zmode == 3) {
+        StageTimer tm(pl, prj::kStZSolve, st);
+        const cudaError_t e = prj::launch_zline(pl, st);
+        if (e != cudaErrorNotSupported) {
+            CK(e, "z transform + Thomas (per-wavenumber kernel)");
+            return PRJ_OK;
+        }
+    }
+    if (pl->zmode == 0 || pl->zmode == 3) {
         {
             StageTimer tm(pl, prj::kStZfftFwd, st);
             CK(prj::launch_zfft(pl, -1, st), "z transform");
@@ -633,7 +647,11 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if ((rc = make_dif(pl->fx64.m, &pl->xd, &bytes))) return bail(rc);
     if ((rc = make_dif(nz, &pl->zd, &bytes))) return bail(rc);
     if (pl->zd.ok && (rc = make_slot_table(nz, &pl->kz_of_slot, &bytes))) return bail(rc);
-    pl->zmode = z_mode(pl->zd.ok && pl->kz_of_slot);
+    {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pl->device) != cudaSuccess) sms = 0;
+        pl->zmode = z_mode(pl->zd.ok && pl->kz_of_slot, sms > 0 && g.nxh >= 2 * sms);
+    }
     {
         // PRJ_FFT_KERNELS=runtime keeps the runtime-radix kernels for lengths with a pass plan
         const char* v = getenv("PRJ_FFT_KERNELS");
@@ -817,7 +835,7 @@ bool x_pass_active(const prj_plan* pl);
 bool overlap_ok(const prj_plan* pl) {
     int fac[8];
     const int C = pl->overlap_chunks;
-    return C >= 2 && !pl->timing && pl->zmode == 0 && x_pass_active(pl) && pl->zd.ok && pl->kz_of_slot &&
+    return C >= 2 && !pl->timing && (pl->zmode == 0 || pl->zmode == 3) && x_pass_active(pl) && pl->zd.ok && pl->kz_of_slot &&
            prj::pass_radices(pl->g.nz, fac, 8) > 0 && pl->g.ny >= 2 * C;
 }
 
@@ -1186,7 +1204,8 @@ int prj_plan_schedule(const prj_plan* plan, int mode, int* launches, int* chunks
     const bool ov = mode == PRJ_MODE_FP64 && overlap_ok(plan);
     *chunks = ov ? plan->overlap_chunks : 0;
     if (ov) *launches = 5 * plan->overlap_chunks + 1;
-    else if (mode == PRJ_MODE_FP64) *launches = plan->zmode == 0 ? 6 : 4;
+    else if (mode == PRJ_MODE_FP64)
+        *launches = (plan->zmode == 0 || (plan->zmode == 3 && !prj::zline_supported(plan))) ? 6 : 4;
     else {
         // forward x, z transforms of the FP64 and FP32 rows, one Thomas launch, inverse z of both,
         // inverse x; per refinement pass also the plane means, the residual and a norm reset;
@@ -1212,8 +1231,10 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
     auto pow2 = [](int v) { return v >= 1 && v <= 16 && (v & (v - 1)) == 0; };
     if (!pow2(t->x_rows)) return fail(PRJ_ERR_ARG, "x_rows=%d must be a power of two in [1, 16]", t->x_rows);
     if (t->z_rows != 0 && !pow2(t->z_rows)) return fail(PRJ_ERR_ARG, "z_rows=%d must be 0 or a power of two in [1, 16]", t->z_rows);
-    if (t->z_mode != 0 && t->z_mode != 1) return fail(PRJ_ERR_ARG, "z_mode=%d must be 0 or 1", t->z_mode);
-    if (t->z_mode == 0 && !(plan->zd.ok && plan->kz_of_slot)) return fail(PRJ_ERR_UNSUPPORTED, "no in-place z plan for nz=%d", plan->g.nz);
+    if (t->z_mode != 0 && t->z_mode != 1 && t->z_mode != 3)
+        return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1 or 3", t->z_mode);
+    if ((t->z_mode == 0 || t->z_mode == 3) && !(plan->zd.ok && plan->kz_of_slot))
+        return fail(PRJ_ERR_UNSUPPORTED, "no in-place z plan for nz=%d", plan->g.nz);
     const int rs = plan->fx64.even ? plan->fx64.m + 1 : plan->fx64.m;
     if ((size_t)prj::padded_len(t->x_rows * rs, true) * sizeof(double2) + (size_t)plan->fx64.m * sizeof(int) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "x_rows=%d does not fit shared memory for nx=%d", t->x_rows, plan->g.nx);

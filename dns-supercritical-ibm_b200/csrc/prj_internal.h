@@ -118,7 +118,8 @@ struct prj_plan {
     double* mix_b = nullptr;      // Poisson-only mixed solve: copy of the right-hand side
     double* mix_r = nullptr;      // Poisson-only mixed solve: residual
     int zfft_rows = 0;            // rows per CTA of the z-transform kernels (0: default rule)
-    int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined
+    int zmode = 0;                // z direction: 0 split kernels, 1 fused pipelined, 2 unpipelined,
+                                  // 3 one pass-plan kernel per x wavenumber (split where no plan)
     bool use_pass = true;         // compile-time pass-plan FFT kernels where the length has one
     int thomas_async = -1;        // Thomas lines streamed through a cp.async shared-memory ring:
                                   // -1 for the mixed storage only, 0 never, 1..4 always (ring shape)
@@ -166,6 +167,10 @@ cudaError_t launch_stats(const prj_plan* pl, const double* U, const double* V, c
 // when the grid does not fit its shared-memory budget.  *err_word is raised if a
 // bounded wait gives up.
 cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStream_t st);
+// z transform + Thomas + inverse z as one kernel per x wavenumber on the pass-plan
+// butterflies (prj_zline.cu); cudaErrorNotSupported when nz has no pass plan
+cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st);
+bool zline_supported(const prj_plan* pl);  // launch_zline would run (not fall back)
 
 // x transforms with the in-place DIF FFT (prj_xfft.cu); used when pl->xd.ok
 // bout: also store the source field (divergence) there; accum: P += result; sq: norms of

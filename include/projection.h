@@ -254,7 +254,9 @@ int prj_batch_destroy(prj_batch* batch);
  *   x_rows  x-rows per CTA of the x-transform kernels (power of two, 1..16);
  *   z_rows  spectral rows per CTA of the z-transform kernels (power of two, 1..16);
  *   z_mode  0 = z FFT / Thomas / inverse z FFT as three kernels, 1 = one fused
- *           pipelined kernel per x-wavenumber.
+ *           pipelined kernel per x-wavenumber (runtime radices), 3 = one kernel per
+ *           x-wavenumber on the compile-time pass plans (three kernels where nz has
+ *           no pass plan).  The default is 3 when nx/2+1 >= 2 x the SM count, else 0.
  * prj_plan_set_tuning rejects shapes that do not fit shared memory.
  */
 typedef struct prj_tuning {
