@@ -180,6 +180,7 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->t.ax);
     dfree(pl->t.az);
     dfree(pl->t.piv);
+    dfree(pl->t.pivc);
     dfree(pl->fx64.tw);
     dfree(pl->fx64.post);
     dfree(pl->fz64.tw);
@@ -723,6 +724,9 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     bytes += spec_elems * sizeof(double2);
     if ((e = cudaMalloc((void**)&pl->t.piv, piv_elems * sizeof(double))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(pivots)"));
+    bytes += piv_elems * sizeof(double);
+    if ((e = cudaMalloc((void**)&pl->t.pivc, piv_elems * sizeof(double))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(back-substitution factors)"));
     bytes += piv_elems * sizeof(double);
     if ((e = cudaMalloc((void**)&pl->stat_buf, 8 * sizeof(double))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(stats)"));

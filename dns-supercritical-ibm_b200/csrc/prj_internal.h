@@ -62,6 +62,7 @@ struct DeviceTables {
     double* ax = nullptr;        // nxh: -4/dx^2 sin^2(kx pi / nx)
     double* az = nullptr;        // nzh: -4/dz^2 sin^2(kzs pi / nz)
     double* piv = nullptr;       // D[y][kx][kzs]: Thomas pivots b + lambda - a c'
+    double* pivc = nullptr;      // c'[y][kx][kzs] = c_y / D_y (the reference's poi_C, PSM:164-179), folded like D
 };
 
 }  // namespace prj

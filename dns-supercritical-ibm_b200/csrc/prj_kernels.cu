@@ -273,14 +273,19 @@ __global__ void __launch_bounds__(512) k_zsolve(const ZArgs a) {
 // Thomas pivots of every (kx, kzs) line, poisson_solver_multigpu.f90:164-179:
 // D_0 = b_0 + lambda, D_k = (b_k + lambda) - a_k c'_{k-1}, c'_k = c_k / D_k.
 // Also reduces min |D| (min_abs_div_bacp, :181-197) into *minpiv (as bits).
+// pivc (may be null): the back-substitution factors c'_y = c_y / D_y of every line, the
+// quotients the backward sweep would otherwise form
 __global__ void k_build_pivots(int nh, int nzh, int mzp, int ny, const double* __restrict__ bands,
                                const double* __restrict__ ax, const double* __restrict__ az, double* piv,
-                               unsigned long long* minpiv) {
+                               double* pivc, unsigned long long* minpiv) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int kx = gid / mzp, t = gid - kx * mzp;
     if (kx >= nh) return;
     if (t >= nzh) {  // padding slots
-        for (int y = 0; y < ny; y++) piv[((size_t)y * nh + kx) * mzp + t] = 1.0;
+        for (int y = 0; y < ny; y++) {
+            piv[((size_t)y * nh + kx) * mzp + t] = 1.0;
+            if (pivc) pivc[((size_t)y * nh + kx) * mzp + t] = 0.0;
+        }
         return;
     }
     const bool is00 = (kx == 0 && t == 0);
@@ -292,11 +297,13 @@ __global__ void k_build_pivots(int nh, int nzh, int mzp, int ny, const double* _
     double cp = __ddiv_rn(C[0], D);
     double mn = fabs(D);
     piv[((size_t)0 * nh + kx) * mzp + t] = D;
+    if (pivc) pivc[((size_t)0 * nh + kx) * mzp + t] = cp;
     for (int y = 1; y < ny; y++) {
         D = __dsub_rn(__dadd_rn(Bb[y], lam), __dmul_rn(A[y], cp));
         cp = __ddiv_rn(C[y], D);
         mn = fmin(mn, fabs(D));
         piv[((size_t)y * nh + kx) * mzp + t] = D;
+        if (pivc) pivc[((size_t)y * nh + kx) * mzp + t] = cp;
     }
     if (mn == mn) atomicMin(minpiv, (unsigned long long)__double_as_longlong(mn));
     else atomicMin(minpiv, 0ull);  // NaN pivot: report 0
@@ -479,7 +486,7 @@ cudaError_t launch_build_pivots(const prj_plan* pl, cudaStream_t st) {
     cudaError_t e = cudaMemcpyAsync(mp, &big, sizeof(double), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
     k_build_pivots<<<(tot + 127) / 128, 128, 0, st>>>(g.nxh, g.nzh, g.mzp, g.ny, pl->t.bands, pl->t.ax, pl->t.az,
-                                                      pl->t.piv, mp);
+                                                      pl->t.piv, pl->t.pivc, mp);
     return cudaGetLastError();
 }
 

@@ -12,8 +12,9 @@
 //     d'_y = (d_y - a_y d'_{y-1}) / D_y for the chunk's planes, stored to the row
 //     (slot order);
 //   backward phase, y descending:
-//     d' rows and pivot rows streamed back the same way;
-//     x_y = d'_y - (c_y / D_y) x_{y+1} in the stage;
+//     d' rows and the rows of c'_y = c_y / D_y (tabulated with the pivots) streamed
+//     back the same way;
+//     x_y = d'_y - c'_y x_{y+1} in the stage;
 //     inverse z FFT in place, the last pass storing natural-order rows.
 //
 // The spectrum crosses HBM four times (rows in, d' out, d' in, rows out) against
@@ -37,6 +38,7 @@ struct ZLineArgs {
     const double2* tw;    // z pass-plan twiddles
     const double* bands;  // a, b, c, a00, b00, c00
     const double* piv;    // D[y][kx][kzs]
+    const double* pivc;   // c'[y][kx][kzs] = c_y / D_y
     const int* kz_of_slot;
     double2* X;           // [y][kx][z]
 };
@@ -76,12 +78,12 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
         is00[q] = (kx == 0 && kz == 0);
     }
     const double* bA = a.bands;
-    const double* bC = a.bands + 2 * ny;
     const double* bA0 = a.bands + 3 * ny;
-    const double* bC0 = a.bands + 5 * ny;
 
-    // chunk c (planes c yb ..) into stage s; every thread copies a share; one group per call
-    auto issue = [&](int c, int s) {
+    // chunk c (planes c yb ..) into stage s with the rows of table tab (pivots on the way
+    // up, back-substitution factors on the way down); every thread copies a share; one
+    // group per call
+    auto issue = [&](int c, int s, const double* tab) {
         if (c >= 0 && c < nch) {
             const int y0 = c * yb, nr = min(yb, ny - y0);
             double2* buf = ring + sidx<true>(s * yb * n);
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
             double* dbuf = dring + (size_t)s * yb * mzp;
             for (int i = tid; i < nr * hp; i += NT) {
                 const int r = i / hp, j = i - r * hp;
-                zl_cp16(dbuf + (size_t)r * mzp + 2 * j, a.piv + ((size_t)(y0 + r) * nh + kx) * mzp + 2 * j);
+                zl_cp16(dbuf + (size_t)r * mzp + 2 * j, tab + ((size_t)(y0 + r) * nh + kx) * mzp + 2 * j);
             }
         }
         zl_commit();
@@ -105,9 +107,9 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
 
     // ------------------------------------------------------------ forward phase
 #pragma unroll
-    for (int c = 0; c < NS - 1; c++) issue(c, c);
+    for (int c = 0; c < NS - 1; c++) issue(c, c, a.piv);
     for (int c = 0; c < nch; c++) {
-        issue(c + NS - 1, (c + NS - 1) % NS);  // that stage was last read in iteration c - 1
+        issue(c + NS - 1, (c + NS - 1) % NS, a.piv);  // that stage was last read in iteration c - 1
         zl_wait<NS - 1>();
         __syncthreads();
         const int s = c % NS, y0 = c * yb, nr = min(yb, ny - y0);
@@ -145,9 +147,9 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
     // ----------------------------------------------------------- backward phase
     // j-th chunk from the top (chunk nch-1-j) uses stage j % NS
 #pragma unroll
-    for (int j = 0; j < NS - 1; j++) issue(nch - 1 - j, j);
+    for (int j = 0; j < NS - 1; j++) issue(nch - 1 - j, j, a.pivc);
     for (int j = 0; j < nch; j++) {
-        issue(nch - 1 - (j + NS - 1), (j + NS - 1) % NS);
+        issue(nch - 1 - (j + NS - 1), (j + NS - 1) % NS, a.pivc);
         zl_wait<NS - 1>();
         __syncthreads();
         const int s = j % NS, c = nch - 1 - j, y0 = c * yb, nr = min(yb, ny - y0);
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
                     if (y == ny - 1) {
                         prev[q] = d;
                     } else {
-                        const double C = __ddiv_rn(is00[q] ? bC0[y] : bC[y], dbuf[(size_t)r * mzp + kzs[q]]);
+                        const double C = dbuf[(size_t)r * mzp + kzs[q]];  // c_y / D_y
                         prev[q].x = __dsub_rn(d.x, __dmul_rn(prev[q].x, C));
                         prev[q].y = __dsub_rn(d.y, __dmul_rn(prev[q].y, C));
                     }
@@ -214,7 +216,7 @@ int zl_env(const char* name, int dflt) {
 }  // namespace
 
 bool zline_supported(const prj_plan* pl) {
-    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot) return false;
+    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc) return false;
     switch (pl->g.nz) {
 #define PRJ_ZL_HAS(N, ...) \
     case N: return same_radices<PassList<__VA_ARGS__>>(pl->zd.f) && zline_smem(N, pl->g.mzp, 1, 2) <= (size_t)200 * 1024;
@@ -227,11 +229,12 @@ bool zline_supported(const prj_plan* pl) {
 
 // cudaErrorNotSupported when nz has no pass plan (the caller runs the split kernels)
 cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st) {
-    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot) return cudaErrorNotSupported;
+    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc) return cudaErrorNotSupported;
     const Geometry& g = pl->g;
     ZLineArgs a{};
     a.ny = g.ny; a.nh = g.nxh; a.mzp = g.mzp;
-    a.tw = pl->zd.tw; a.bands = pl->t.bands; a.piv = pl->t.piv; a.kz_of_slot = pl->kz_of_slot; a.X = pl->spec;
+    a.tw = pl->zd.tw; a.bands = pl->t.bands; a.piv = pl->t.piv; a.pivc = pl->t.pivc;
+    a.kz_of_slot = pl->kz_of_slot; a.X = pl->spec;
     // planes per stage and stage count: PRJ_ZLINE_YB / PRJ_ZLINE_NS, else 4 x 2; the
     // planes per stage shrink until the ring fits PRJ_ZLINE_SMEM_KB (default 72 KB: three
     // CTAs per SM)

@@ -5,8 +5,9 @@
 //                (wavenumber kz at slot pos[kz]);
 //   k_thomas   : one thread per (kx, slot) line, streaming over y: forward
 //                sweep d'_y = (d_y - a_y d'_{y-1}) / D_y, backward sweep
-//                x_y = d'_y - (c_y / D_y) x_{y+1}, in place, rows prefetched
-//                into registers kBlock planes at a time;
+//                x_y = d'_y - c'_y x_{y+1} with c'_y = c_y / D_y tabulated with the
+//                pivots, in place, rows prefetched into registers kBlock planes at
+//                a time;
 //   k_zfft_inv : slot-order rows -> in-place DIT inverse FFT -> natural z.
 //
 // Compared with one fused per-kx kernel this moves the spectrum through HBM
@@ -102,6 +103,7 @@ struct ThomasArgs {
     int nhb, kx0;                // rows per plane in this buffer; its first kx
     const double* bands;         // a, b, c, a00, b00, c00
     const double* piv;           // D[y][kx][kzs], kx over all nh rows
+    const double* pivc;          // c'[y][kx][kzs] = c_y / D_y, same layout
     const int* kz_of_slot;       // wavenumber held by each slot
     void* X;                     // T rows [y][kx - kx0][slot]
 };
@@ -121,11 +123,11 @@ __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
     const int kzs = kz <= nz - kz ? kz : nz - kz;
     const bool is00 = (kx == 0 && kz == 0);
     const double* A = a.bands + (is00 ? 3 : 0) * ny;
-    const double* C = a.bands + (is00 ? 5 : 2) * ny;
     const size_t rstride = (size_t)a.nhb * nz;  // X: next y plane
     const size_t pstride = (size_t)nh * mzp;     // D: next y plane
     T* x = static_cast<T*>(a.X) + (size_t)kb * nz + slot;
     const double* d = a.piv + (size_t)kx * mzp + kzs;
+    const double* dc = a.pivc + (size_t)kx * mzp + kzs;
 
     // forward sweep, y ascending
     double2 prev = make_double2(0.0, 0.0);
@@ -162,21 +164,20 @@ __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
     from_d2(x[(size_t)(ny - 1) * rstride], prev);
     for (int y1 = ny - 2; y1 >= 0; y1 -= kBlock) {
         double2 v[kBlock];
-        double D[kBlock], cv[kBlock];
+        double cp[kBlock];
 #pragma unroll
         for (int u = 0; u < kBlock; u++) {
             const int y = y1 - u;
             if (y >= 0) {
                 v[u] = to_d2(x[(size_t)y * rstride]);
-                D[u] = d[(size_t)y * pstride];
-                cv[u] = C[y];
+                cp[u] = dc[(size_t)y * pstride];  // c_y / D_y, tabulated with the pivots
             }
         }
 #pragma unroll
         for (int u = 0; u < kBlock; u++) {
             const int y = y1 - u;
             if (y >= 0) {
-                const double c = __ddiv_rn(cv[u], D[u]);
+                const double c = cp[u];
                 double2 r;
                 r.x = __dsub_rn(v[u].x, __dmul_rn(prev.x, c));
                 r.y = __dsub_rn(v[u].y, __dmul_rn(prev.y, c));
@@ -215,11 +216,11 @@ __device__ __forceinline__ void thomas_line_async(const ThomasArgs& a, int blk, 
     const int kzs = kz <= nz - kz ? kz : nz - kz;
     const bool is00 = (kx == 0 && kz == 0);
     const double* A = a.bands + (is00 ? 3 : 0) * ny;
-    const double* C = a.bands + (is00 ? 5 : 2) * ny;
     const size_t rstride = (size_t)a.nhb * nz;
     const size_t pstride = (size_t)nh * mzp;
     T* x = static_cast<T*>(a.X) + (size_t)kb * nz + slot;
     const double* d = a.piv + (size_t)kx * mzp + kzs;
+    const double* dc = a.pivc + (size_t)kx * mzp + kzs;
     T* Xs = reinterpret_cast<T*>(sm);                                        // [NS][B][tile]
     double* Ds = reinterpret_cast<double*>(sm + (size_t)NS * B * kThomasTile * sizeof(T));  // [NS][B][tile]
     auto xs = [&](int st, int u) -> T& { return Xs[((size_t)st * B + u) * kThomasTile + tid]; };
@@ -279,7 +280,7 @@ __device__ __forceinline__ void thomas_line_async(const ThomasArgs& a, int blk, 
                 const int y = ny - 2 - b * B - u;
                 if (y >= 0) {
                     cp_async(&xs(st, u), x + (size_t)y * rstride, (int)sizeof(T));
-                    cp_async(&ds(st, u), d + (size_t)y * pstride, 8);
+                    cp_async(&ds(st, u), dc + (size_t)y * pstride, 8);
                 }
             }
         }
@@ -295,7 +296,7 @@ __device__ __forceinline__ void thomas_line_async(const ThomasArgs& a, int blk, 
         for (int u = 0; u < B; u++) {
             const int y = ny - 2 - b * B - u;
             if (y >= 0) {
-                const double c = __ddiv_rn(C[y], ds(st, u));
+                const double c = ds(st, u);  // c_y / D_y, tabulated with the pivots
                 const double2 v = to_d2(xs(st, u));
                 double2 r;
                 r.x = __dsub_rn(v.x, __dmul_rn(prev.x, c));
@@ -456,13 +457,14 @@ ThomasArgs thomas_args(const prj_plan* pl, void* X, int kx0, int rows_per_plane)
     t.nz = g.nz; t.ny = g.ny; t.nh = g.nxh; t.mzp = g.mzp;
     t.tiles = (g.nz + kThomasTile - 1) / kThomasTile;
     t.nhb = rows_per_plane; t.kx0 = kx0;
-    t.bands = pl->t.bands; t.piv = pl->t.piv; t.kz_of_slot = pl->kz_of_slot; t.X = X;
+    t.bands = pl->t.bands; t.piv = pl->t.piv; t.pivc = pl->t.pivc; t.kz_of_slot = pl->kz_of_slot; t.X = X;
     return t;
 }
 
 template <typename T>
 cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_plane, cudaStream_t st) {
     if (rows_per_plane <= 0) return cudaSuccess;
+    if (!pl->t.piv || !pl->t.pivc) return cudaErrorInvalidValue;
     const ThomasArgs t = thomas_args(pl, X, kx0, rows_per_plane);
     const unsigned grid = (unsigned)(rows_per_plane * t.tiles);
     switch (pl->thomas_async > 0 ? pl->thomas_async : 0) {
@@ -496,6 +498,7 @@ cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st) {
 }
 
 cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st) {
+    if (!pl->t.piv || !pl->t.pivc) return cudaErrorInvalidValue;
     const int rows32 = pl->g.nxh - pl->kxs;
     if (rows32 <= 0) return launch_thomas_t<double2>(pl, pl->spec, 0, pl->kxs, st);
     const ThomasArgs a64 = thomas_args(pl, pl->spec, 0, pl->kxs);
