@@ -221,21 +221,31 @@ inline bool same_radices(const DifDev& f) {
 
 // Lengths with a compile-time pass plan: X(n, radices...).  The host plans these
 // lengths with the same radices (fft_host.h), so twiddle tables and slot orders
-// agree with the runtime-radix kernels.
+// agree with the runtime-radix kernels.  The radix order is the one whose passes
+// address the padded shared-memory rows (slot g + g/8) without bank conflicts, or
+// with the fewest (counted for 16-byte accesses, eight lanes per wavefront): a
+// pass of span L and radix R strides its butterflies by L/R elements, and with the
+// odd radices early every later stride is a multiple of 8 or spread by the padding.
 #define PRJ_PASS_PLANS(X)       \
     X(16, 4, 4)                 \
     X(24, 6, 4)                 \
     X(32, 8, 4)                 \
-    X(48, 8, 6)                 \
+    X(48, 6, 8)                 \
     X(64, 8, 8)                 \
-    X(96, 8, 6, 2)              \
-    X(128, 8, 4, 4)             \
-    X(192, 8, 8, 3)             \
-    X(256, 8, 8, 4)             \
-    X(384, 8, 8, 6)             \
+    X(96, 2, 6, 8)              \
+    X(128, 4, 4, 8)             \
+    X(192, 3, 8, 8)             \
+    X(256, 8, 4, 8)             \
+    X(384, 6, 8, 8)             \
     X(512, 8, 8, 8)             \
-    X(768, 8, 8, 6, 2)          \
-    X(1024, 8, 8, 4, 4)         \
-    X(1536, 8, 8, 6, 4)
+    X(768, 8, 6, 2, 8)          \
+    X(1024, 4, 8, 4, 8)         \
+    X(1536, 4, 8, 6, 8)
+
+// Row stride (in elements) of the x kernels' shared-memory rows of m complex values:
+// a multiple of 8, so every row starts on a padding boundary and the passes of
+// consecutive rows see the same bank pattern; the +8 offsets consecutive rows by
+// one bank group for the row-fastest split and load phases.
+__host__ __device__ constexpr int pass_row_stride(int m) { return m + 8; }
 
 }  // namespace prj

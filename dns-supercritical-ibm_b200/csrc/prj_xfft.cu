@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
 
 // ---------------------------------------------------------------------------
 // Pass-plan x kernels (fft_pass.cuh), m = nx/2 with a compile-time plan PL.
-// Row stride m + 1 (odd) keeps the row-fastest split and load phases free of
-// bank conflicts.  nr = rows present in this CTA (the last CTA may hold fewer).
+// Rows at stride pass_row_stride(m) in shared memory.  nr = rows present in this
+// CTA (the last CTA may hold fewer).
 
 // k_fwd_xp: source (P, or the divergence of u_hat) -> packed complex -> DIF
 // passes -> split X_k, X_{m-k} -> transposed store.  SRC 0 reads P in the first
@@ -271,7 +271,7 @@ template <int SRC, class PL>
 __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_fwd_xp(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
-    constexpr int m = PL::n, nx = 2 * m, rs = m + 1;
+    constexpr int m = PL::n, nx = 2 * m, rs = pass_row_stride(m);
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
     const int nr = min(a.tz, a.nz - z0);
@@ -404,7 +404,7 @@ template <class PL, int TZ, int NT>
 __global__ void __launch_bounds__(NT) k_fwd_xs(const XsArgs xs) {
     const XArgs& a = xs.a;
     extern __shared__ __align__(16) unsigned char sm[];
-    constexpr int m = PL::n, nx = 2 * m, rs = m + 1, hrow = nx + 2;
+    constexpr int m = PL::n, nx = 2 * m, rs = pass_row_stride(m), hrow = nx + 2;
     constexpr int NROW = 4 * TZ + 1;  // U: TZ, W: TZ + 1, V(y): TZ, V(y+1): TZ
     double* stage = reinterpret_cast<double*>(sm);
     double2* A = reinterpret_cast<double2*>(sm + (size_t)NROW * hrow * sizeof(double));
@@ -516,7 +516,7 @@ template <class PL>
 __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_bwd_xp(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     double2* A = reinterpret_cast<double2*>(sm);
-    constexpr int m = PL::n, rs = m + 1, half = m / 2;
+    constexpr int m = PL::n, rs = pass_row_stride(m), half = m / 2;
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
     const int nr = min(a.tz, a.nz - z0);
@@ -630,14 +630,14 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 int bwd_tiles_per_plane(const prj_plan* pl) { return (pl->g.nz + pl->tz_xp - 1) / pl->tz_xp; }
 
 // rows per CTA of the pass-plan x kernels: a power of two up to 16 whose padded rows
-// (stride m + 1) fit 28 KB, so that 7-8 CTAs share an SM
+// (stride pass_row_stride(m)) fit 32 KB, so that 6 CTAs share an SM
 int choose_tz_xp(int m) {
     int tz = 16;
-    while (tz > 1 && (size_t)padded_len(tz * (m + 1), true) * sizeof(double2) > 28 * 1024) tz /= 2;
+    while (tz > 1 && (size_t)padded_len(tz * pass_row_stride(m), true) * sizeof(double2) > 32 * 1024) tz /= 2;
     return tz;
 }
 
-size_t pass_x_smem(int m, int tz) { return (size_t)padded_len(tz * (m + 1), true) * sizeof(double2); }
+size_t pass_x_smem(int m, int tz) { return (size_t)padded_len(tz * pass_row_stride(m), true) * sizeof(double2); }
 
 // rows per CTA of the in-place x kernels: a power of two up to 16 within ~56 KB
 int choose_tz_xd(int m, bool even) {
@@ -651,7 +651,9 @@ namespace {
 
 inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-size_t pass_smem_bytes(const XArgs& a) { return (size_t)padded_len(a.tz * (a.m + 1), true) * sizeof(double2); }
+size_t pass_smem_bytes(const XArgs& a) {
+    return (size_t)padded_len(a.tz * pass_row_stride(a.m), true) * sizeof(double2);
+}
 
 template <class PL>
 cudaError_t launch_fwd_xp_pl(const XArgs& a, FwdSource src, const dim3& grid, cudaStream_t st) {
@@ -682,7 +684,7 @@ int staged_tz(int m, int nz) {
     for (int tz = 4; tz >= 1; tz /= 2) {
         if (nz % tz) continue;
         const size_t bytes = (size_t)(4 * tz + 1) * (2 * m + 2) * sizeof(double) +
-                             (size_t)padded_len(tz * (m + 1), true) * sizeof(double2) + 16;
+                             (size_t)padded_len(tz * pass_row_stride(m), true) * sizeof(double2) + 16;
         if (bytes <= 72 * 1024) return tz;
     }
     return 0;
@@ -692,7 +694,7 @@ template <class PL, int TZ, int NT>
 cudaError_t launch_fwd_xs_tz(const XArgs& a, int* err, cudaStream_t st) {
     constexpr int m = PL::n;
     const size_t smem = (size_t)(4 * TZ + 1) * (2 * m + 2) * sizeof(double) +
-                        (size_t)padded_len(TZ * (m + 1), true) * sizeof(double2) + 16;
+                        (size_t)padded_len(TZ * pass_row_stride(m), true) * sizeof(double2) + 16;
     XsArgs xs{};
     xs.a = a;
     xs.a.tz = TZ;
