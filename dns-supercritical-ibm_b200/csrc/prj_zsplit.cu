@@ -16,6 +16,8 @@
 // of nx/2+1 CTAs.  The Thomas arithmetic keeps the reference's operation order
 // and rounding (poisson_solver_multigpu.f90:401-419) with pivots D from the
 // plan's table (the pair kz, nz-kz shares one pivot row entry).
+#include <cstdlib>
+
 #include "fft_pass.cuh"
 #include "prj_internal.h"
 
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
 
 // Pass-plan z transform (fft_pass.cuh): the first pass reads the rows from global
 // memory, the last writes them back; rb rows per CTA, kPassThreads threads.
-template <int DIR, typename T, class PL>
+template <int DIR, typename T, class PL, bool STAGE_INV = false>
 __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_zfft_pass(const ZfftArgs a) {
     extern __shared__ __align__(16) double2 zp[];
     constexpr int n = PL::n;
@@ -83,7 +85,8 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_zfft_pass(const
     const double2* tw = a.tw;
     // the forward transform's slot-order rows leave shared memory in whole coalesced
     // rows (its last pass would store R contiguous elements per thread: half-sector
-    // writes per instruction); the inverse reads them directly (measured faster)
+    // writes per instruction); the inverse copies them in whole rows the same way
+    // (STAGE_INV) or reads them in its first pass
     const int tot = nr * n;
     if (DIR < 0) {
         dif_first_pass<-1, PL>(zp, nr, n, tw, [&](int r, int e) { return to_d2(X[(size_t)r * n + e]); });
@@ -91,9 +94,17 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_zfft_pass(const
         dif_passes_shared<-1, PL, 1, PL::P>(zp, nr, n, tw);
         for (int i = threadIdx.x; i < tot; i += blockDim.x) from_d2(X[i], zp[sidx<true>(i)]);
     } else {
-        dit_first_pass<+1, PL>(zp, nr, n, [&](int r, int q) { return to_d2(X[(size_t)r * n + q]); });
-        __syncthreads();
-        dit_passes_shared<+1, PL, PL::P - 2, 0>(zp, nr, n, tw);
+        if (STAGE_INV) {
+            // slot-order rows copied in whole (coalesced), every pass in shared memory
+#pragma unroll 4
+            for (int i = threadIdx.x; i < tot; i += blockDim.x) zp[sidx<true>(i)] = to_d2(X[i]);
+            __syncthreads();
+            dit_passes_shared<+1, PL, PL::P - 1, 0>(zp, nr, n, tw);
+        } else {
+            dit_first_pass<+1, PL>(zp, nr, n, [&](int r, int q) { return to_d2(X[(size_t)r * n + q]); });
+            __syncthreads();
+            dit_passes_shared<+1, PL, PL::P - 2, 0>(zp, nr, n, tw);
+        }
         dit_last_pass<+1, PL>(zp, nr, n, tw, [&](int r, int e, double2 v) { from_d2(X[(size_t)r * n + e], v); });
     }
 }
@@ -384,6 +395,19 @@ cudaError_t launch_zfft_pass_pl(ZfftArgs a, int rows_req, cudaStream_t st) {
     const size_t smem = (size_t)padded_len(a.rb * PL::n, true) * sizeof(double2);
     const unsigned grid = (unsigned)((a.nrow_total + a.rb - 1) / a.rb);
     if (grid == 0) return cudaSuccess;
+    // the inverse stages its slot-order rows through shared memory (coalesced copy-in);
+    // PRJ_ZINV_STAGE=0 reads them in its first pass instead (measured at 768x384x384:
+    // 0.33 ms staged against 0.37 ms direct; 0.093 / 0.113 ms at 512x256x256)
+    static const bool stage_inv = [] {
+        const char* v = getenv("PRJ_ZINV_STAGE");
+        return !(v && atoi(v) == 0);
+    }();
+    if (DIR > 0 && stage_inv) {
+        cudaError_t e = allow_smem(k_zfft_pass<DIR, T, PL, true>, smem);
+        if (e != cudaSuccess) return e;
+        k_zfft_pass<DIR, T, PL, true><<<grid, kPassThreads, smem, st>>>(a);
+        return cudaGetLastError();
+    }
     cudaError_t e = allow_smem(k_zfft_pass<DIR, T, PL>, smem);
     if (e != cudaSuccess) return e;
     k_zfft_pass<DIR, T, PL><<<grid, kPassThreads, smem, st>>>(a);
