@@ -24,7 +24,10 @@ namespace prj {
 
 namespace {
 
-constexpr int kUnroll = 4;  // global loads kept in flight per thread in the load phases
+#ifndef PRJ_X_UNROLL
+#define PRJ_X_UNROLL 4
+#endif
+constexpr int kUnroll = PRJ_X_UNROLL;  // items whose global loads are in flight per thread in the load phases
 
 __device__ __forceinline__ size_t hidx_d(int nx, int nz, int i, int j, int k) {
     return (size_t)(i + 1) + (size_t)(nx + 2) * ((size_t)(j + 1) + (size_t)(nz + 2) * (size_t)(k + 1));

@@ -75,8 +75,14 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
 
 // Pass-plan z transform (fft_pass.cuh): the first pass reads the rows from global
 // memory, the last writes them back; rb rows per CTA, kPassThreads threads.
+// resident CTAs per SM asked of the pass-plan z kernels (measured at 768x384x384: 5 gives
+// the forward z 0.300 ms against 0.345 ms at 6, the x kernels' setting)
+#ifndef PRJ_ZPASS_MINB
+#define PRJ_ZPASS_MINB 5
+#endif
+
 template <int DIR, typename T, class PL, bool STAGE_INV = false>
-__global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_zfft_pass(const ZfftArgs a) {
+__global__ void __launch_bounds__(kPassThreads, PRJ_ZPASS_MINB) k_zfft_pass(const ZfftArgs a) {
     extern __shared__ __align__(16) double2 zp[];
     constexpr int n = PL::n;
     const size_t row0 = (size_t)blockIdx.x * a.rb;
