@@ -610,12 +610,13 @@ def main():
                                        world=world, dist=dist)
         torch.cuda.empty_cache()
     if not args.no_extra and world == 1:
-        extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
-        torch.cuda.empty_cache()
-        # the same request mix at a rate one GPU sustains: latency without queue growth
-        extra["served_sustainable"] = run_served(device, min(10.0, args.served_seconds), 1000.0,
-                                                 args.served_budget_gb * 1e9)
-        torch.cuda.empty_cache()
+        if args.served_seconds > 0:  # --served-seconds 0 leaves the served legs out
+            extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
+            torch.cuda.empty_cache()
+            # the same request mix at a rate one GPU sustains: latency without queue growth
+            extra["served_sustainable"] = run_served(device, min(10.0, args.served_seconds), 1000.0,
+                                                     args.served_budget_gb * 1e9)
+            torch.cuda.empty_cache()
         extra["variable_density"] = run_vd(device, NX, NY, NZ, steps=max(3, args.steps // 4), warmup=args.warmup)
         torch.cuda.empty_cache()
         if args.rough_grid:

@@ -1044,8 +1044,7 @@ int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_V
     }
     {
         StageTimer tm(plan, prj::kStVdRhs, st);
-        CK(prj::launch_vd_rho_min(plan, vd->rho, slot, st), "rho_min");
-        CK(prj::launch_vd_half_inv(plan, vd->rho, plan->vd_ih, st), "0.5 / rho");
+        CK(prj::launch_vd_prep(plan, vd->rho, plan->vd_ih, slot, st), "rho_min and 0.5 / rho");
         CK(prj::launch_vd_rhs(plan, d_Uh, d_Vh, d_Wh, f, sc, slot, d_P, st), "variable-density right-hand side");
     }
     if (mode == PRJ_MODE_FP32_REFINE) {

@@ -219,8 +219,9 @@ struct VdFields {
     const double* div_now;
     double* P_next;
 };
-cudaError_t launch_vd_rho_min(const prj_plan* pl, const double* rho, unsigned long long* slot, cudaStream_t st);
-cudaError_t launch_vd_half_inv(const prj_plan* pl, const double* rho, double* ih, cudaStream_t st);
+// rho_min and 0.5 / rho in one pass over rho
+cudaError_t launch_vd_prep(const prj_plan* pl, const double* rho, double* ih, unsigned long long* slot,
+                           cudaStream_t st);
 cudaError_t launch_vd_rhs(const prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, const VdFields& f,
                           const StepScalars& sc, const unsigned long long* slot, double* P, cudaStream_t st);
 cudaError_t launch_vd_correction(const prj_plan* pl, const double* P, const double* Uh, const double* Vh,

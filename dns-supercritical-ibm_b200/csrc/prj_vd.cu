@@ -34,23 +34,22 @@ __device__ __forceinline__ double of_ord(unsigned long long o) {
     return __longlong_as_double((long long)b);
 }
 
-__global__ void k_rho_min(int nx, int nz, int ny, const double* __restrict__ rho, unsigned long long* out) {
+// one read of rho: ih = 0.5 / rho on the whole halo'd box (the quotient both stencils form
+// for every neighbour, computed once: the same correctly rounded values), and rho_min, the
+// minimum over the interior (mod_cfd_subroutines.f90:476-486), reduced by fmin and an
+// atomicMin on the order-preserving integer image, both exact and order-free
+__global__ void k_rho_prep(int nx, int nz, int ny, const double* __restrict__ rho, double* __restrict__ ih,
+                           unsigned long long* out) {
+    const size_t hx = (size_t)nx + 2, hz = (size_t)nz + 2, n = hx * hz * ((size_t)ny + 2);
     double m = 1e20;  // mod_cfd_subroutines.f90:476
-    const size_t tot = (size_t)nx * nz * ny;
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < tot; idx += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(idx % nx);
-        const size_t r = idx / nx;
-        m = fmin(m, rho[hix(nx, nz, i, (int)(r % nz), (int)(r / nz))]);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double r = rho[i];
+        ih[i] = __ddiv_rn(0.5, r);
+        const size_t x = i % hx, zr = i / hx, z = zr % hz, y = zr / hz;
+        if (x >= 1 && x <= (size_t)nx && z >= 1 && z <= (size_t)nz && y >= 1 && y <= (size_t)ny) m = fmin(m, r);
     }
     for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMin(out, ord_of(m));
-}
-
-// ih = 0.5 / rho on the whole halo'd box (the quotient both stencils form for every
-// neighbour; computed once, the same correctly rounded values)
-__global__ void k_half_inv(size_t n, const double* __restrict__ rho, double* __restrict__ ih) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        ih[i] = __ddiv_rn(0.5, rho[i]);
 }
 
 struct VdArgs {
@@ -191,21 +190,14 @@ __global__ void __launch_bounds__(128) k_vd_correct(const VdArgs a) {
 
 }  // namespace
 
-cudaError_t launch_vd_rho_min(const prj_plan* pl, const double* rho, unsigned long long* slot, cudaStream_t st) {
+cudaError_t launch_vd_prep(const prj_plan* pl, const double* rho, double* ih, unsigned long long* slot,
+                           cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(slot, 0xff, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const Geometry& g = pl->g;
-    const size_t tot = (size_t)g.nx * g.nz * g.ny;
-    const unsigned blocks = (unsigned)std::min<size_t>((tot + 255) / 256, 148 * 8);
-    k_rho_min<<<blocks, 256, 0, st>>>(g.nx, g.nz, g.ny, rho, slot);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_vd_half_inv(const prj_plan* pl, const double* rho, double* ih, cudaStream_t st) {
-    const Geometry& g = pl->g;
     const size_t n = (size_t)(g.nx + 2) * (g.nz + 2) * (g.ny + 2);
     const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
-    k_half_inv<<<blocks, 256, 0, st>>>(n, rho, ih);
+    k_rho_prep<<<blocks, 256, 0, st>>>(g.nx, g.nz, g.ny, rho, ih, slot);
     return cudaGetLastError();
 }
 
