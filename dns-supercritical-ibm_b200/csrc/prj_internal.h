@@ -195,6 +195,8 @@ size_t pass_x_smem(int m, int tz);       // their shared memory
 // z direction as separate kernels (prj_zsplit.cu); need pl->zd.ok and pl->kz_of_slot
 cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st, YRange yr = YRange{});
 cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st);
+// Thomas sweeps of the lines kx0 .. kx0+rows-1 held in X as [y][kx - kx0][z] (FP64)
+cudaError_t launch_thomas_rows(const prj_plan* pl, double2* X, int kx0, int rows, cudaStream_t st);
 // mixed storage (FP64 rows kx < kxs in spec, FP32 rows in spec32)
 cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st);
 cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st);

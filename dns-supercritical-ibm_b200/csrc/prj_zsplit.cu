@@ -520,6 +520,10 @@ cudaError_t launch_thomas(const prj_plan* pl, cudaStream_t st) {
     return launch_thomas_t<double2>(pl, pl->spec, 0, pl->g.nxh, st);
 }
 
+cudaError_t launch_thomas_rows(const prj_plan* pl, double2* X, int kx0, int rows, cudaStream_t st) {
+    return launch_thomas_t<double2>(pl, X, kx0, rows, st);
+}
+
 // mixed storage: FP64 rows kx < kxs in pl->spec (kxs rows per plane), FP32 rows in pl->spec32
 cudaError_t launch_zfft_mixed(const prj_plan* pl, int dir, cudaStream_t st) {
     cudaError_t e = launch_zfft_t<double2>(pl, dir, pl->spec, pl->kxs, st);

@@ -56,6 +56,7 @@ EXPORTS = (
     "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
     "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
     "prj_projection_step_host_async", "prj_host_async_wait", "prj_selftest_wait_timeout",
+    "prj_dist_forward", "prj_dist_pack", "prj_dist_thomas", "prj_dist_unpack", "prj_dist_inverse",
 )
 
 BANDS_REFERENCE = 0
@@ -162,6 +163,11 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_set_vd_metric.argtypes = [_vp, _dp]
     L.prj_projection_step_vd.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(StepParams),
                                          ctypes.POINTER(VdFields), i, ctypes.POINTER(Stats), _vp]
+    L.prj_dist_forward.argtypes = [_vp, _vp, i, i, _vp]
+    L.prj_dist_pack.argtypes = [_vp, i, i, ip, i, _vp, _vp]
+    L.prj_dist_thomas.argtypes = [_vp, _vp, i, i, _vp]
+    L.prj_dist_unpack.argtypes = [_vp, i, i, ip, i, _vp, _vp]
+    L.prj_dist_inverse.argtypes = [_vp, _vp, i, i, _vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.prj_last_error_string.restype = ctypes.c_char_p

@@ -1,0 +1,156 @@
+"""One FP64 Poisson solve spread over several GPUs (ranks).
+
+The reference spreads a solve over MPI ranks and moves the spectrum between pencil
+ownerships with diezDecomp transposes (src/poisson_solver_mgpu_dtdma/
+poisson_solver_multigpu.f90:328-554).  Here rank r owns the y planes ``y_bounds[r] ..
+y_bounds[r+1]`` of P for the x and z transforms and the x wavenumbers ``kx_bounds[r] ..
+kx_bounds[r+1]`` for the Thomas lines, and one all-to-all each way moves the spectrum
+between the two ownerships:
+
+    forward x, z (own planes) -> pack by destination kx range -> all-to-all ->
+    Thomas (own lines, all planes) -> all-to-all back -> unpack -> inverse z, x.
+
+The stages are the engine's C-ABI calls ``prj_dist_*`` (the single-GPU kernels on plane
+and line subsets), so the assembled P equals the one-GPU solve bit for bit.  The
+exchange is a callable ``exchange(out, inp, out_splits, in_splits)`` with the meaning of
+``torch.distributed.all_to_all_single``: ``nccl_exchange`` between GPUs, or the in-process
+copy of ``solve_emulated``, which runs all ranks' stages on one device.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import prj
+
+
+def split_bounds(n: int, parts: int):
+    """Bounds of ``parts`` contiguous ranges tiling [0, n), sizes differing by at most one."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    q, r = divmod(n, parts)
+    b = [0]
+    for p in range(parts):
+        b.append(b[-1] + q + (1 if p < r else 0))
+    return b
+
+
+class Engine:
+    """The stage calls of one rank on its plan (ctypes into libprj_b200.so)."""
+
+    def __init__(self, plan):
+        self.plan = plan
+        self.L = prj.load_library()
+
+    def _s(self, stream):
+        return prj._stream_ptr(stream)
+
+    def forward(self, P_local, y0, y1, stream=None):
+        prj._check(self.L.prj_dist_forward(self.plan.handle, ctypes.c_void_p(P_local.data_ptr()), y0, y1,
+                                           self._s(stream)))
+
+    def pack(self, y0, y1, kx_bounds, send, stream=None):
+        kb = (ctypes.c_int * len(kx_bounds))(*kx_bounds)
+        prj._check(self.L.prj_dist_pack(self.plan.handle, y0, y1, kb, len(kx_bounds) - 1,
+                                        ctypes.c_void_p(send.data_ptr()), self._s(stream)))
+
+    def thomas(self, lines, kx0, kx1, stream=None):
+        prj._check(self.L.prj_dist_thomas(self.plan.handle, ctypes.c_void_p(lines.data_ptr()), kx0, kx1,
+                                          self._s(stream)))
+
+    def unpack(self, y0, y1, kx_bounds, recv, stream=None):
+        kb = (ctypes.c_int * len(kx_bounds))(*kx_bounds)
+        prj._check(self.L.prj_dist_unpack(self.plan.handle, y0, y1, kb, len(kx_bounds) - 1,
+                                          ctypes.c_void_p(recv.data_ptr()), self._s(stream)))
+
+    def inverse(self, P_local, y0, y1, stream=None):
+        prj._check(self.L.prj_dist_inverse(self.plan.handle, ctypes.c_void_p(P_local.data_ptr()), y0, y1,
+                                           self._s(stream)))
+
+
+class DistSolve:
+    """Rank ``rank`` of ``world`` in a solve of the grid ``(nx, nz, ny)``.  Buffers are
+    float64 tensors on ``device`` (two doubles per complex spectrum value)."""
+
+    def __init__(self, grid, rank: int, world: int, engine, device):
+        import torch
+        nx, nz, ny = grid
+        self.rank, self.world, self.engine = rank, world, engine
+        self.nz, self.ny = nz, ny
+        self.nh = nx // 2 + 1
+        self.y_bounds = split_bounds(ny, world)
+        self.kx_bounds = split_bounds(self.nh, world)
+        self.y0, self.y1 = self.y_bounds[rank], self.y_bounds[rank + 1]
+        self.kx0, self.kx1 = self.kx_bounds[rank], self.kx_bounds[rank + 1]
+        rows, nkx = self.y1 - self.y0, self.kx1 - self.kx0
+        z2 = 2 * nz
+        # forward exchange: blocks [q][y - y0][kx - kxb[q]][z] out, lines [y][kx - kx0][z] in
+        self.fwd_in = [rows * (self.kx_bounds[q + 1] - self.kx_bounds[q]) * z2 for q in range(world)]
+        self.fwd_out = [(self.y_bounds[p + 1] - self.y_bounds[p]) * nkx * z2 for p in range(world)]
+        self.send = torch.empty(max(1, sum(self.fwd_in)), dtype=torch.float64, device=device)
+        self.lines = torch.empty(max(1, sum(self.fwd_out)), dtype=torch.float64, device=device)
+        self.back = torch.empty(max(1, sum(self.fwd_in)), dtype=torch.float64, device=device)
+
+    # the three phases between the exchanges
+    def phase_forward(self, P_local, stream=None):
+        self.engine.forward(P_local, self.y0, self.y1, stream)
+        self.engine.pack(self.y0, self.y1, self.kx_bounds, self.send, stream)
+
+    def phase_lines(self, stream=None):
+        self.engine.thomas(self.lines, self.kx0, self.kx1, stream)
+
+    def phase_inverse(self, P_local, stream=None):
+        self.engine.unpack(self.y0, self.y1, self.kx_bounds, self.back, stream)
+        self.engine.inverse(P_local, self.y0, self.y1, stream)
+
+    def solve(self, P_local, exchange, stream=None):
+        """In-place solve of this rank's planes ``P_local`` ((y1-y0) x nz x nx, x fastest).
+        Every rank calls it; ``exchange`` is collective."""
+        self.phase_forward(P_local, stream)
+        exchange(self.lines, self.send, self.fwd_out, self.fwd_in)
+        self.phase_lines(stream)
+        exchange(self.back, self.lines, self.fwd_in, self.fwd_out)
+        self.phase_inverse(P_local, stream)
+
+
+def nccl_exchange(dist, stream=None):
+    """all_to_all_single over the default process group (NCCL between GPUs), ordered after
+    the work queued on ``stream`` (the current stream if None)."""
+    import torch
+
+    def ex(out, inp, out_splits, in_splits):
+        s = stream or torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            dist.all_to_all_single(out[:sum(out_splits)], inp[:sum(in_splits)], out_splits, in_splits)
+    return ex
+
+
+def solve_emulated(plans, P, world: int):
+    """Run the ``world`` ranks of one solve on a single device, one plan per rank, with an
+    in-process exchange (for tests: the data movement of the distributed solve without
+    NCCL).  ``P`` is the whole (ny, nz, nx) tensor, solved in place; returns it."""
+    g = plans[0].grid
+    ranks = [DistSolve((g.nx, g.nz, g.ny), r, world, Engine(plans[r]), P.device) for r in range(world)]
+    locs = [P[rk.y0:rk.y1] for rk in ranks]
+
+    def exchange_all(outs, inps, out_splits, in_splits):
+        # rank p's input chunk q goes to rank q's output chunk p
+        in_off = [[sum(in_splits[p][:q]) for q in range(world)] for p in range(world)]
+        out_off = [[sum(out_splits[q][:p]) for p in range(world)] for q in range(world)]
+        for p in range(world):
+            for q in range(world):
+                n = in_splits[p][q]
+                assert n == out_splits[q][p]
+                if n:
+                    outs[q][out_off[q][p]:out_off[q][p] + n].copy_(inps[p][in_off[p][q]:in_off[p][q] + n])
+
+    for rk, Pl in zip(ranks, locs):
+        rk.phase_forward(Pl)
+    exchange_all([rk.lines for rk in ranks], [rk.send for rk in ranks],
+                 [rk.fwd_out for rk in ranks], [rk.fwd_in for rk in ranks])
+    for rk in ranks:
+        rk.phase_lines()
+    exchange_all([rk.back for rk in ranks], [rk.lines for rk in ranks],
+                 [rk.fwd_in for rk in ranks], [rk.fwd_out for rk in ranks])
+    for rk, Pl in zip(ranks, locs):
+        rk.phase_inverse(Pl)
+    return P

@@ -350,6 +350,37 @@ int prj_poisson_fp64_noalloc(int nx, int nz, int ny, double dx, double dz,
                              const double* band_a00, const double* band_b00, const double* band_c00,
                              double* d_P, void* stream);
 
+/* One FP64 Poisson solve spread over several GPUs (one rank per GPU, each with a
+ * plan of the whole grid on its own device).  Replaces the multi-rank form of
+ * run_spec_poisson_multigpu (poisson_solver_multigpu.f90:328-554 with
+ * mpi_divs_z x mpi_divs_y > 1, whose diezDecomp transposes tr_poi_xy / tr_poi_yx
+ * move the spectrum between ownerships).  Rank r owns the y planes [y0, y1) of P
+ * for the transforms and the x wavenumbers [kx_bounds[r], kx_bounds[r+1]) for the
+ * Thomas lines; the caller moves the spectrum between the two with an all-to-all
+ * (dns-supercritical-ibm_b200/prj_dist.py does it over torch.distributed / NCCL).
+ * The y ranges ascend with the rank and tile [0, ny); kx_bounds[0] = 0 and
+ * kx_bounds[nranks] = nx/2+1.  Needs a z length with a compile-time pass plan and
+ * an x length of radices 2, 3, 4, 5, 6, 8.
+ * All calls are asynchronous on `stream`.  Spectrum values are complex FP64
+ * (two doubles).
+ *   prj_dist_forward  forward x and z transforms of the planes [y0, y1); d_P_local
+ *                     holds those planes, (y1-y0) x nz x nx values, x fastest.
+ *   prj_dist_pack     the planes' spectrum as blocks for the destinations q,
+ *                     q-major: [q][y - y0][kx - kx_bounds[q]][z].
+ *   prj_dist_thomas   Thomas sweeps of the lines kx0 .. kx1-1 held in d_lines as
+ *                     [y][kx - kx0][z] over all ny planes (the blocks received
+ *                     from all ranks, in rank order).
+ *   prj_dist_unpack   the blocks received back (layout of prj_dist_pack) into the
+ *                     planes' spectrum.
+ *   prj_dist_inverse  inverse z and x transforms of the planes into d_P_local.
+ * The assembled P equals prj_poisson_fp64's on one GPU bit for bit. */
+int prj_dist_forward(prj_plan* plan, const double* d_P_local, int y0, int y1, void* stream);
+int prj_dist_pack(prj_plan* plan, int y0, int y1, const int* kx_bounds, int nranks, double* d_send, void* stream);
+int prj_dist_thomas(prj_plan* plan, double* d_lines, int kx0, int kx1, void* stream);
+int prj_dist_unpack(prj_plan* plan, int y0, int y1, const int* kx_bounds, int nranks, const double* d_recv,
+                    void* stream);
+int prj_dist_inverse(prj_plan* plan, double* d_P_local, int y0, int y1, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* prj_last_error_string(void);
 
