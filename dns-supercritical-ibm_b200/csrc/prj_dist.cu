@@ -84,9 +84,63 @@ int move_blocks(prj_plan* pl, int y0, int y1, const int* kxb, int R, double2* bl
     return PRJ_OK;
 }
 
+prj::StepScalars scalars(const prj_step_params* params) {
+    prj::StepScalars sc{};
+    sc.dt = params->dt;
+    sc.inv_dt = 1.0 / params->dt;
+    sc.wall[0] = params->wall_U_bot; sc.wall[1] = params->wall_V_bot; sc.wall[2] = params->wall_W_bot;
+    sc.wall[3] = params->wall_U_top; sc.wall[4] = params->wall_V_top; sc.wall[5] = params->wall_W_top;
+    return sc;
+}
+
+int step_check(const prj_plan* pl, const prj_step_params* params) {
+    if (!pl->has_metrics) return record_error(PRJ_ERR_STATE, "prj_dist: plan was created without inv_dy_p / dPdy");
+    if (!params || !(params->dt > 0)) return record_error(PRJ_ERR_ARG, "prj_dist: NULL params or dt <= 0");
+    return PRJ_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int prj_dist_divergence(prj_plan* plan, const double* d_Uh_loc, const double* d_Vh_loc, const double* d_Wh_loc,
+                        int y0, int y1, const prj_step_params* params, void* stream) {
+    int rc = dist_check(plan, y0, y1);
+    if (rc || (rc = step_check(plan, params))) return rc;
+    if (y1 == y0) return PRJ_OK;
+    if (!d_Uh_loc || !d_Vh_loc || !d_Wh_loc) return record_error(PRJ_ERR_ARG, "prj_dist_divergence: NULL field");
+    OnPlanDevice od(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const prj::StepScalars sc = scalars(params);
+    // the local halo'd arrays start at halo'd plane y0 (global plane y0 - 1)
+    const ptrdiff_t shift = (ptrdiff_t)y0 * (plan->g.nx + 2) * (plan->g.nz + 2);
+    const prj::YRange yr{y0, y1};
+    if ((rc = cuda_rc(prj::launch_fwd_x_range(plan, d_Uh_loc - shift, d_Vh_loc - shift, d_Wh_loc - shift, &sc, st, yr),
+                      "divergence + forward x")))
+        return rc;
+    return cuda_rc(prj::launch_zfft(plan, -1, st, yr), "forward z");
+}
+
+int prj_dist_correct(prj_plan* plan, const double* d_P_ext, const double* d_Uh_loc, const double* d_Vh_loc,
+                     const double* d_Wh_loc, double* d_U_loc, double* d_V_loc, double* d_W_loc, int y0, int y1,
+                     const prj_step_params* params, void* stream) {
+    int rc = dist_check(plan, y0, y1);
+    if (rc || (rc = step_check(plan, params))) return rc;
+    if (y1 == y0) return PRJ_OK;
+    if (!d_P_ext || !d_Uh_loc || !d_Vh_loc || !d_Wh_loc || !d_U_loc || !d_V_loc || !d_W_loc)
+        return record_error(PRJ_ERR_ARG, "prj_dist_correct: NULL array");
+    OnPlanDevice od(plan->device);
+    const prj::StepScalars sc = scalars(params);
+    const ptrdiff_t shift = (ptrdiff_t)y0 * (plan->g.nx + 2) * (plan->g.nz + 2);
+    // d_P_ext holds planes y0-1 .. y1-1 of P
+    const double* Pg = d_P_ext - (ptrdiff_t)(y0 - 1) * plan->g.nz * plan->g.nx;
+    // halo'd planes y0+1 .. y1 (global planes y0 .. y1-1), plus the wall planes at the ends
+    const prj::YRange kh{y0 == 0 ? 0 : y0 + 1, y1 == plan->g.ny ? plan->g.ny + 2 : y1 + 1};
+    return cuda_rc(prj::launch_correction(plan, Pg, d_Uh_loc - shift, d_Vh_loc - shift, d_Wh_loc - shift,
+                                          d_U_loc - shift, d_V_loc - shift, d_W_loc - shift, sc, (cudaStream_t)stream,
+                                          kh),
+                   "correction");
+}
 
 int prj_dist_forward(prj_plan* plan, const double* d_P_local, int y0, int y1, void* stream) {
     int rc = dist_check(plan, y0, y1);

@@ -57,6 +57,7 @@ EXPORTS = (
     "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
     "prj_projection_step_host_async", "prj_host_async_wait", "prj_selftest_wait_timeout",
     "prj_dist_forward", "prj_dist_pack", "prj_dist_thomas", "prj_dist_unpack", "prj_dist_inverse",
+    "prj_dist_divergence", "prj_dist_correct",
 )
 
 BANDS_REFERENCE = 0
@@ -168,6 +169,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_dist_thomas.argtypes = [_vp, _vp, i, i, _vp]
     L.prj_dist_unpack.argtypes = [_vp, i, i, ip, i, _vp, _vp]
     L.prj_dist_inverse.argtypes = [_vp, _vp, i, i, _vp]
+    L.prj_dist_divergence.argtypes = [_vp, _vp, _vp, _vp, i, i, ctypes.POINTER(StepParams), _vp]
+    L.prj_dist_correct.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, i, ctypes.POINTER(StepParams), _vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.prj_last_error_string.restype = ctypes.c_char_p

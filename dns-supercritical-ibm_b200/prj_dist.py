@@ -66,6 +66,16 @@ class Engine:
         prj._check(self.L.prj_dist_inverse(self.plan.handle, ctypes.c_void_p(P_local.data_ptr()), y0, y1,
                                            self._s(stream)))
 
+    def divergence(self, Uh, Vh, Wh, y0, y1, params, stream=None):
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        prj._check(self.L.prj_dist_divergence(self.plan.handle, p(Uh), p(Vh), p(Wh), y0, y1, ctypes.byref(params),
+                                              self._s(stream)))
+
+    def correct(self, P_ext, Uh, Vh, Wh, U, V, W, y0, y1, params, stream=None):
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        prj._check(self.L.prj_dist_correct(self.plan.handle, p(P_ext), p(Uh), p(Vh), p(Wh), p(U), p(V), p(W), y0, y1,
+                                           ctypes.byref(params), self._s(stream)))
+
 
 class DistSolve:
     """Rank ``rank`` of ``world`` in a solve of the grid ``(nx, nz, ny)``.  Buffers are
@@ -102,6 +112,27 @@ class DistSolve:
         self.engine.unpack(self.y0, self.y1, self.kx_bounds, self.back, stream)
         self.engine.inverse(P_local, self.y0, self.y1, stream)
 
+    def phase_divergence(self, fields, params, stream=None):
+        Uh, Vh, Wh = fields
+        self.engine.divergence(Uh, Vh, Wh, self.y0, self.y1, params, stream)
+        self.engine.pack(self.y0, self.y1, self.kx_bounds, self.send, stream)
+
+    def project(self, fields, outs, P_ext, params, exchange, plane_exchange, stream=None):
+        """Projection step of this rank's planes.  ``fields`` = (Uh, Vh, Wh) and ``outs`` =
+        (U, V, W): local halo'd arrays of halo'd planes y0 .. y1+1 ((y1-y0+2) x (nz+2) x
+        (nx+2)), ghost planes of the inputs filled by the caller.  ``P_ext`` holds P planes
+        y0-1 .. y1-1 ((y1-y0+1) x nz x nx); its own planes receive P.  ``plane_exchange(
+        P_ext)`` must copy the last own plane of every rank into plane 0 of the next rank's
+        ``P_ext`` (send/recv with the neighbours); ``exchange`` is the all-to-all."""
+        P_own = P_ext[1:]
+        self.phase_divergence(fields, params, stream)
+        exchange(self.lines, self.send, self.fwd_out, self.fwd_in)
+        self.phase_lines(stream)
+        exchange(self.back, self.lines, self.fwd_in, self.fwd_out)
+        self.phase_inverse(P_own, stream)
+        plane_exchange(P_ext)
+        self.engine.correct(P_ext, *fields, *outs, self.y0, self.y1, params, stream)
+
     def solve(self, P_local, exchange, stream=None):
         """In-place solve of this rank's planes ``P_local`` ((y1-y0) x nz x nx, x fastest).
         Every rank calls it; ``exchange`` is collective."""
@@ -122,6 +153,73 @@ def nccl_exchange(dist, stream=None):
         with torch.cuda.stream(s):
             dist.all_to_all_single(out[:sum(out_splits)], inp[:sum(in_splits)], out_splits, in_splits)
     return ex
+
+
+def nccl_plane_exchange(dist, rank: int, world: int):
+    """The neighbour exchange of ``DistSolve.project``: rank r sends its last P plane to
+    rank r+1 and receives plane y0-1 from rank r-1 (point-to-point over the process group)."""
+    def ex(P_ext):
+        ops = []
+        if rank + 1 < world:
+            ops.append(dist.P2POp(dist.isend, P_ext[-1].contiguous(), rank + 1))
+        recv = None
+        if rank > 0:
+            recv = P_ext[0].new_empty(P_ext[0].shape)
+            ops.append(dist.P2POp(dist.irecv, recv, rank - 1))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        if recv is not None:
+            P_ext[0].copy_(recv)
+    return ex
+
+
+def project_emulated(plans, Uh, Vh, Wh, U, V, W, P, params, world: int):
+    """The projection step of ``world`` ranks emulated on one device (one plan per rank,
+    in-process exchanges).  Halo'd tensors are (ny+2, nz+2, nx+2) with filled halos, P is
+    (ny, nz, nx); U, V, W and P are written."""
+    import torch
+    g = plans[0].grid
+    ranks = [DistSolve((g.nx, g.nz, g.ny), r, world, Engine(plans[r]), P.device) for r in range(world)]
+    fields = [tuple(F[rk.y0:rk.y1 + 2] for F in (Uh, Vh, Wh)) for rk in ranks]
+    outs = [tuple(F[rk.y0:rk.y1 + 2] for F in (U, V, W)) for rk in ranks]
+    pext = [torch.zeros((rk.y1 - rk.y0 + 1, g.nz, g.nx), dtype=torch.float64, device=P.device) for rk in ranks]
+    for rk, f in zip(ranks, fields):
+        rk.phase_divergence(f, params)
+    _exchange_all(ranks, world, forward=True)
+    for rk in ranks:
+        rk.phase_lines()
+    _exchange_all(ranks, world, forward=False)
+    for rk, pe in zip(ranks, pext):
+        rk.phase_inverse(pe[1:])
+    for r in range(1, world):
+        pext[r][0].copy_(pext[r - 1][-1])
+    # the correction writes its own planes of the shared output tensors; the local halo'd
+    # views of neighbouring ranks overlap only in ghost planes that neither writes
+    for rk, pe, f, o in zip(ranks, pext, fields, outs):
+        rk.engine.correct(pe, *f, *o, rk.y0, rk.y1, params)
+    for rk, pe in zip(ranks, pext):
+        P[rk.y0:rk.y1].copy_(pe[1:])
+    return U, V, W, P
+
+
+def _exchange_all(ranks, world, forward):
+    """In-process all-to-all between emulated ranks (rank p's input chunk q goes to rank
+    q's output chunk p)."""
+    if forward:
+        outs, inps = [rk.lines for rk in ranks], [rk.send for rk in ranks]
+        out_splits, in_splits = [rk.fwd_out for rk in ranks], [rk.fwd_in for rk in ranks]
+    else:
+        outs, inps = [rk.back for rk in ranks], [rk.lines for rk in ranks]
+        out_splits, in_splits = [rk.fwd_in for rk in ranks], [rk.fwd_out for rk in ranks]
+    for p in range(world):
+        for q in range(world):
+            n = in_splits[p][q]
+            assert n == out_splits[q][p]
+            if n:
+                i0 = sum(in_splits[p][:q])
+                o0 = sum(out_splits[q][:p])
+                outs[q][o0:o0 + n].copy_(inps[p][i0:i0 + n])
 
 
 def solve_emulated(plans, P, world: int):

@@ -380,6 +380,21 @@ int prj_dist_thomas(prj_plan* plan, double* d_lines, int kx0, int kx1, void* str
 int prj_dist_unpack(prj_plan* plan, int y0, int y1, const int* kx_bounds, int nranks, const double* d_recv,
                     void* stream);
 int prj_dist_inverse(prj_plan* plan, double* d_P_local, int y0, int y1, void* stream);
+/* The projection step over ranks (the plan made with metrics, as for
+ * prj_projection_step): prj_dist_divergence takes the place of prj_dist_forward
+ * (the divergence of the predictor, then the forward x and z transforms of the
+ * planes [y0, y1)), and prj_dist_correct follows prj_dist_inverse.  The halo'd local
+ * arrays hold the halo'd planes y0 .. y1+1 (global planes y0-1 .. y1, ghost planes
+ * filled by the caller's halo exchange), (nx+2) x (nz+2) x (y1-y0+2) values, x
+ * fastest.  d_P_ext holds the P planes y0-1 .. y1-1: plane y0-1 from the rank below
+ * (not read on the first rank), then the rank's own planes as prj_dist_inverse left
+ * them.  prj_dist_correct writes the rank's planes of U, V, W with their periodic
+ * x/z halos, and the wall planes on the first and last ranks. */
+int prj_dist_divergence(prj_plan* plan, const double* d_Uh_loc, const double* d_Vh_loc, const double* d_Wh_loc,
+                        int y0, int y1, const prj_step_params* params, void* stream);
+int prj_dist_correct(prj_plan* plan, const double* d_P_ext, const double* d_Uh_loc, const double* d_Vh_loc,
+                     const double* d_Wh_loc, double* d_U_loc, double* d_V_loc, double* d_W_loc, int y0, int y1,
+                     const prj_step_params* params, void* stream);
 
 /* Message of the calling thread's last failure ("" if none). */
 const char* prj_last_error_string(void);

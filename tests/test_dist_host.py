@@ -116,3 +116,50 @@ def test_gloo_ranks_exchange_spectrum_blocks(world):
     assert kxs[0][0] == 0 and kxs[-1][1] == 6 and all(kxs[i][1] == kxs[i + 1][0] for i in range(world - 1))
     for r in res:
         assert r[2] == [], r
+
+
+def _plane_main(rank, world, port, q):
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "dns-supercritical-ibm_b200"))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import prj_dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        b = prj_dist.split_bounds(7, world)
+        y0, y1 = b[rank], b[rank + 1]
+        P_ext = torch.full((y1 - y0 + 1, 3, 4), -1.0, dtype=torch.float64)
+        for y in range(y0, y1):
+            P_ext[y - y0 + 1] = float(y)
+        prj_dist.nccl_plane_exchange(dist, rank, world)(P_ext)
+        dist.barrier()
+        q.put((rank, float(P_ext[0].min()), float(P_ext[0].max()), y0))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_neighbour_plane_exchange(world):
+    """The P plane below each rank's first plane arrives from the rank below (rank 0 keeps
+    its unused plane)."""
+    import socket
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_plane_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(180)
+        assert p.exitcode == 0
+    for rank, lo, hi, y0 in sorted(q.get(timeout=10) for _ in range(world)):
+        if rank == 0:
+            assert lo == hi == -1.0
+        else:
+            assert lo == hi == float(y0 - 1)

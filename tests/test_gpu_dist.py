@@ -52,3 +52,39 @@ def test_bad_ranges_are_refused(cuda_device):
         assert L.prj_dist_pack(plan.handle, 0, ny, bad, 2, ptr, None) == prj.PRJ_ERR_ARG
         assert L.prj_dist_thomas(plan.handle, ptr, 5, 40, None) == prj.PRJ_ERR_ARG
         torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("shape", [(96, 40, 48), (64, 21, 32)])
+def test_emulated_projection_step_equals_single_gpu(cuda_device, monkeypatch, world, shape):
+    """The whole projection step over ranks (divergence of each rank's planes, the
+    exchanges, the solve, the neighbour P plane, each rank's correction) equals the
+    single-GPU step bit for bit in U, V, W (halos and wall planes included) and P."""
+    import torch
+    import prj
+    import prj_dist
+    import workloads
+    from test_gpu_projection import run_engine
+    monkeypatch.setenv("PRJ_ZSOLVE", "split")
+    nx, ny, nz = shape
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=9)
+    for F in (Uh, Vh, Wh):
+        workloads.fill_halos(F)
+    wall = (0.01, 0.0, -0.02, 0.03, 0.0, 0.04)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        ref = run_engine(plan, Uh, Vh, Wh, 0.6, wall)
+    plans = [prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") for _ in range(world)]
+    try:
+        t = lambda A: torch.from_numpy(np.ascontiguousarray(A.transpose(2, 1, 0))).cuda()
+        dUh, dVh, dWh = t(Uh), t(Vh), t(Wh)
+        dU, dV, dW = (torch.full_like(dUh, np.nan) for _ in range(3))
+        dP = torch.zeros((ny, nz, nx), dtype=torch.float64, device="cuda")
+        params = prj.StepParams(0.6, *wall, 0)
+        prj_dist.project_emulated(plans, dUh, dVh, dWh, dU, dV, dW, dP, params, world)
+        torch.cuda.synchronize()
+        got = [A.cpu().numpy().transpose(2, 1, 0) for A in (dU, dV, dW, dP)]
+    finally:
+        for p in plans:
+            p.close()
+    for a, b in zip(got, ref[:4]):
+        np.testing.assert_array_equal(a, b)
