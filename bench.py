@@ -355,6 +355,21 @@ def run_rough(device, nx, ny, nz, steps, warmup):
     out = {"grid": f"{nx}x{ny}x{nz}", "solid_fraction": float(solid.float().mean()),
            "dy_wall": float(yu[1] - yu[0]), "dy_max": float(np.diff(yu).max())}
     stream = torch.cuda.current_stream(device)
+    # immersed-boundary column forcing of the predictor ahead of the step (prj_rough_force,
+    # ibm_part_2): per column the last bottom cell and the first top cell inside the roughness
+    cnt_bot = (yp < ht).sum(dim=0).to(torch.int32)          # [z, x]
+    cnt_top = (yp > 2.0 - ht).sum(dim=0).to(torch.int32)
+    bot = (cnt_bot - 1).contiguous()
+    top = (ny - cnt_top).contiguous()
+    inds = {"U_bot": bot, "U_top": top, "V_bot": bot, "V_top": top, "W_bot": bot, "W_top": top}
+    Uf, Vf, Wf = Uh.clone(), Vh.clone(), Wh.clone()
+    force = lambda: prj.rough_force(Uf, Vf, Wf, inds, stream=stream)
+    for _ in range(warmup):
+        force()
+    f_ms = timed_steps(force, stream, steps) / steps
+    out["ibm_column_forcing"] = {"ms": f_ms, "cells_forced": int(3 * (cnt_bot.sum() + cnt_top.sum())),
+                                 "call": "prj_rough_force on the three predictor components"}
+    del Uf, Vf, Wf
     with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent", device=device.index or 0) as plan:
         P64 = None
         for name, mode in (("fp64", prj.MODE_FP64), ("mixed", prj.MODE_FP32_REFINE)):
