@@ -126,7 +126,10 @@ struct ThomasArgs {
 };
 
 constexpr int kThomasTile = 128;
-constexpr int kBlock = 8;  // planes loaded together (independent loads in flight)
+#ifndef PRJ_THOMAS_BLOCK
+#define PRJ_THOMAS_BLOCK 8
+#endif
+constexpr int kBlock = PRJ_THOMAS_BLOCK;  // planes loaded together (independent loads in flight)
 
 // One line: the CTA's block index `blk` within the buffer a.X (T storage).
 template <typename T>
