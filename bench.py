@@ -13,9 +13,17 @@ the 126 MB L2, so no flush is needed between steps.
 
 value: Gpts/s = (points of all ranks x K) / (max over ranks of the device time
 of K steps), CUDA events on the launching stream.  e2e: the same metric through
-the host-buffer C-ABI call prj_projection_step_host (H2D of u_hat, projection,
-D2H of u, v, w, p inside the timed region).  Multi-GPU runs are independent
-replicas (the path does not shard): weak scaling, no collective.
+the host-buffer C-ABI (H2D of u_hat, projection, D2H of u, v, w, p inside the
+timed region): prj_projection_step_host_async, steps pipelined over two staging
+slots, with the synchronous drop-in prj_projection_step_host beside it.
+Multi-GPU runs are independent replicas (one solve fits one GPU; the API for one
+solve over several GPUs, prj_dist_*, is not timed here): weak scaling, no
+collective on the data path.
+
+roofline: the dominant kernel (algorithmic bytes per launch / its CUDA-event
+duration against the measured HBM peak, and its DRAM traffic from the committed
+ncu summary); roofline_kernels: the same for every step kernel; roofline_step:
+the whole step at 88 B per point.
 
 --impl reference times the CPU restatement of the reference's FFTW path
 (oracle/, all host threads) on the same workload, per step a bounded sample
@@ -590,6 +598,18 @@ def main():
     dom_ms = stages[dom][0] / stages[dom][1]
     achieved = alg[dom] / (dom_ms / 1e3) / 1e9
     traffic = read_traffic(dom)
+    # every step kernel: algorithmic bytes, achieved GB/s and fraction of the peak, and the DRAM
+    # traffic of the committed ncu summary with the GB/s it implies at this duration
+    per_kernel = {}
+    for k, (tot_ms, cnt) in stages.items():
+        if k not in alg or cnt == 0:
+            continue
+        k_ms = tot_ms / cnt
+        tr = read_traffic(k)
+        gbs = alg[k] / (k_ms / 1e3) / 1e9
+        per_kernel[k] = {"alg_bytes": alg[k], "ms": k_ms, "achieved": gbs, "frac": gbs / peak, "traffic": tr,
+                         "traffic_gbs": (tr / (k_ms / 1e3) / 1e9) if tr else None,
+                         "traffic_frac": (tr / (k_ms / 1e3) / 1e9 / peak) if tr else None}
     step_ms = ms_max / args.steps
     roof_step = ALG_BYTES_PER_POINT * NX * NY * NZ / (step_ms / 1e3) / 1e9
     launches = launches_per_step * args.steps
@@ -653,6 +673,7 @@ def main():
                          "alg_bytes_per_launch": alg[dom], "avg_launch_ms": dom_ms},
             "roofline_step": {"alg_bytes_per_point": ALG_BYTES_PER_POINT, "achieved": roof_step, "peak": peak,
                               "unit": "GB/s", "frac": roof_step / peak},
+            "roofline_kernels": per_kernel,
             "stages_ms_per_launch": {k: v[0] / v[1] for k, v in stages.items()},
             "schedule": schedule,
             "stage_share": {k: v[0] / sum(x[0] for x in stages.values()) for k, v in stages.items()},
