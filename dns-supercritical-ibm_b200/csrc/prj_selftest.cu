@@ -7,6 +7,7 @@
 // thread waits, with a short budget, on an mbarrier that nothing arrives on.
 #include "../../include/projection.h"
 #include "prj_internal.h"
+#include "div_rn.cuh"
 #include "tma_util.cuh"
 
 namespace prj {
@@ -23,8 +24,75 @@ __global__ void k_wait_selftest(long long budget, int* err) {
     if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicExch(err, 3);
 }
 
+// splitmix64: a reproducible stream of 64-bit words per index
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// a double with a random sign and mantissa and an exponent in [-span, span] about 1;
+// every eighth value has an all-ones or all-zeros mantissa (the rounding edges)
+__device__ __forceinline__ double random_double(unsigned long long w, unsigned long long w2, int span) {
+    unsigned long long mant = w & 0xfffffffffffffull;
+    const int sel = (int)(w2 & 7);
+    if (sel == 0) mant = 0xfffffffffffffull;
+    if (sel == 1) mant = 0;
+    const int ex = 1023 + (int)((w2 >> 8) % (unsigned long long)(2 * span + 1)) - span;
+    const unsigned long long bits = ((w >> 63) << 63) | ((unsigned long long)ex << 52) | mant;
+    return __longlong_as_double((long long)bits);
+}
+
+__global__ void k_div_selftest(long long n, unsigned long long seed, unsigned long long* bad, double* first) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = seed * 0x100000000ull + (unsigned long long)i * 4;
+        const unsigned long long wu = mix64(k), wu2 = mix64(k + 1);
+        double u = random_double(wu, wu2, 200);
+        if (((wu2 >> 20) & 31) == 0) u = (wu >> 63) ? -0.0 : 0.0;  // signed zero numerators
+        const double D = random_double(mix64(k + 2), mix64(k + 3), 100);
+        const double want = __ddiv_rn(u, D);
+        const double got = div_by_recip(u, D, __drcp_rn(D));
+        if (__double_as_longlong(want) != __double_as_longlong(got)) {
+            if (atomicAdd(bad, 1ull) == 0) {
+                first[0] = u;
+                first[1] = D;
+            }
+        }
+    }
+}
+
 }  // namespace
 }  // namespace prj
+
+extern "C" int prj_selftest_division(int device, long long n, unsigned long long seed, long long* mismatches,
+                                     double* first_u, double* first_d) {
+    if (n < 1 || !mismatches) return prj::record_error(PRJ_ERR_ARG, "need n >= 1 and a result pointer");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaError_t e = cudaSetDevice(device);
+    unsigned long long* d_bad = nullptr;
+    double* d_first = nullptr;
+    unsigned long long h_bad = 0;
+    double h_first[2] = {0.0, 0.0};
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_bad, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_first, 2 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(d_bad, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        prj::k_div_selftest<<<148 * 8, 256>>>(n, seed, d_bad, d_first);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h_bad, d_bad, sizeof(h_bad), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(h_first, d_first, sizeof(h_first), cudaMemcpyDeviceToHost);
+    if (d_bad) cudaFree(d_bad);
+    if (d_first) cudaFree(d_first);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return prj::record_error(PRJ_ERR_CUDA, cudaGetErrorString(e));
+    *mismatches = (long long)h_bad;
+    if (first_u) *first_u = h_bad ? h_first[0] : 0.0;
+    if (first_d) *first_d = h_bad ? h_first[1] : 0.0;
+    return PRJ_OK;
+}
 
 extern "C" int prj_selftest_wait_timeout(int device, long long budget_cycles) {
     if (budget_cycles < 1 || budget_cycles > prj::kWaitBudgetCycles)

@@ -25,6 +25,7 @@
 // cp.async copies complete on their own, so no wait here can hang.
 #include <cstdlib>
 
+#include "div_rn.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
 
@@ -124,13 +125,14 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
                 if (slot[q] < n) {
                     double2 v = buf[sidx<true>(r * n + slot[q])];
                     const double D = dbuf[(size_t)r * mzp + kzs[q]];
+                    const double rD = __drcp_rn(D);  // off the recurrence's chain
                     if (y == 0) {
-                        v.x = __ddiv_rn(v.x, D);
-                        v.y = __ddiv_rn(v.y, D);
+                        v.x = div_by_recip(v.x, D, rD);
+                        v.y = div_by_recip(v.y, D, rD);
                     } else {
                         const double av = is00[q] ? bA0[y] : bA[y];
-                        v.x = __ddiv_rn(__dsub_rn(v.x, __dmul_rn(av, prev[q].x)), D);
-                        v.y = __ddiv_rn(__dsub_rn(v.y, __dmul_rn(av, prev[q].y)), D);
+                        v.x = div_by_recip(__dsub_rn(v.x, __dmul_rn(av, prev[q].x)), D, rD);
+                        v.y = div_by_recip(__dsub_rn(v.y, __dmul_rn(av, prev[q].y)), D, rD);
                     }
                     prev[q] = v;
                     grow[slot[q]] = v;

@@ -18,6 +18,7 @@
 // plan's table (the pair kz, nz-kz shares one pivot row entry).
 #include <cstdlib>
 
+#include "div_rn.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
 
@@ -168,12 +169,13 @@ __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
             const int y = y0 + u;
             if (y < ny) {
                 double2 r = v[u];
+                const double rD = __drcp_rn(D[u]);  // off the recurrence's chain
                 if (y == 0) {
-                    r.x = __ddiv_rn(r.x, D[u]);
-                    r.y = __ddiv_rn(r.y, D[u]);
+                    r.x = div_by_recip(r.x, D[u], rD);
+                    r.y = div_by_recip(r.y, D[u], rD);
                 } else {
-                    r.x = __ddiv_rn(__dsub_rn(r.x, __dmul_rn(av[u], prev.x)), D[u]);
-                    r.y = __ddiv_rn(__dsub_rn(r.y, __dmul_rn(av[u], prev.y)), D[u]);
+                    r.x = div_by_recip(__dsub_rn(r.x, __dmul_rn(av[u], prev.x)), D[u], rD);
+                    r.y = div_by_recip(__dsub_rn(r.y, __dmul_rn(av[u], prev.y)), D[u], rD);
                 }
                 prev = r;
                 if (y < ny - 1) from_d2(x[(size_t)y * rstride], r);
@@ -274,13 +276,14 @@ __device__ __forceinline__ void thomas_line_async(const ThomasArgs& a, int blk, 
             if (y < ny) {
                 double2 r = to_d2(xs(st, u));
                 const double D = ds(st, u);
+                const double rD = __drcp_rn(D);  // off the recurrence's chain
                 if (y == 0) {
-                    r.x = __ddiv_rn(r.x, D);
-                    r.y = __ddiv_rn(r.y, D);
+                    r.x = div_by_recip(r.x, D, rD);
+                    r.y = div_by_recip(r.y, D, rD);
                 } else {
                     const double av = A[y];
-                    r.x = __ddiv_rn(__dsub_rn(r.x, __dmul_rn(av, prev.x)), D);
-                    r.y = __ddiv_rn(__dsub_rn(r.y, __dmul_rn(av, prev.y)), D);
+                    r.x = div_by_recip(__dsub_rn(r.x, __dmul_rn(av, prev.x)), D, rD);
+                    r.y = div_by_recip(__dsub_rn(r.y, __dmul_rn(av, prev.y)), D, rD);
                 }
                 prev = r;
                 if (y < ny - 1) from_d2(x[(size_t)y * rstride], r);

@@ -57,7 +57,7 @@ EXPORTS = (
     "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
     "prj_projection_step_host_async", "prj_host_async_wait", "prj_selftest_wait_timeout",
     "prj_dist_forward", "prj_dist_pack", "prj_dist_thomas", "prj_dist_unpack", "prj_dist_inverse",
-    "prj_dist_divergence", "prj_dist_correct",
+    "prj_dist_divergence", "prj_dist_correct", "prj_selftest_division",
 )
 
 BANDS_REFERENCE = 0
@@ -169,6 +169,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_dist_thomas.argtypes = [_vp, _vp, i, i, _vp]
     L.prj_dist_unpack.argtypes = [_vp, i, i, ip, i, _vp, _vp]
     L.prj_dist_inverse.argtypes = [_vp, _vp, i, i, _vp]
+    L.prj_selftest_division.argtypes = [i, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(d), ctypes.POINTER(d)]
     L.prj_dist_divergence.argtypes = [_vp, _vp, _vp, _vp, i, i, ctypes.POINTER(StepParams), _vp]
     L.prj_dist_correct.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, i, ctypes.POINTER(StepParams), _vp]
     for name in EXPORTS:

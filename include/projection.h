@@ -274,6 +274,15 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
  * completed.  No fault, trap or unbounded wait is involved. */
 int prj_selftest_wait_timeout(int device, long long budget_cycles);
 
+/* Diagnostic of the division the Thomas forward sweeps use: n pseudo-random pairs
+ * (u, D) from `seed` (exponents within 2^+-200 and 2^+-100 of 1, random and edge
+ * mantissas), each divided both by __ddiv_rn and by the reciprocal-and-correction form
+ * of div_rn.cuh; *mismatches counts the pairs whose two results differ in any bit
+ * (the first such pair in first_u, first_d when not NULL).  No counterpart in the
+ * reference. */
+int prj_selftest_division(int device, long long n, unsigned long long seed, long long* mismatches,
+                          double* first_u, double* first_d);
+
 /* Kernel launches one prj_projection_step of `mode` issues with the plan's current
  * configuration (statistics excluded), and the number of y chunks of the overlapped
  * FP64 schedule (0 when the kernels run one after another).  The overlapped
