@@ -58,11 +58,20 @@ __host__ __device__ constexpr int zl_lpt(int n) { return n <= 128 ? 1 : n <= 512
 __host__ __device__ constexpr int zl_threads(int n, int lpt) { return n / lpt < 32 ? 32 : n / lpt; }
 __host__ __device__ constexpr int zl_minb(int nt) { return nt <= 64 ? 8 : nt <= 128 ? 5 : nt <= 384 ? 3 : 2; }
 
+// Pivot rows in shared memory: rows of mzs = mzp rounded up to 16 doubles; the 16-byte
+// piece j (kzs 2j, 2j+1) sits at piece zl_piece(j), which permutes the pieces of each
+// 128-byte group by the group index.  The Thomas phase gathers pivots by wavenumber in
+// the slots' digit-reversed order: the permutation spreads the 8 pieces that a stride of
+// 8 groups apart would put on one bank pair (n = 384: 129 -> 68 wavefronts per plane for
+// the CTA's pivot reads, against 24 conflict-free).
+__host__ __device__ constexpr int zl_mzs(int mzp) { return (mzp + 15) & ~15; }
+__device__ __forceinline__ int zl_piece(int j) { return (j & ~7) | ((j ^ (j >> 3)) & 7); }
+
 template <class PL, int NS, int LPT>
 __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL::n, LPT))) k_zline(const ZLineArgs a) {
     constexpr int n = PL::n, NT = zl_threads(n, LPT);
     extern __shared__ __align__(16) unsigned char zsm[];
-    const int ny = a.ny, nh = a.nh, mzp = a.mzp, yb = a.yb, tid = threadIdx.x;
+    const int ny = a.ny, nh = a.nh, mzp = a.mzp, mzs = zl_mzs(mzp), yb = a.yb, tid = threadIdx.x;
     const int kx = blockIdx.x;
     double2* ring = reinterpret_cast<double2*>(zsm);  // NS * yb rows of n, padded as one array
     double* dring = reinterpret_cast<double*>(zsm + (size_t)padded_len(NS * yb * n, true) * sizeof(double2));
@@ -75,7 +84,8 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
     for (int q = 0; q < LPT; q++) {
         slot[q] = tid + q * NT;
         const int kz = slot[q] < n ? a.kz_of_slot[slot[q]] : 0;
-        kzs[q] = kz <= n - kz ? kz : n - kz;
+        const int kf = kz <= n - kz ? kz : n - kz;
+        kzs[q] = 2 * zl_piece(kf >> 1) + (kf & 1);  // position in a shared pivot row
         is00[q] = (kx == 0 && kz == 0);
     }
     const double* bA = a.bands;
@@ -93,10 +103,10 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
                 zl_cp16(&buf[sidx<true>(r * n + e)], a.X + ((size_t)(y0 + r) * nh + kx) * n + e);
             }
             const int hp = mzp / 2;  // 16-byte pieces of a pivot row
-            double* dbuf = dring + (size_t)s * yb * mzp;
+            double* dbuf = dring + (size_t)s * yb * mzs;
             for (int i = tid; i < nr * hp; i += NT) {
                 const int r = i / hp, j = i - r * hp;
-                zl_cp16(dbuf + (size_t)r * mzp + 2 * j, tab + ((size_t)(y0 + r) * nh + kx) * mzp + 2 * j);
+                zl_cp16(dbuf + (size_t)r * mzs + 2 * zl_piece(j), tab + ((size_t)(y0 + r) * nh + kx) * mzp + 2 * j);
             }
         }
         zl_commit();
@@ -115,7 +125,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
         __syncthreads();
         const int s = c % NS, y0 = c * yb, nr = min(yb, ny - y0);
         double2* buf = ring + sidx<true>(s * yb * n);
-        const double* dbuf = dring + (size_t)s * yb * mzp;
+        const double* dbuf = dring + (size_t)s * yb * mzs;
         dif_passes_shared<-1, PL, 0, PL::P>(buf, nr, n, a.tw);  // barrier after every pass
         for (int r = 0; r < nr; r++) {
             const int y = y0 + r;
@@ -124,7 +134,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
             for (int q = 0; q < LPT; q++) {
                 if (slot[q] < n) {
                     double2 v = buf[sidx<true>(r * n + slot[q])];
-                    const double D = dbuf[(size_t)r * mzp + kzs[q]];
+                    const double D = dbuf[(size_t)r * mzs + kzs[q]];
                     const double rD = __drcp_rn(D);  // off the recurrence's chain
                     if (y == 0) {
                         v.x = div_by_recip(v.x, D, rD);
@@ -156,7 +166,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
         __syncthreads();
         const int s = j % NS, c = nch - 1 - j, y0 = c * yb, nr = min(yb, ny - y0);
         double2* buf = ring + sidx<true>(s * yb * n);
-        const double* dbuf = dring + (size_t)s * yb * mzp;
+        const double* dbuf = dring + (size_t)s * yb * mzs;
         for (int r = nr - 1; r >= 0; r--) {
             const int y = y0 + r;
 #pragma unroll
@@ -167,7 +177,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
                     if (y == ny - 1) {
                         prev[q] = d;
                     } else {
-                        const double C = dbuf[(size_t)r * mzp + kzs[q]];  // c_y / D_y
+                        const double C = dbuf[(size_t)r * mzs + kzs[q]];  // c_y / D_y
                         prev[q].x = __dsub_rn(d.x, __dmul_rn(prev[q].x, C));
                         prev[q].y = __dsub_rn(d.y, __dmul_rn(prev[q].y, C));
                     }
@@ -186,7 +196,7 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
 }
 
 size_t zline_smem(int n, int mzp, int yb, int ns) {
-    return (size_t)padded_len(ns * yb * n, true) * sizeof(double2) + (size_t)ns * yb * mzp * sizeof(double);
+    return (size_t)padded_len(ns * yb * n, true) * sizeof(double2) + (size_t)ns * yb * zl_mzs(mzp) * sizeof(double);
 }
 
 template <class PL, int NS, int LPT>
