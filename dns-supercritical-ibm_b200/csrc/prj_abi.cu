@@ -161,8 +161,8 @@ int make_slot_table(int n, int** d_out, size_t* bytes) {
 // z-direction kernel choice: PRJ_ZSOLVE=split|fused|basic|line (split and line need the
 // in-place plan).  By default the per-wavenumber kernel when there are at least two x
 // wavenumbers (its CTAs) per SM, else the split kernels: measured on B200, the
-// per-wavenumber kernel took 1.35 / 1.50 / 7.87 ms against 1.40 / 1.60 / 8.67 ms for
-// nx/2+1 = 385 / 513 / 769, but 0.39 / 0.57 ms against 0.26 / 0.44 ms for 193 / 257.
+// per-wavenumber kernel took 1.12 / 1.41 / 6.91 ms against 1.31 / 1.49 / 7.87 ms for
+// nx/2+1 = 385 / 513 / 769, but 0.30 / 0.45 ms against 0.21 / 0.37 ms for 193 / 257.
 int z_mode(bool split_ok, bool line_pref) {
     const char* v = getenv("PRJ_ZSOLVE");
     if (v && !strcmp(v, "fused")) return 1;
