@@ -11,7 +11,9 @@
 // y comes from __drcp_rn; when it is formed off a recurrence's critical path (D does
 // not depend on the previous step), the dependent work per step is one multiply, two
 // fused multiply-adds and a select.  prj_selftest_division compares it with __ddiv_rn
-// bit for bit, signed zero numerators and negative divisors included.
+// bit for bit, signed zero numerators and negative divisors included.  The divisors here
+// are Thomas pivots, which plan creation requires to be nonzero and finite (a zero D would
+// give NaN where IEEE division gives an infinity; the step's NaN check reports either).
 #pragma once
 
 namespace prj {
