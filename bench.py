@@ -27,7 +27,8 @@ the whole step at 88 B per point.
 
 --impl reference times the CPU restatement of the reference's FFTW path
 (oracle/, all host threads) on the same workload, per step a bounded sample
-(768 x ny_s x 384, ny_s chosen so the run ends within a few minutes).
+(768 x ny_s x 384, ny_s chosen so that the warm-up and timed steps together take about
+--ref-budget-s seconds, 100 by default).
 """
 from __future__ import annotations
 
@@ -173,7 +174,7 @@ def run_reference(args, rank):
     t0 = time.perf_counter()
     C.projection(Uh, Vh, Wh, dx, dz, 1.0, yu, "consistent", nthreads=cores)
     per_pt = (time.perf_counter() - t0) / (NX * probe_ny * NZ)
-    budget = 100.0
+    budget = args.ref_budget_s
     nsteps = args.steps + args.warmup
     ny_s = int(budget / max(nsteps, 1) / (per_pt * NX * NZ))
     ny_s = max(8, min(NY, ny_s - ny_s % 2))
@@ -482,6 +483,8 @@ def main():
     ap.add_argument("--served-rate", type=float, default=2000.0)
     ap.add_argument("--served-budget-gb", type=float, default=150.0)
     ap.add_argument("--rough-grid", default="1536x512x768", help="rough-wall leg nx x ny x nz ('' skips it)")
+    ap.add_argument("--ref-budget-s", type=float, default=100.0,
+                    help="reference arm: host seconds for its warm-up and timed steps together")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
