@@ -165,3 +165,39 @@ def test_pipelined_host_steps_match_sync(cuda_device):
             plan.projection_step(Uh, Vh, Wh, *want, 0.8, stats=False)
             for a, b in zip(o, want):
                 np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+def test_staged_x_forward_matches_oracle(cuda_device, oracle, monkeypatch, threads):
+    """PRJ_X_STAGED selects the persistent divergence x kernel (k_fwd_xs) whose halo'd rows
+    arrive by bulk copies on mbarriers with bounded waits: same step as the oracle."""
+    import prj
+    import workloads
+    monkeypatch.setenv("PRJ_X_STAGED", str(threads))
+    nx, ny, nz = 128, 96, 64
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=6)
+    wall = (0.01, 0.0, -0.02, 0.03, 0.0, 0.04)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        U, V, W, P, st = run_engine(plan, Uh, Vh, Wh, 0.5, wall)
+    Uo, Vo, Wo, Po = oracle.projection(Uh, Vh, Wh, dx, dz, 0.5, yu, "consistent", wall)
+    assert rel_l2(P, Po) <= 1e-12
+    for a, b in ((U, Uo), (V, Vo), (W, Wo)):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+    assert st["div_maxabs"] <= 1e-10
+
+
+@pytest.mark.parametrize("shape", [(64, 48, 32), (30, 17, 21)])
+def test_basic_z_kernel_matches_oracle(cuda_device, oracle, monkeypatch, shape):
+    """PRJ_ZSOLVE=basic selects the first, unpipelined per-wavenumber z kernel."""
+    import prj
+    import workloads
+    monkeypatch.setenv("PRJ_ZSOLVE", "basic")
+    nx, ny, nz = shape
+    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=7)
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        assert plan.tuning["z_mode"] == 2
+        U, V, W, P, st = run_engine(plan, Uh, Vh, Wh, 0.5)
+    Uo, Vo, Wo, Po = oracle.projection(Uh, Vh, Wh, dx, dz, 0.5, yu, "consistent")
+    assert rel_l2(P, Po) <= 1e-12
+    for a, b in ((U, Uo), (V, Vo), (W, Wo)):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
