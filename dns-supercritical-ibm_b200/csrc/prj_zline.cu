@@ -65,7 +65,27 @@ __host__ __device__ constexpr int zl_minb(int nt) { return nt <= 64 ? 8 : nt <= 
 // 8 groups apart would put on one bank pair (n = 384: 129 -> 68 wavefronts per plane for
 // the CTA's pivot reads, against 24 conflict-free).
 __host__ __device__ constexpr int zl_mzs(int mzp) { return (mzp + 15) & ~15; }
-__device__ __forceinline__ int zl_piece(int j) { return (j & ~7) | ((j ^ (j >> 3)) & 7); }
+__host__ __device__ constexpr int zl_piece(int j) { return (j & ~7) | ((j ^ (j >> 3)) & 7); }
+
+// For a z length n (mzp = nz/2 + 1 rounded up to even, as the plan sets it): the copied
+// pieces land on distinct pieces inside the padded row, and every folded wavenumber a
+// thread reads lies in a copied piece.  Checked at compile time for every pass-plan length.
+constexpr bool zl_layout_ok(int n) {
+    const int mzp = (n / 2 + 2) / 2 * 2, mzs = zl_mzs(mzp), hp = mzp / 2;
+    bool used[1024] = {};
+    if (mzs / 2 > 1024) return false;
+    for (int j = 0; j < hp; j++) {
+        const int p = zl_piece(j);
+        if (p < 0 || p >= mzs / 2 || used[p]) return false;
+        used[p] = true;
+    }
+    for (int kf = 0; kf <= n / 2; kf++)
+        if ((kf >> 1) >= hp || 2 * zl_piece(kf >> 1) + (kf & 1) >= mzs) return false;
+    return true;
+}
+#define PRJ_ZL_LAYOUT_CHECK(N, ...) static_assert(zl_layout_ok(N), "pivot stage layout of length " #N);
+PRJ_PASS_PLANS(PRJ_ZL_LAYOUT_CHECK)
+#undef PRJ_ZL_LAYOUT_CHECK
 
 template <class PL, int NS, int LPT>
 __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL::n, LPT))) k_zline(const ZLineArgs a) {
