@@ -204,16 +204,47 @@ def run_reference(args, rank):
 
 # ----------------------------------------------------------------------------- engine arm
 def cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz):
-    """Time the oracle projection once on the bench workload (host copies of the inputs)."""
+    """Time the oracle projection once on the bench workload (host copies of the inputs).
+    Returns the baseline record and the oracle's (U, V, W, P), the parity check of the
+    engine's step on the same input."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     C = pyoracle.COracle()
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    C.projection(Uh_h, Vh_h, Wh_h, dx, dz, 1.0, yu, "consistent", nthreads=cores)
+    out = C.projection(Uh_h, Vh_h, Wh_h, dx, dz, 1.0, yu, "consistent", nthreads=cores)
     dt = time.perf_counter() - t0
     return {"value": NX * NY * NZ / dt / 1e9, "unit": "Gpts/s", "cores": cores, "kind": "port",
-            "sample": f"one full {NX}x{NY}x{NZ} projection step ({dt:.2f} s)"}
+            "sample": f"one full {NX}x{NY}x{NZ} projection step ({dt:.2f} s)"}, out
+
+
+def parity_vs_oracle(dev_out, oracle_out):
+    """rel-L2 of P and max |u - u_oracle| / max |u_oracle| over U, V, W: the engine's device
+    tensors ([y, z, x] memory) against the oracle's Fortran-ordered [x, z, y] arrays."""
+    import numpy as np
+    U, V, W, P = (t.cpu().numpy() for t in dev_out)
+    Uo, Vo, Wo, Po = (a.T for a in oracle_out)
+    p_rel = float(np.linalg.norm((P - Po).ravel()) / np.linalg.norm(Po.ravel()))
+    u_rel = max(float(np.abs(a - b).max()) / float(np.abs(b).max()) for a, b in ((U, Uo), (V, Vo), (W, Wo)))
+    return {"p_rel_l2_vs_oracle": p_rel, "u_maxabs_vs_oracle": u_rel}
+
+
+def parity_reference_bands(Uh, Vh, Wh, Uh_h, Vh_h, Wh_h, yu, dx, dz, device, stream):
+    """The same step with the reference's own bands (mk_P_abc), the parity mode, against the
+    oracle with the same bands (outside every timed region)."""
+    import torch
+    import prj
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    out = [torch.empty_like(Uh) for _ in range(3)] + [torch.empty((NY, NZ, NX), dtype=torch.float64, device=device)]
+    with prj.Plan.from_yu(NX, NZ, dx, dz, yu, "reference", device=device.index or 0) as plan:
+        plan.projection_step(Uh, Vh, Wh, *out, 1.0, stats=False, stream=stream)
+        torch.cuda.synchronize()
+    ref = pyoracle.COracle().projection(Uh_h, Vh_h, Wh_h, dx, dz, 1.0, yu, "reference", nthreads=os.cpu_count() or 1)
+    res = parity_vs_oracle(out, ref)
+    del out, ref
+    torch.cuda.empty_cache()
+    return res
 
 
 # ----------------------------------------------------------------------------- extra legs
@@ -618,8 +649,14 @@ def main():
     launches = launches_per_step * args.steps
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz)
+        cpu, orc = cpu_baseline_engine_workload(Uh_h, Vh_h, Wh_h, yu, dx, dz)
+        if mode == prj.MODE_FP64:  # U, V, W, P still hold the accuracy step's outputs
+            parity = {"consistent_bands": parity_vs_oracle((U, V, W, P), orc)}
+            parity["reference_bands"] = parity_reference_bands(Uh, Vh, Wh, Uh_h, Vh_h, Wh_h, yu, dx, dz, device,
+                                                               stream)
+        del orc
 
     extra = {}
     if not args.no_extra:
@@ -681,7 +718,8 @@ def main():
             "schedule": schedule,
             "stage_share": {k: v[0] / sum(x[0] for x in stages.values()) for k, v in stages.items()},
             "gpu_launches": launches,
-            "accuracy": {"div_maxabs": st["div_maxabs"], "p_maxabs": st["p_maxabs"], "min_pivot": st["min_pivot"]},
+            "accuracy": {"div_maxabs": st["div_maxabs"], "p_maxabs": st["p_maxabs"], "min_pivot": st["min_pivot"],
+                         **(parity["consistent_bands"] if parity else {}), "vs_oracle": parity},
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,

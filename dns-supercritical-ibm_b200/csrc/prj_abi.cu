@@ -761,6 +761,20 @@ int prj_plan_min_pivot(const prj_plan* plan, double* out) {
     return PRJ_OK;
 }
 
+int prj_plan_check_error(prj_plan* plan, void* stream) {
+    int rc = check_plan(plan);
+    if (rc) return rc;
+    DeviceGuard dg(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int* word = reinterpret_cast<int*>(plan->stat_buf + prj::kStatErrSlot);
+    int dev_err = 0;
+    CK(cudaMemcpyAsync(&dev_err, word, sizeof(int), cudaMemcpyDeviceToHost, st), "error word copy");
+    CK(cudaMemsetAsync(word, 0, sizeof(int), st), "error word reset");
+    CK(cudaStreamSynchronize(st), "error word sync");
+    if (dev_err) return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
+    return PRJ_OK;
+}
+
 int prj_plan_device_bytes(const prj_plan* plan, size_t* out) {
     if (!plan || !out) return fail(PRJ_ERR_ARG, "NULL argument");
     *out = plan->device_bytes + plan->host_stage_elems * sizeof(double);
@@ -955,7 +969,10 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
         CK(cudaStreamSynchronize(st), "stats sync");
         int dev_err = 0;
         std::memcpy(&dev_err, &h[prj::kStatErrSlot - 2], sizeof(int));
-        if (dev_err) return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
+        if (dev_err) {  // reported once: the word is cleared for the next check
+            cudaMemsetAsync(plan->stat_buf + prj::kStatErrSlot, 0, sizeof(int), st);
+            return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
+        }
         if (stats) {
             stats->div_maxabs = h[0];
             stats->p_maxabs = h[1];
@@ -1067,7 +1084,10 @@ int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_V
         CK(cudaStreamSynchronize(st), "stats sync");
         int dev_err = 0;
         std::memcpy(&dev_err, &h[prj::kStatErrSlot - 2], sizeof(int));
-        if (dev_err) return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
+        if (dev_err) {  // reported once: the word is cleared for the next check
+            cudaMemsetAsync(plan->stat_buf + prj::kStatErrSlot, 0, sizeof(int), st);
+            return fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait gave up (code %d)", dev_err);
+        }
         unsigned long long ord = 0;
         std::memcpy(&ord, &h[prj::kStatRhoSlot - 2], sizeof(ord));
         const double rmin = prj::vd_rho_min_host(ord);

@@ -222,9 +222,20 @@ extern "C" int prj_poisson_fp64_noalloc(int nx, int nz, int ny, double dx, doubl
         return na_fail(PRJ_ERR_CUDA, "pivot table: %s", cudaGetErrorString(e));
     if (!(minpiv > 0) || !std::isfinite(minpiv))
         return na_fail(PRJ_ERR_NUMERIC, "zero or non-finite Thomas pivot (min_abs_div_bacp = %g)", minpiv);
+    // the error word of the bounded device waits (the z kernel's copy pipeline): cleared
+    // here, because the array keeps whatever the previous call left, and read back below
+    int* err_word = reinterpret_cast<int*>(pl.stat_buf + prj::kStatErrSlot);
+    if ((e = cudaMemsetAsync(err_word, 0, sizeof(int), st)) != cudaSuccess)
+        return na_fail(PRJ_ERR_CUDA, "error word: %s", cudaGetErrorString(e));
     if ((e = prj::launch_fwd_x(&pl, prj::FwdSource::Pressure, d_P, nullptr, nullptr, nullptr, nullptr, st)) != cudaSuccess ||
-        (e = prj::launch_zsolve(&pl, st)) != cudaSuccess || (e = prj::launch_bwd_x(&pl, d_P, st)) != cudaSuccess ||
+        (e = prj::launch_zsolve(&pl, st)) != cudaSuccess || (e = prj::launch_bwd_x(&pl, d_P, st)) != cudaSuccess)
+        return na_fail(PRJ_ERR_CUDA, "solve: %s", cudaGetErrorString(e));
+    int dev_err = 0;
+    if ((e = cudaMemcpyAsync(&dev_err, err_word, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return na_fail(PRJ_ERR_CUDA, "solve: %s", cudaGetErrorString(e));
+    if (dev_err)
+        return na_fail(PRJ_ERR_TIMEOUT, "a bounded device-side wait of the z solve gave up (code %d); P is not solved",
+                       dev_err);
     return PRJ_OK;
 }

@@ -57,7 +57,8 @@ EXPORTS = (
     "prj_field_write_device", "prj_rough_force", "prj_ibm_interp", "prj_plan_schedule",
     "prj_projection_step_host_async", "prj_host_async_wait", "prj_selftest_wait_timeout",
     "prj_dist_forward", "prj_dist_pack", "prj_dist_thomas", "prj_dist_unpack", "prj_dist_inverse",
-    "prj_dist_divergence", "prj_dist_correct", "prj_selftest_division",
+    "prj_dist_divergence", "prj_dist_correct", "prj_selftest_division", "prj_plan_check_error",
+    "prj_geom_read_column", "prj_geom_read_bands", "prj_geom_read_metrics", "prj_geom_read_base_params",
 )
 
 BANDS_REFERENCE = 0
@@ -94,6 +95,18 @@ class VdFields(ctypes.Structure):
 
 class RoughInds(ctypes.Structure):
     _fields_ = [(f"{c}_{w}", ctypes.c_void_p) for c in "UVW" for w in ("bot", "top")]
+
+
+class CaseParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int), ("ny", ctypes.c_int), ("use_rough_surf", ctypes.c_int),
+                ("nstep", ctypes.c_longlong), ("dtmax", ctypes.c_double), ("dx", ctypes.c_double),
+                ("dz", ctypes.c_double),
+                ("wall_U_bot", ctypes.c_double), ("wall_V_bot", ctypes.c_double), ("wall_W_bot", ctypes.c_double),
+                ("wall_U_top", ctypes.c_double), ("wall_V_top", ctypes.c_double), ("wall_W_top", ctypes.c_double),
+                ("use_incompressible", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class StepParams(ctypes.Structure):
@@ -134,6 +147,11 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_projection_step_host.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.POINTER(StepParams), i,
                                            ctypes.POINTER(Stats)]
     L.prj_plan_min_pivot.argtypes = [_vp, _dp]
+    L.prj_plan_check_error.argtypes = [_vp, _vp]
+    L.prj_geom_read_column.argtypes = [ctypes.c_char_p, i, i, i, _dp]
+    L.prj_geom_read_bands.argtypes = [ctypes.c_char_p, i, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.prj_geom_read_metrics.argtypes = [ctypes.c_char_p, i, _dp, _dp, _dp]
+    L.prj_geom_read_base_params.argtypes = [ctypes.c_char_p, ctypes.POINTER(CaseParams)]
     L.prj_plan_device_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_size_t)]
     L.prj_bands_from_yu.argtypes = [i, _dp, i, _dp, _dp, _dp, _dp, _dp, _dp]
     L.prj_metrics_from_yu.argtypes = [i, _dp, _dp, _dp, _dp]
@@ -248,6 +266,22 @@ def metrics(yu):
     return tuple(out)
 
 
+def read_geom(geom_dir):
+    """A reference case's geometry folder (geom_data written by calc_bands.py): the
+    base_params.txt records of this path, the six band arrays and the three metrics
+    (prj_geom_read_*; host-only)."""
+    L = load_library()
+    enc = os.fsencode(geom_dir)
+    cp = CaseParams()
+    _check(L.prj_geom_read_base_params(os.path.join(enc, b"base_params.txt"), ctypes.byref(cp)))
+    ny = cp.ny
+    b6 = [np.zeros(ny) for _ in range(6)]
+    m3 = [np.zeros(ny) for _ in range(3)]
+    _check(L.prj_geom_read_bands(enc, ny, *[_p(v) for v in b6]))
+    _check(L.prj_geom_read_metrics(enc, ny, *[_p(v) for v in m3]))
+    return {"params": cp.as_dict(), "bands": tuple(b6), "metrics": tuple(m3)}
+
+
 @dataclass
 class Grid:
     nx: int
@@ -278,6 +312,16 @@ class Plan:
         yu = np.asarray(yu, dtype=np.float64)
         plan = cls(nx, nz, len(yu) - 1, dx, dz, bands(yu, band_mode), metrics(yu), device)
         plan.set_vd_metric(vd_metric(yu))
+        return plan
+
+    @classmethod
+    def from_geom(cls, geom_dir, device=0):
+        """A plan for a reference case's geometry folder (base_params.txt, P_band_abc(_00).dat,
+        inv_dy_p.dat, dPdy_ddy_lh.dat); ``plan.case`` holds its base parameters."""
+        geo = read_geom(geom_dir)
+        c = geo["params"]
+        plan = cls(c["nx"], c["nz"], c["ny"], c["dx"], c["dz"], geo["bands"], geo["metrics"], device)
+        plan.case = c
         return plan
 
     def projection_step_host_async(self, Uh, Vh, Wh, U, V, W, P, dt, mode=MODE_FP64, wall=(0.0,) * 6):
@@ -343,6 +387,11 @@ class Plan:
         v = ctypes.c_double()
         _check(load_library().prj_plan_min_pivot(self.handle, ctypes.byref(v)))
         return v.value
+
+    def check_error(self, stream=None):
+        """Raise PrjError(PRJ_ERR_TIMEOUT) if a bounded device-side wait gave up since the last
+        check (prj_plan_check_error; waits for the stream and clears the word)."""
+        _check(load_library().prj_plan_check_error(self.handle, _stream_ptr(stream)))
 
     @property
     def device_bytes(self) -> int:

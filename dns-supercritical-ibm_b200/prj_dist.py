@@ -155,22 +155,32 @@ def nccl_exchange(dist, stream=None):
     return ex
 
 
-def nccl_plane_exchange(dist, rank: int, world: int):
+def nccl_plane_exchange(dist, rank: int, world: int, stream=None):
     """The neighbour exchange of ``DistSolve.project``: rank r sends its last P plane to
-    rank r+1 and receives plane y0-1 from rank r-1 (point-to-point over the process group)."""
+    rank r+1 and receives plane y0-1 from rank r-1 (point-to-point over the process group).
+    For CUDA tensors the sends, receives and the copy into ``P_ext[0]`` are ordered on
+    ``stream`` (the current stream if None), the stream the inverse transform wrote P on
+    and the correction reads it on."""
+    import contextlib
+
     def ex(P_ext):
-        ops = []
-        if rank + 1 < world:
-            ops.append(dist.P2POp(dist.isend, P_ext[-1].contiguous(), rank + 1))
-        recv = None
-        if rank > 0:
-            recv = P_ext[0].new_empty(P_ext[0].shape)
-            ops.append(dist.P2POp(dist.irecv, recv, rank - 1))
-        if ops:
-            for w in dist.batch_isend_irecv(ops):
-                w.wait()
-        if recv is not None:
-            P_ext[0].copy_(recv)
+        ctx = contextlib.nullcontext()
+        if P_ext.is_cuda:
+            import torch
+            ctx = torch.cuda.stream(stream or torch.cuda.current_stream(P_ext.device))
+        with ctx:
+            ops = []
+            if rank + 1 < world:
+                ops.append(dist.P2POp(dist.isend, P_ext[-1].contiguous(), rank + 1))
+            recv = None
+            if rank > 0:
+                recv = P_ext[0].new_empty(P_ext[0].shape)
+                ops.append(dist.P2POp(dist.irecv, recv, rank - 1))
+            if ops:
+                for w in dist.batch_isend_irecv(ops):
+                    w.wait()
+            if recv is not None:
+                P_ext[0].copy_(recv)
     return ex
 
 

@@ -236,6 +236,39 @@ int prj_field_read_device(const char* path, int nx, int nz, int ny, double* d_ds
 int prj_field_write_device(const char* path, int nx, int nz, int ny, const double* d_src, int halo, int device);
 
 /*
+ * Geometry folder of a reference case (the geom_data files that
+ * src/pycode/calc_bands.py writes, calc_bands.py:358-364: first line the row
+ * count, then one row of space-separated values per line).  Host only.
+ *
+ * prj_geom_read_column: read_column_r8 (src/mod_utils.f90:14-35): rows
+ *   n_prev .. n_prev+n-1 of column icol (0..3) into out[0..n-1]; PRJ_ERR_ARG when
+ *   that range runs past the row count (the reference stops there).
+ * prj_geom_read_bands: P_band_a/b/c from P_band_abc.dat and the pinned-mode bands
+ *   from P_band_abc_00.dat, rows 0..ny-1 (src/inc_set_alloc_arrays.f90:54-59),
+ *   the band_* arguments of prj_plan_create.
+ * prj_geom_read_metrics: inv_dy_p (inv_dy_p.dat) and dPdy_ddy_lo/hi (columns 0
+ *   and 1 of dPdy_ddy_lh.dat), rows 0..ny-1 (inc_set_alloc_arrays.f90:51-53, :61).
+ * prj_geom_read_base_params: the records of base_params.txt this path needs
+ *   (src/inc_set_read_params.f90:14-40): the grid, nstep, dtmax, dx, dz, the
+ *   rough-surface flag, the wall values of U, V, W and use_incompressible.
+ */
+typedef struct prj_case_params {
+    int nx, nz, ny;
+    int use_rough_surf;
+    long long nstep;
+    double dtmax;
+    double dx, dz;
+    double wall_U_bot, wall_V_bot, wall_W_bot;
+    double wall_U_top, wall_V_top, wall_W_top;
+    int use_incompressible;
+} prj_case_params;
+int prj_geom_read_column(const char* path, int icol, int n, int n_prev, double* out);
+int prj_geom_read_bands(const char* geom_dir, int ny, double* band_a, double* band_b, double* band_c,
+                        double* band_a00, double* band_b00, double* band_c00);
+int prj_geom_read_metrics(const char* geom_dir, int ny, double* inv_dy_p, double* dPdy_lo, double* dPdy_hi);
+int prj_geom_read_base_params(const char* path, prj_case_params* out);
+
+/*
  * Batched solves: one CUDA graph holding every case (case i solves plans[i] in
  * place on the device array d_P[i], FP64 or PRJ_MODE_FP32_REFINE), the cases
  * on parallel graph branches, replayed by one graph launch.  The plans must be
@@ -349,9 +382,13 @@ const char* prj_stage_name(int stage);
  * 256 x 128 x 128 fits).
  * The first call on a device resolves the array's address on that device
  * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Calls share the array: the function is synchronous on `stream` and
- * serialises its callers with a process lock; work that overlapped on the
- * GPU with another user of the array would race.
+ * The function is synchronous: before it returns it waits for `stream` and
+ * reads back the minimum pivot and the error word of the z solve's bounded
+ * device waits (PRJ_ERR_TIMEOUT when one gave up; P is then not solved).
+ * Calls share the array and each finds what the previous one left, so every
+ * region it reads, the error word included, is re-initialised first; calls are
+ * serialised with a process lock, and work that overlapped on the GPU with
+ * another user of the array would race.
  */
 #define PRJ_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int prj_poisson_fp64_noalloc(int nx, int nz, int ny, double dx, double dz,
@@ -404,6 +441,15 @@ int prj_dist_divergence(prj_plan* plan, const double* d_Uh_loc, const double* d_
 int prj_dist_correct(prj_plan* plan, const double* d_P_ext, const double* d_Uh_loc, const double* d_Vh_loc,
                      const double* d_Wh_loc, double* d_U_loc, double* d_V_loc, double* d_W_loc, int y0, int y1,
                      const prj_step_params* params, void* stream);
+
+/* Device error word of the plan's bounded device-side waits (the pipelined z
+ * kernel used for z lengths with a prime factor above 5, and the diagnostics).
+ * The asynchronous solves cannot report a wait that gave up when they return;
+ * this call waits for `stream`, reads the word, clears it, and returns
+ * PRJ_ERR_TIMEOUT if any wait gave up since the last check (the results of
+ * that work are then not valid), else PRJ_OK.  prj_projection_step with
+ * statistics performs the same check. */
+int prj_plan_check_error(prj_plan* plan, void* stream);
 
 /* Message of the calling thread's last failure ("" if none). */
 const char* prj_last_error_string(void);

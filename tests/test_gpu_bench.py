@@ -1,5 +1,6 @@
 """bench.py's engine arm on a small grid: one JSON line with every key of the contract
-(roofline, e2e through the host-buffer call, clocks, launch count)."""
+(roofline, e2e through the host-buffer call, clocks, launch count, the CPU baseline and
+the parity of the measured step against the oracle in both band modes)."""
 import json
 import os
 import subprocess
@@ -15,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_engine_arm_prints_the_contract_line(cuda_device):
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "4", "--warmup", "3",
-                        "--no-extra", "--e2e-steps", "1", "--no-cpu-baseline", "--grid", "128x96x64",
+                        "--no-extra", "--e2e-steps", "1", "--grid", "128x96x64",
                         "--rough-grid", ""], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
@@ -36,3 +37,10 @@ def test_engine_arm_prints_the_contract_line(cuda_device):
     assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] == 3 * 8 * nh
     assert e2e["d2h_bytes_per_step"] == 3 * 8 * nh + 8 * 128 * 96 * 64
     assert "sm_mhz" in j["clocks"] and "reasons" in j["clocks"]
+    cpu = j["cpu_baseline"]
+    assert cpu["value"] > 0 and cpu["kind"] == "port" and cpu["cores"] >= 1
+    acc = j["accuracy"]
+    assert acc["p_rel_l2_vs_oracle"] <= 1e-12 and acc["u_maxabs_vs_oracle"] <= 1e-12
+    for mode in ("consistent_bands", "reference_bands"):
+        rec = acc["vs_oracle"][mode]
+        assert rec["p_rel_l2_vs_oracle"] <= 1e-12 and rec["u_maxabs_vs_oracle"] <= 1e-12, (mode, rec)

@@ -3,11 +3,12 @@ cannot allocate device memory (for example a Fortran/OpenACC host program that
 owns every device array, or a time loop that must not call cudaMalloc).
 
 It calls the entry point through the C ABI and compares each result with the
-planned entry point (prj_plan_create + prj_poisson_fp64) on the same input,
-within the FP64 tolerance of the other parity tests, on several calls in a row
-of different sizes (the calls share one static scratch array, so each call
-must start from a clean state).  It also checks that a grid too large for the
-scratch array is refused with a clear message and leaves P untouched.
+planned entry point (prj_plan_create + prj_poisson_fp64) and with the CPU
+oracle on the same input, within the FP64 tolerance of the other parity tests,
+on several calls in a row of different sizes (the calls share one static
+scratch array, so each call must start from a clean state, its device error
+word included).  It also checks that a grid too large for the scratch array is
+refused with a clear message and leaves P untouched.
 
 This file is collected last on purpose.
 """
@@ -54,7 +55,7 @@ def _case(shape, seed, mode):
     return rhs, prj.bands(yu, mode), dx, dz
 
 
-def test_noalloc_matches_planned_solve(cuda_device):
+def test_noalloc_matches_planned_solve(cuda_device, oracle):
     import prj
     import torch
     lib = prj.load_library()
@@ -70,6 +71,8 @@ def test_noalloc_matches_planned_solve(cuda_device):
         got = from_dev(t)
         assert np.isfinite(got).all()
         assert rel_l2(got, want) <= TOL_REL, (shape, rel_l2(got, want))
+        Po, _ = oracle.poisson(rhs, dx, dz, b6)
+        assert rel_l2(got, Po) <= TOL_REL, (shape, rel_l2(got, Po))
 
 
 def test_noalloc_rejects_grid_beyond_scratch(cuda_device):
