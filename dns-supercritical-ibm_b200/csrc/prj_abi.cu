@@ -165,6 +165,7 @@ int make_slot_table(int n, int** d_out, size_t* bytes) {
 // nx/2+1 = 385 / 513 / 769, but 0.30 / 0.45 ms against 0.21 / 0.37 ms for 193 / 257.
 int z_mode(bool split_ok, bool line_pref) {
     const char* v = getenv("PRJ_ZSOLVE");
+    if (v && !strcmp(v, "cluster")) return split_ok ? 4 : 1;
     if (v && !strcmp(v, "fused")) return 1;
     if (v && !strcmp(v, "basic")) return 2;
     if (v && !strcmp(v, "line")) return split_ok ? 3 : 1;
@@ -189,6 +190,9 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->zd.tw);
     dfree(pl->zd.pos);
     dfree(pl->kz_of_slot);
+    dfree(pl->zcl_dcls);
+    dfree(pl->zcl_ccls);
+    dfree(pl->zcl_pos);
     dfree(pl->spec32);
     dfree(pl->pbar);
     dfree(pl->psum);
@@ -414,7 +418,7 @@ int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const doub
 }
 
 int mixed_supported(const prj_plan* pl) {
-    if ((pl->zmode != 0 && pl->zmode != 3) || !pl->xd.ok)
+    if ((pl->zmode != 0 && pl->zmode != 3 && pl->zmode != 4) || !pl->xd.ok)
         return fail(PRJ_ERR_UNSUPPORTED, "the mixed-precision path needs in-place plans for nx/2 and nz (radices 2, 3, 4, 5, 8)");
     return PRJ_OK;
 }
@@ -437,7 +441,15 @@ int run_mixed_poisson(prj_plan* pl, double* P, cudaStream_t st) {
 
 // z transforms + Thomas: three kernels (split) or one fused kernel
 int run_zsolve(prj_plan* pl, cudaStream_t st) {
-    if (pl->zmode == 3) {
+    if (pl->zmode == 4) {
+        StageTimer tm(pl, prj::kStZSolve, st);
+        const cudaError_t e = prj::launch_zcl(pl, st);
+        if (e != cudaErrorNotSupported) {
+            CK(e, "z transform + Thomas (cluster kernel)");
+            return PRJ_OK;
+        }
+    }
+    if (pl->zmode == 3 || pl->zmode == 4) {
         StageTimer tm(pl, prj::kStZSolve, st);
         const cudaError_t e = prj::launch_zline(pl, st);
         if (e != cudaErrorNotSupported) {
@@ -445,7 +457,7 @@ int run_zsolve(prj_plan* pl, cudaStream_t st) {
             return PRJ_OK;
         }
     }
-    if (pl->zmode == 0 || pl->zmode == 3) {
+    if (pl->zmode == 0 || pl->zmode == 3 || pl->zmode == 4) {
         {
             StageTimer tm(pl, prj::kStZfftFwd, st);
             CK(prj::launch_zfft(pl, -1, st), "z transform");
@@ -741,6 +753,17 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if (!(mp > 0) || !std::isfinite(mp))
         return bail(fail(PRJ_ERR_NUMERIC, "zero or non-finite Thomas pivot (min_abs_div_bacp = %g)", mp));
     pl->device_bytes = bytes;
+    {
+        const char* yb = getenv("PRJ_ZCL_YB");
+        const char* ns = getenv("PRJ_ZCL_NS");
+        pl->zcl_yb = yb ? atoi(yb) : 0;
+        pl->zcl_ns = ns ? atoi(ns) : 0;
+    }
+    if (pl->zmode == 4) {
+        if (!prj::zcl_supported(pl)) pl->zmode = 3;
+        else if ((e = prj::zcl_prepare(pl, 0)) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess)
+            return bail(cuda_fail(e, "cluster z kernel tables"));
+    }
     *out = pl;
     return PRJ_OK;
 }
@@ -1228,7 +1251,10 @@ int prj_plan_schedule(const prj_plan* plan, int mode, int* launches, int* chunks
     *chunks = ov ? plan->overlap_chunks : 0;
     if (ov) *launches = 5 * plan->overlap_chunks + 1;
     else if (mode == PRJ_MODE_FP64)
-        *launches = (plan->zmode == 0 || (plan->zmode == 3 && !prj::zline_supported(plan))) ? 6 : 4;
+        *launches = (plan->zmode == 0 || (plan->zmode == 3 && !prj::zline_supported(plan)) ||
+                     (plan->zmode == 4 && !prj::zcl_supported(plan) && !prj::zline_supported(plan)))
+                        ? 6
+                        : 4;
     else {
         // forward x, z transforms of the FP64 and FP32 rows, one Thomas launch, inverse z of both,
         // inverse x; per refinement pass also the plane means, the residual and a norm reset;
@@ -1254,15 +1280,21 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
     auto pow2 = [](int v) { return v >= 1 && v <= 16 && (v & (v - 1)) == 0; };
     if (!pow2(t->x_rows)) return fail(PRJ_ERR_ARG, "x_rows=%d must be a power of two in [1, 16]", t->x_rows);
     if (t->z_rows != 0 && !pow2(t->z_rows)) return fail(PRJ_ERR_ARG, "z_rows=%d must be 0 or a power of two in [1, 16]", t->z_rows);
-    if (t->z_mode != 0 && t->z_mode != 1 && t->z_mode != 3)
-        return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1 or 3", t->z_mode);
-    if ((t->z_mode == 0 || t->z_mode == 3) && !(plan->zd.ok && plan->kz_of_slot))
+    if (t->z_mode != 0 && t->z_mode != 1 && t->z_mode != 3 && t->z_mode != 4)
+        return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1, 3 or 4", t->z_mode);
+    if ((t->z_mode == 0 || t->z_mode == 3 || t->z_mode == 4) && !(plan->zd.ok && plan->kz_of_slot))
         return fail(PRJ_ERR_UNSUPPORTED, "no in-place z plan for nz=%d", plan->g.nz);
     const int rs = plan->fx64.even ? plan->fx64.m + 1 : plan->fx64.m;
     if ((size_t)prj::padded_len(t->x_rows * rs, true) * sizeof(double2) + (size_t)plan->fx64.m * sizeof(int) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "x_rows=%d does not fit shared memory for nx=%d", t->x_rows, plan->g.nx);
     if (t->z_rows && (size_t)prj::padded_len(t->z_rows * plan->g.nz, true) * sizeof(double2) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "z_rows=%d does not fit shared memory for nz=%d", t->z_rows, plan->g.nz);
+    if (t->z_mode == 4 && prj::zcl_supported(plan)) {
+        DeviceGuard dg(plan->device);
+        cudaError_t e = prj::zcl_prepare(plan, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return cuda_fail(e, "cluster z kernel tables");
+    }
     plan->tz_xd = t->x_rows;
     plan->tz_xp = t->x_rows;
     plan->zfft_rows = t->z_rows;

@@ -129,6 +129,11 @@ struct prj_plan {
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
     double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
     double* vd_ih = nullptr;      // 0.5 / rho (halo'd) of the variable-density step (scratch)
+    double* zcl_dcls = nullptr;   // class tables of the pivots for the cluster z kernel (prj_zcluster.cu)
+    double* zcl_ccls = nullptr;   // class tables of the back-substitution factors
+    int* zcl_pos = nullptr;       // position of each slot's line in its class row
+    int zcl_yb = 0;               // planes per chunk of the cluster z kernel (0: default)
+    int zcl_ns = 0;               // its stages (0: default)
     int overlap_chunks = 0;       // y chunks of the overlapped projection schedule (0: sequential)
     cudaStream_t ov_st[2] = {nullptr, nullptr};  // its two helper streams (created on first use)
     std::vector<cudaEvent_t> ov_ev;              // its events
@@ -172,6 +177,12 @@ cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStrea
 // butterflies (prj_zline.cu); cudaErrorNotSupported when nz has no pass plan
 cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st);
 bool zline_supported(const prj_plan* pl);  // launch_zline would run (not fall back)
+// the same on a thread-block cluster of R_0 CTAs per x wavenumber (prj_zcluster.cu);
+// zcl_prepare builds its pivot class tables once (allocates; not under capture)
+bool zcl_supported(const prj_plan* pl);
+cudaError_t zcl_prepare(prj_plan* pl, cudaStream_t st);
+cudaError_t launch_zcl(const prj_plan* pl, cudaStream_t st);
+size_t zcl_smem(int nz, int yb, int ns);
 
 // x transforms with the in-place DIF FFT (prj_xfft.cu); used when pl->xd.ok
 // bout: also store the source field (divergence) there; accum: P += result; sq: norms of
