@@ -563,8 +563,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    launches_per_step, ov_chunks = plan.schedule(mode)
-    schedule = f"{ov_chunks} y-chunks overlapped on 3 streams" if ov_chunks else "sequential"
+    launches_per_step = plan.launches_per_step(mode)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -578,8 +577,8 @@ def main():
     ms = e0.elapsed_time(e1)
     ms_max = sharding.max_over_ranks(ms, dist, device)
     value = sharding.job_throughput(NX * NY * NZ, args.steps, world, ms_max)
-    # per-kernel CUDA-event times: a separate run with stage timing, which launches the
-    # kernels one after another on one stream (the timed run above may overlap chunks)
+    # per-kernel CUDA-event times: a separate run with stage timing (events around every
+    # kernel, which the timed run above does without)
     plan.enable_stage_timing(True)
     for _ in range(max(3, args.steps // 5)):
         step()
@@ -715,7 +714,6 @@ def main():
                               "unit": "GB/s", "frac": roof_step / peak},
             "roofline_kernels": per_kernel,
             "stages_ms_per_launch": {k: v[0] / v[1] for k, v in stages.items()},
-            "schedule": schedule,
             "stage_share": {k: v[0] / sum(x[0] for x in stages.values()) for k, v in stages.items()},
             "gpu_launches": launches,
             "accuracy": {"div_maxabs": st["div_maxabs"], "p_maxabs": st["p_maxabs"], "min_pivot": st["min_pivot"],

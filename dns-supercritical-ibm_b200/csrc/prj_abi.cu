@@ -215,12 +215,6 @@ void free_plan_buffers(prj_plan* pl) {
         if (hs) cudaStreamDestroy(hs);
         hs = nullptr;
     }
-    for (cudaEvent_t e : pl->ov_ev) cudaEventDestroy(e);
-    pl->ov_ev.clear();
-    for (cudaStream_t& s : pl->ov_st) {
-        if (s) cudaStreamDestroy(s);
-        s = nullptr;
-    }
     dfree(pl->host_stage);
     pl->host_stage_elems = 0;
 }
@@ -279,11 +273,6 @@ struct StageTimer {
     }
 };
 
-double env_double(const char* name, double dflt) {
-    const char* v = getenv(name);
-    return (v && *v) ? atof(v) : dflt;
-}
-
 // Mixed-path set-up on first use: FP64 rows are the x-wavenumbers whose lines
 // are badly conditioned, |a_x(kx)| < tau * max_k |b_k| (their condition number
 // exceeds about 1/tau; with FP32 storage their error would not contract under
@@ -296,13 +285,11 @@ int ensure_mixed(prj_plan* pl) {
     CK(cudaMemcpy(bands.data(), pl->t.bands, bands.size() * sizeof(double), cudaMemcpyDeviceToHost), "mixed set-up");
     double bmax = 0.0;
     for (int k = 0; k < g.ny; k++) bmax = std::max(bmax, std::fabs(bands[(size_t)g.ny + k]));
-    const double tau = env_double("PRJ_MIXED_TAU", 1e-3);
+    const double tau = pl->mixed_tau;
     int kxs = g.nxh;
     for (int kx = 1; kx < g.nxh; kx++)
         if (std::fabs(ax[kx]) >= tau * bmax) { kxs = kx; break; }
     pl->kxs_mixed = kxs;
-    pl->mixed_iters = (int)env_double("PRJ_MIXED_ITERS", 1);  // one pass leaves ~1e-13 (the next update measures 1e-14)
-    if (pl->mixed_iters < 0) pl->mixed_iters = 0;
     const size_t n32 = (size_t)(g.nxh - kxs) * g.nz * g.ny;
     if (n32) {
         CK(cudaMalloc((void**)&pl->spec32, n32 * sizeof(float2)), "cudaMalloc(FP32 spectrum)");
@@ -673,15 +660,6 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
         // 1..4 always with ring shape 4x4, 8x2, 2x8, 8x3 (planes x stages)
         const char* ta = getenv("PRJ_THOMAS_ASYNC");
         pl->thomas_async = ta ? atoi(ta) : -1;
-        // PRJ_OVERLAP_CHUNKS: y chunks of the overlapped projection schedule; off by default
-        // (measured on B200 at 768x384x384: 4.16 ms sequential, 4.18 / 4.27 / 4.35 ms with
-        // 2 / 4 / 8 chunks -- every kernel already fills the GPU)
-        const char* oc = getenv("PRJ_OVERLAP_CHUNKS");
-        pl->overlap_chunks = oc ? atoi(oc) : 0;
-        // PRJ_X_STAGED=128|256 selects the staged persistent x-forward kernel for the
-        // divergence source with that many threads per CTA (measured slower; off by default)
-        const char* xs = getenv("PRJ_X_STAGED");
-        pl->x_staged = xs ? atoi(xs) : 0;
     }
     pl->kxs = g.nxh;
     pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);
@@ -753,12 +731,6 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if (!(mp > 0) || !std::isfinite(mp))
         return bail(fail(PRJ_ERR_NUMERIC, "zero or non-finite Thomas pivot (min_abs_div_bacp = %g)", mp));
     pl->device_bytes = bytes;
-    {
-        const char* yb = getenv("PRJ_ZCL_YB");
-        const char* ns = getenv("PRJ_ZCL_NS");
-        pl->zcl_yb = yb ? atoi(yb) : 0;
-        pl->zcl_ns = ns ? atoi(ns) : 0;
-    }
     if (pl->zmode == 4) {
         if (!prj::zcl_supported(pl)) pl->zmode = 3;
         else if ((e = prj::zcl_prepare(pl, 0)) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess)
@@ -862,81 +834,7 @@ int prj_poisson_fp64(prj_plan* plan, double* d_P, void* stream) {
     return run_poisson(plan, d_P, (cudaStream_t)stream);
 }
 
-// Overlapped FP64 projection: the y planes split into chunks; the forward x
-// transform of chunk c+1 runs beside the forward z transform of chunk c, and the
-// inverse z transform, inverse x transform and correction of successive chunks
-// overlap on three streams (the caller's and two of the plan's).  Kernels bound by
-// different limits (load latency, shared memory, DRAM) share the SMs.  Thomas
-// couples all planes and runs alone.  The streams fork from and join back into
-// `st` with events, so the schedule is graph-capturable.  Returns -1 (nothing
-// launched) when the plan does not qualify: pass-plan x and z kernels, split z
-// direction, no stage timing, ny >= 2 chunks.
 bool x_pass_active(const prj_plan* pl);
-
-bool overlap_ok(const prj_plan* pl) {
-    int fac[8];
-    const int C = pl->overlap_chunks;
-    return C >= 2 && !pl->timing && (pl->zmode == 0 || pl->zmode == 3) && x_pass_active(pl) && pl->zd.ok && pl->kz_of_slot &&
-           prj::pass_radices(pl->g.nz, fac, 8) > 0 && pl->g.ny >= 2 * C;
-}
-
-int ensure_overlap(prj_plan* pl) {
-    const size_t need = (size_t)3 * pl->overlap_chunks + 6;
-    for (cudaStream_t& s : pl->ov_st)
-        if (!s) CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "overlap stream");
-    while (pl->ov_ev.size() < need) {
-        cudaEvent_t e;
-        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "overlap event");
-        pl->ov_ev.push_back(e);
-    }
-    return PRJ_OK;
-}
-
-int run_projection_overlapped(prj_plan* pl, const double* Uh, const double* Vh, const double* Wh, double* U,
-                              double* V, double* W, double* P, const prj::StepScalars& sc, cudaStream_t s0) {
-    int rc = ensure_overlap(pl);
-    if (rc) return rc;
-    const int C = pl->overlap_chunks, ny = pl->g.ny;
-    cudaStream_t s1 = pl->ov_st[0], s2 = pl->ov_st[1];
-    cudaEvent_t* ev = pl->ov_ev.data();
-    cudaEvent_t fork = ev[0], zdone = ev[1], tdone = ev[2], j1 = ev[3], j2 = ev[4];
-    cudaEvent_t* ef = ev + 6;
-    cudaEvent_t* ei = ef + C;
-    cudaEvent_t* eb = ei + C;
-    auto lo = [&](int c) { return (int)((long)ny * c / C); };
-    CK(cudaEventRecord(fork, s0), "fork");
-    CK(cudaStreamWaitEvent(s1, fork, 0), "fork");
-    CK(cudaStreamWaitEvent(s2, fork, 0), "fork");
-    for (int c = 0; c < C; c++) {
-        const prj::YRange yr{lo(c), lo(c + 1)};
-        CK(prj::launch_fwd_x_range(pl, Uh, Vh, Wh, &sc, s0, yr), "divergence + forward x");
-        CK(cudaEventRecord(ef[c], s0), "event");
-        CK(cudaStreamWaitEvent(s1, ef[c], 0), "event");
-        CK(prj::launch_zfft(pl, -1, s1, yr), "z transform");
-    }
-    CK(cudaEventRecord(zdone, s1), "event");
-    CK(cudaStreamWaitEvent(s0, zdone, 0), "event");
-    CK(prj::launch_thomas(pl, s0), "Thomas sweeps");
-    CK(cudaEventRecord(tdone, s0), "event");
-    CK(cudaStreamWaitEvent(s1, tdone, 0), "event");
-    for (int c = 0; c < C; c++) {
-        const prj::YRange yr{lo(c), lo(c + 1)};
-        CK(prj::launch_zfft(pl, +1, s0, yr), "inverse z transform");
-        CK(cudaEventRecord(ei[c], s0), "event");
-        CK(cudaStreamWaitEvent(s1, ei[c], 0), "event");
-        CK(prj::launch_bwd_xd(pl, P, s1, 0, nullptr, yr), "inverse x");
-        CK(cudaEventRecord(eb[c], s1), "event");
-        CK(cudaStreamWaitEvent(s2, eb[c], 0), "event");
-        // halo'd planes of the chunk, the wall planes with the first and last chunk
-        const prj::YRange kh{c == 0 ? 0 : yr.y0 + 1, c == C - 1 ? ny + 2 : yr.y1 + 1};
-        CK(prj::launch_correction(pl, P, Uh, Vh, Wh, U, V, W, sc, s2, kh), "correction");
-    }
-    CK(cudaEventRecord(j1, s1), "join");
-    CK(cudaEventRecord(j2, s2), "join");
-    CK(cudaStreamWaitEvent(s0, j1, 0), "join");
-    CK(cudaStreamWaitEvent(s0, j2, 0), "join");
-    return PRJ_OK;
-}
 
 int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, const double* d_Wh, double* d_U,
                         double* d_V, double* d_W, double* d_P, const prj_step_params* params, int mode,
@@ -958,10 +856,7 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
     sc.inv_dt = 1.0 / params->dt;
     sc.wall[0] = params->wall_U_bot; sc.wall[1] = params->wall_V_bot; sc.wall[2] = params->wall_W_bot;
     sc.wall[3] = params->wall_U_top; sc.wall[4] = params->wall_V_top; sc.wall[5] = params->wall_W_top;
-    const bool overlapped = mode == PRJ_MODE_FP64 && overlap_ok(plan);
-    if (overlapped) {
-        if ((rc = run_projection_overlapped(plan, d_Uh, d_Vh, d_Wh, d_U, d_V, d_W, d_P, sc, st))) return rc;
-    } else if (mode == PRJ_MODE_FP32_REFINE) {
+    if (mode == PRJ_MODE_FP32_REFINE) {
         const int rm = run_mixed_solve(plan, d_Uh, d_Vh, d_Wh, d_U, d_V, d_P, sc, st);
         if (rm) return rm;
     } else {
@@ -978,7 +873,7 @@ int prj_projection_step(prj_plan* plan, const double* d_Uh, const double* d_Vh, 
             CK(prj::launch_bwd_x(plan, d_P, st), "inverse x");
         }
     }
-    if (!overlapped) {
+    {
         StageTimer tm(plan, prj::kStCorrect, st);
         CK(prj::launch_correction(plan, d_P, d_Uh, d_Vh, d_Wh, d_U, d_V, d_W, sc, st), "correction");
     }
@@ -1245,17 +1140,13 @@ bool x_pass_active(const prj_plan* pl) {
     return pl->use_pass && pl->fx64.even && pl->xd.ok && prj::pass_radices(pl->fx64.m, fac, 8) > 0;
 }
 
-int prj_plan_schedule(const prj_plan* plan, int mode, int* launches, int* chunks) {
-    if (!plan || !launches || !chunks) return fail(PRJ_ERR_ARG, "NULL argument");
-    const bool ov = mode == PRJ_MODE_FP64 && overlap_ok(plan);
-    *chunks = ov ? plan->overlap_chunks : 0;
-    if (ov) *launches = 5 * plan->overlap_chunks + 1;
-    else if (mode == PRJ_MODE_FP64)
-        *launches = (plan->zmode == 0 || (plan->zmode == 3 && !prj::zline_supported(plan)) ||
-                     (plan->zmode == 4 && !prj::zcl_supported(plan) && !prj::zline_supported(plan)))
-                        ? 6
-                        : 4;
-    else {
+int prj_plan_schedule(const prj_plan* plan, int mode, int* launches) {
+    if (!plan || !launches) return fail(PRJ_ERR_ARG, "NULL argument");
+    if (mode == PRJ_MODE_FP64) {
+        const bool one_z = (plan->zmode == 1 || plan->zmode == 2) || (plan->zmode == 3 && prj::zline_supported(plan)) ||
+                           (plan->zmode == 4 && (prj::zcl_supported(plan) || prj::zline_supported(plan)));
+        *launches = one_z ? 4 : 6;
+    } else {
         // forward x, z transforms of the FP64 and FP32 rows, one Thomas launch, inverse z of both,
         // inverse x; per refinement pass also the plane means, the residual and a norm reset;
         // then the correction
@@ -1270,6 +1161,11 @@ int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out) {
     out->x_rows = x_pass_active(plan) ? plan->tz_xp : plan->tz_xd;
     out->z_rows = plan->zfft_rows;
     out->z_mode = plan->zmode;
+    out->z_planes = plan->z_planes;
+    out->z_stages = plan->z_stages;
+    out->thomas_ring = plan->thomas_async;
+    out->mixed_iters = plan->mixed_iters;
+    out->mixed_tau = plan->mixed_tau;
     return PRJ_OK;
 }
 
@@ -1280,25 +1176,49 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
     auto pow2 = [](int v) { return v >= 1 && v <= 16 && (v & (v - 1)) == 0; };
     if (!pow2(t->x_rows)) return fail(PRJ_ERR_ARG, "x_rows=%d must be a power of two in [1, 16]", t->x_rows);
     if (t->z_rows != 0 && !pow2(t->z_rows)) return fail(PRJ_ERR_ARG, "z_rows=%d must be 0 or a power of two in [1, 16]", t->z_rows);
-    if (t->z_mode != 0 && t->z_mode != 1 && t->z_mode != 3 && t->z_mode != 4)
-        return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1, 3 or 4", t->z_mode);
+    if (t->z_mode < 0 || t->z_mode > 4) return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1, 2, 3 or 4", t->z_mode);
     if ((t->z_mode == 0 || t->z_mode == 3 || t->z_mode == 4) && !(plan->zd.ok && plan->kz_of_slot))
         return fail(PRJ_ERR_UNSUPPORTED, "no in-place z plan for nz=%d", plan->g.nz);
+    if (t->z_planes < 0 || t->z_planes > 64) return fail(PRJ_ERR_ARG, "z_planes=%d must lie in [0, 64]", t->z_planes);
+    if (t->z_stages != 0 && (t->z_stages < 2 || t->z_stages > (t->z_mode == 1 ? 8 : 4)))
+        return fail(PRJ_ERR_ARG, "z_stages=%d must be 0 or in [2, %d]", t->z_stages, t->z_mode == 1 ? 8 : 4);
+    if (t->thomas_ring < -1 || t->thomas_ring > 4) return fail(PRJ_ERR_ARG, "thomas_ring=%d must lie in [-1, 4]", t->thomas_ring);
+    if (t->mixed_iters < 0 || t->mixed_iters > 8) return fail(PRJ_ERR_ARG, "mixed_iters=%d must lie in [0, 8]", t->mixed_iters);
+    if (!(t->mixed_tau > 0.0 && t->mixed_tau < 1.0)) return fail(PRJ_ERR_ARG, "mixed_tau=%g must lie in (0, 1)", t->mixed_tau);
     const int rs = plan->fx64.even ? plan->fx64.m + 1 : plan->fx64.m;
     if ((size_t)prj::padded_len(t->x_rows * rs, true) * sizeof(double2) + (size_t)plan->fx64.m * sizeof(int) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "x_rows=%d does not fit shared memory for nx=%d", t->x_rows, plan->g.nx);
     if (t->z_rows && (size_t)prj::padded_len(t->z_rows * plan->g.nz, true) * sizeof(double2) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "z_rows=%d does not fit shared memory for nz=%d", t->z_rows, plan->g.nz);
+    if (t->z_mode == 4 && t->z_planes && prj::zcl_supported(plan) &&
+        prj::zcl_smem(plan->g.nz, t->z_planes, t->z_stages ? t->z_stages : 3) > (size_t)200 * 1024)
+        return fail(PRJ_ERR_ARG, "z_planes=%d does not fit shared memory for nz=%d", t->z_planes, plan->g.nz);
+    DeviceGuard dg(plan->device);
     if (t->z_mode == 4 && prj::zcl_supported(plan)) {
-        DeviceGuard dg(plan->device);
         cudaError_t e = prj::zcl_prepare(plan, 0);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) return cuda_fail(e, "cluster z kernel tables");
+    }
+    if (t->mixed_tau != plan->mixed_tau && (plan->spec32 || plan->kxs_mixed)) {
+        // the FP64 row count follows mixed_tau: the mixed set-up runs again at the next mixed call
+        cudaDeviceSynchronize();
+        if (plan->spec32) {
+            const size_t n32 = (size_t)(plan->g.nxh - plan->kxs_mixed) * plan->g.nz * plan->g.ny;
+            dfree(plan->spec32);
+            plan->spec32 = nullptr;
+            plan->device_bytes -= n32 * sizeof(float2);
+        }
+        plan->kxs_mixed = 0;
     }
     plan->tz_xd = t->x_rows;
     plan->tz_xp = t->x_rows;
     plan->zfft_rows = t->z_rows;
     plan->zmode = t->z_mode;
+    plan->z_planes = t->z_planes;
+    plan->z_stages = t->z_stages;
+    plan->thomas_async = t->thomas_ring;
+    plan->mixed_iters = t->mixed_iters;
+    plan->mixed_tau = t->mixed_tau;
     return PRJ_OK;
 }
 

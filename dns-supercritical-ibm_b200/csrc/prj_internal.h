@@ -110,7 +110,7 @@ struct prj_plan {
     int* kz_of_slot = nullptr;    // z wavenumber held by each slot of zd's output
     int kxs = 0;                  // spectral rows kx < kxs stored in FP64 (nxh on the FP64 path)
     int kxs_mixed = 0;            // FP64 row count of the mixed path
-    int mixed_iters = 2;          // refinement iterations of the mixed path
+    int mixed_iters = 1;          // refinement iterations of the mixed path
     float2* spec32 = nullptr;     // FP32 spectral rows of the mixed path
     double* pbar = nullptr;       // per-plane means of P (ny) for the mixed-path residual
     double* psum = nullptr;       // per-CTA partial sums of P from the inverse x kernel (ny x tiles)
@@ -124,19 +124,15 @@ struct prj_plan {
     bool use_pass = true;         // compile-time pass-plan FFT kernels where the length has one
     int thomas_async = -1;        // Thomas lines streamed through a cp.async shared-memory ring:
                                   // -1 for the mixed storage only, 0 never, 1..4 always (ring shape)
-    int x_staged = 0;             // divergence rows staged by bulk copies (persistent x-forward kernel):
-                                  // 0 off, else its threads per CTA (128 or 256)
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
     double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
     double* vd_ih = nullptr;      // 0.5 / rho (halo'd) of the variable-density step (scratch)
     double* zcl_dcls = nullptr;   // class tables of the pivots for the cluster z kernel (prj_zcluster.cu)
     double* zcl_ccls = nullptr;   // class tables of the back-substitution factors
     int* zcl_pos = nullptr;       // position of each slot's line in its class row
-    int zcl_yb = 0;               // planes per chunk of the cluster z kernel (0: default)
-    int zcl_ns = 0;               // its stages (0: default)
-    int overlap_chunks = 0;       // y chunks of the overlapped projection schedule (0: sequential)
-    cudaStream_t ov_st[2] = {nullptr, nullptr};  // its two helper streams (created on first use)
-    std::vector<cudaEvent_t> ov_ev;              // its events
+    int z_planes = 0;             // planes per chunk of the per-wavenumber z kernels (0: their default)
+    int z_stages = 0;             // stages of their copy rings (0: their default)
+    double mixed_tau = 1e-3;      // FP64-row threshold of the mixed path
 };
 
 namespace prj {

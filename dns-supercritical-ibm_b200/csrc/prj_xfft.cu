@@ -13,7 +13,6 @@
 #include "fft_dif.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
-#include "tma_util.cuh"
 
 // minimum resident CTAs per SM requested for the shared-memory FFT kernels
 #ifndef PRJ_FFT_MINB
@@ -395,131 +394,6 @@ __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_fwd_xp(const XA
     }
 }
 
-// k_fwd_xs: the divergence source of k_fwd_xp<1> with the rows staged by bulk
-// copies.  Persistent CTAs walk tiles t = y * (nz/TZ) + z-tile (z fastest, so the
-// W row z0+TZ and the V plane y+1 a tile reads are read by its neighbours close in
-// time, through L2).  A tile's raw halo'd rows -- U at (z, y), W at (z, y) and
-// (z+TZ, y), V at (z, y) and (z, y+1) -- land in shared memory by cp.async.bulk on
-// an mbarrier.  As soon as the divergence of tile t is formed from them, one
-// thread issues the copies of the CTA's next tile into the same buffer, so they
-// overlap tile t's FFT passes and transposed store.  Waits are bounded; a CTA
-// that gives up raises *err and returns.
-struct XsArgs {
-    XArgs a;
-    int* err;
-    int ntiles, ntz;
-};
-
-template <class PL, int TZ, int NT>
-__global__ void __launch_bounds__(NT) k_fwd_xs(const XsArgs xs) {
-    const XArgs& a = xs.a;
-    extern __shared__ __align__(16) unsigned char sm[];
-    constexpr int m = PL::n, nx = 2 * m, rs = pass_row_stride(m), hrow = nx + 2;
-    constexpr int NROW = 4 * TZ + 1;  // U: TZ, W: TZ + 1, V(y): TZ, V(y+1): TZ
-    double* stage = reinterpret_cast<double*>(sm);
-    double2* A = reinterpret_cast<double2*>(sm + (size_t)NROW * hrow * sizeof(double));
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + (size_t)NROW * hrow * sizeof(double) +
-                                                (size_t)padded_len(TZ * rs, true) * sizeof(double2));
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int nz = a.nz, ny = a.ny;
-    const size_t hplane = (size_t)hrow * (size_t)(nz + 2);
-    const uint32_t rowb = (uint32_t)(hrow * sizeof(double));
-
-    // one thread: copies of tile t's rows into the stage
-    auto issue = [&](int t) {
-        const int y = t / xs.ntz, z0 = (t - y * xs.ntz) * TZ;
-        const int zp = (z0 + TZ == nz) ? 0 : z0 + TZ;
-        const bool wb = (y == 0), wt = (y + 1 == ny);
-        const uint32_t bytes = rowb * (uint32_t)(2 * TZ + 1 + (wb ? 0 : TZ) + (wt ? 0 : TZ));
-        fence_proxy_async_shared();
-        mbar_arrive_expect_tx(bar, bytes);
-        const size_t base = (size_t)(y + 1) * hplane;
-        for (int r = 0; r < TZ; r++) {
-            const size_t row = base + (size_t)(z0 + r + 1) * hrow;
-            bulk_g2s(stage + (size_t)r * hrow, a.Uh + row, rowb, bar);
-            bulk_g2s(stage + (size_t)(TZ + r) * hrow, a.Wh + row, rowb, bar);
-            if (!wb) bulk_g2s(stage + (size_t)(2 * TZ + 1 + r) * hrow, a.Vh + row, rowb, bar);
-            if (!wt) bulk_g2s(stage + (size_t)(3 * TZ + 1 + r) * hrow, a.Vh + row + hplane, rowb, bar);
-        }
-        bulk_g2s(stage + (size_t)(2 * TZ) * hrow, a.Wh + base + (size_t)(zp + 1) * hrow, rowb, bar);
-    };
-
-    int t = blockIdx.x;
-    if (t >= xs.ntiles) return;
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (tid == 0) issue(t);
-    uint32_t phase = 0;
-    for (; t < xs.ntiles; t += gridDim.x) {
-        const bool ok = mbar_wait_bounded(bar, phase);
-        if (__syncthreads_or(!ok)) {
-            // give the copies in flight one more bounded wait before leaving
-            if (tid == 0) {
-                atomicExch(xs.err, 2);
-                mbar_wait_bounded(bar, phase);
-            }
-            return;
-        }
-        phase ^= 1u;
-        const int y = t / xs.ntz, z0 = (t - y * xs.ntz) * TZ;
-        const bool wb = (y == 0), wt = (y + 1 == ny);
-        const double idy = a.inv_dy_p[y];
-        // divergence (the operation order of div_at) into packed complex rows
-        for (int idx = tid; idx < TZ * m; idx += nthr) {
-            const int r = idx / m, e = idx - r * m;
-            const double* U = stage + (size_t)r * hrow + 1;  // interior x = 0
-            const double* W0 = stage + (size_t)(TZ + r) * hrow + 1;
-            const double* W1 = stage + (size_t)(TZ + r + 1) * hrow + 1;
-            const double* V0 = stage + (size_t)(2 * TZ + 1 + r) * hrow + 1;
-            const double* V1 = stage + (size_t)(3 * TZ + 1 + r) * hrow + 1;
-            const int i0 = 2 * e, i1 = i0 + 1, i2 = (i1 + 1 == nx) ? 0 : i1 + 1;
-            const double v00 = wb ? a.vbot : V0[i0], v01 = wb ? a.vbot : V0[i1];
-            const double v10 = wt ? a.vtop : V1[i0], v11 = wt ? a.vtop : V1[i1];
-            double s0 = __dmul_rn(__dsub_rn(U[i1], U[i0]), a.inv_dx);
-            s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(W1[i0], W0[i0]), a.inv_dz));
-            s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(v10, v00), idy));
-            double s1 = __dmul_rn(__dsub_rn(U[i2], U[i1]), a.inv_dx);
-            s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(W1[i1], W0[i1]), a.inv_dz));
-            s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(v11, v01), idy));
-            const double2 v = make_double2(__dmul_rn(a.inv_dt, s0), __dmul_rn(a.inv_dt, s1));
-            if (a.Bout) {
-                double* b = a.Bout + ((size_t)y * nz + z0 + r) * nx + i0;
-                b[0] = v.x;
-                b[1] = v.y;
-            }
-            A[sidx<true>(r * rs + e)] = v;
-        }
-        __syncthreads();
-        // the stage is consumed: the next tile's rows stream in during this tile's FFT
-        if (t + (int)gridDim.x < xs.ntiles && tid == 0) issue(t + gridDim.x);
-        dif_passes_shared<-1, PL, 0, PL::P>(A, TZ, rs, a.tw);
-        constexpr int half = m / 2;
-        for (int idx = tid; idx < TZ * (half + 1); idx += nthr) {
-            const int k = idx / TZ, r = idx - k * TZ;
-            const int base = r * rs;
-            const int z = z0 + r;
-            if (k == 0) {
-                const double2 c = A[sidx<true>(base)];
-                spec_store(a, y, 0, z, make_double2(c.x + c.y, 0.0));
-                spec_store(a, y, m, z, make_double2(c.x - c.y, 0.0));
-            } else {
-                const int kk = m - k;
-                const double2 zk = A[sidx<true>(base + pass_slot<PL>(k))];
-                const double2 zm = cconj(A[sidx<true>(base + pass_slot<PL>(kk))]);
-                const double2 e = cscale(cadd(zk, zm), 0.5);
-                const double2 d = csub(zk, zm);
-                const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
-                spec_store(a, y, k, z, cadd(e, cmul(a.post[k], o)));
-                if (kk != k) spec_store(a, y, kk, z, cadd(cconj(e), cmul(a.post[kk], cconj(o))));
-            }
-        }
-        __syncthreads();  // A is reused by the next tile
-    }
-}
-
 // k_bwd_xp: transposed load of X_k, X_{m-k} -> inverse split (scaled) into slot
 // order -> DIT passes -> P rows (x pairs as double2), optionally accumulated.
 template <class PL>
@@ -688,75 +562,10 @@ cudaError_t launch_bwd_xp_pl(const XArgs& a, const dim3& grid, cudaStream_t st) 
     return cudaGetLastError();
 }
 
-// rows per tile of the staged divergence kernel: the largest of 4, 2, 1 dividing nz
-// whose stage + FFT rows fit ~72 KB (three CTAs per SM); 0 if none
-int staged_tz(int m, int nz) {
-    for (int tz = 4; tz >= 1; tz /= 2) {
-        if (nz % tz) continue;
-        const size_t bytes = (size_t)(4 * tz + 1) * (2 * m + 2) * sizeof(double) +
-                             (size_t)padded_len(tz * pass_row_stride(m), true) * sizeof(double2) + 16;
-        if (bytes <= 72 * 1024) return tz;
-    }
-    return 0;
-}
-
-template <class PL, int TZ, int NT>
-cudaError_t launch_fwd_xs_tz(const XArgs& a, int* err, cudaStream_t st) {
-    constexpr int m = PL::n;
-    const size_t smem = (size_t)(4 * TZ + 1) * (2 * m + 2) * sizeof(double) +
-                        (size_t)padded_len(TZ * pass_row_stride(m), true) * sizeof(double2) + 16;
-    XsArgs xs{};
-    xs.a = a;
-    xs.a.tz = TZ;
-    xs.err = err;
-    xs.ntz = a.nz / TZ;
-    xs.ntiles = xs.ntz * a.ny;
-    cudaError_t e = cudaFuncSetAttribute(k_fwd_xs<PL, TZ, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int dev = 0, sms = 148, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fwd_xs<PL, TZ, NT>, NT, smem);
-    if (e != cudaSuccess) return e;
-    if (per < 1) return cudaErrorNotSupported;
-    const int grid = std::min(xs.ntiles, per * sms);
-    k_fwd_xs<PL, TZ, NT><<<grid, NT, smem, st>>>(xs);
-    return cudaGetLastError();
-}
-
-template <class PL>
-cudaError_t launch_fwd_xs_pl(const XArgs& a, int* err, int nt, cudaStream_t st) {
-    const bool w = nt >= 256;
-    switch (staged_tz(PL::n, a.nz)) {
-    case 4: return w ? launch_fwd_xs_tz<PL, 4, 256>(a, err, st) : launch_fwd_xs_tz<PL, 4, 128>(a, err, st);
-    case 2: return w ? launch_fwd_xs_tz<PL, 2, 256>(a, err, st) : launch_fwd_xs_tz<PL, 2, 128>(a, err, st);
-    case 1: return w ? launch_fwd_xs_tz<PL, 1, 256>(a, err, st) : launch_fwd_xs_tz<PL, 1, 128>(a, err, st);
-    default: return cudaErrorNotSupported;
-    }
-}
-
 // pass-plan x kernels for even nx whose half length has a pass plan built with the
 // same radices; cudaErrorNotSupported otherwise (the caller uses the runtime-radix kernels)
 cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, int ny_launch, cudaStream_t st) {
     if (!pl->use_pass || !a.even) return cudaErrorNotSupported;
-    if (fwd && src == FwdSource::Divergence && pl->x_staged && a.y0 == 0 && ny_launch == pl->g.ny &&
-        aligned16(a.Uh) && aligned16(a.Vh) && aligned16(a.Wh)) {
-        int* err = reinterpret_cast<int*>(pl->stat_buf + kStatErrSlot);
-        switch (a.m) {
-#define PRJ_XS_CASE(N, ...)                                                   \
-    case N: {                                                                 \
-        using PL = PassList<__VA_ARGS__>;                                     \
-        if (!same_radices<PL>(pl->xd.f)) break;                               \
-        const cudaError_t e = launch_fwd_xs_pl<PL>(a, err, pl->x_staged, st); \
-        if (e != cudaErrorNotSupported) return e;                             \
-        break;                                                                \
-    }
-            PRJ_PASS_PLANS(PRJ_XS_CASE)
-#undef PRJ_XS_CASE
-        default:
-            break;
-        }
-    }
     a.tz = pl->tz_xp;
     const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, ny_launch);
     switch (a.m) {

@@ -496,7 +496,7 @@ cudaError_t launch_zcl(const prj_plan* pl, cudaStream_t st) {
     a.ny = g.ny; a.nh = g.nxh;
     a.tw = pl->zd.tw; a.bands = pl->t.bands; a.dcls = pl->zcl_dcls; a.ccls = pl->zcl_ccls; a.pos = pl->zcl_pos;
     a.kz_of_slot = pl->kz_of_slot; a.X = pl->spec;
-    int yb = pl->zcl_yb > 0 ? pl->zcl_yb : 4, ns = pl->zcl_ns > 0 ? pl->zcl_ns : 3;
+    int yb = pl->z_planes > 0 ? pl->z_planes : 4, ns = pl->z_stages > 0 ? pl->z_stages : 3;
     if (ns < 2 || ns > 4) ns = 3;
     if (yb > g.ny) yb = g.ny;
     while (yb > 1 && zcl_smem(g.nz, yb, ns) > (size_t)100 * 1024) yb--;

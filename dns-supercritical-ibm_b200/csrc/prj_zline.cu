@@ -23,8 +23,6 @@
 // (poisson_solver_multigpu.f90:401-419, round-to-nearest intrinsics) are those of
 // k_zfft_pass and k_thomas, so the result is bitwise that of the split kernels.
 // cp.async copies complete on their own, so no wait here can hang.
-#include <cstdlib>
-
 #include "div_rn.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
@@ -228,21 +226,14 @@ cudaError_t launch_zline_pl(const ZLineArgs& a, size_t smem, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// wide = true: half the default lines per thread (twice the threads)
 template <class PL>
-cudaError_t launch_zline_ns(const ZLineArgs& a, int ns, bool wide, size_t smem, cudaStream_t st) {
-    constexpr int L = zl_lpt(PL::n), LW = L > 1 ? L / 2 : 1;
-    if (wide) return launch_zline_pl<PL, 2, LW>(a, smem, st);
+cudaError_t launch_zline_ns(const ZLineArgs& a, int ns, size_t smem, cudaStream_t st) {
+    constexpr int L = zl_lpt(PL::n);
     switch (ns) {
     case 2: return launch_zline_pl<PL, 2, L>(a, smem, st);
     case 3: return launch_zline_pl<PL, 3, L>(a, smem, st);
     default: return launch_zline_pl<PL, 4, L>(a, smem, st);
     }
-}
-
-int zl_env(const char* name, int dflt) {
-    const char* v = getenv(name);
-    return (v && *v) ? atoi(v) : dflt;
 }
 
 }  // namespace
@@ -267,13 +258,13 @@ cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st) {
     a.ny = g.ny; a.nh = g.nxh; a.mzp = g.mzp;
     a.tw = pl->zd.tw; a.bands = pl->t.bands; a.piv = pl->t.piv; a.pivc = pl->t.pivc;
     a.kz_of_slot = pl->kz_of_slot; a.X = pl->spec;
-    // planes per stage and stage count: PRJ_ZLINE_YB / PRJ_ZLINE_NS, else 4 x 2; the
-    // planes per stage shrink until the ring fits PRJ_ZLINE_SMEM_KB (default 72 KB: three
-    // CTAs per SM)
-    int yb = zl_env("PRJ_ZLINE_YB", 4), ns = zl_env("PRJ_ZLINE_NS", 2);
-    const size_t cap = (size_t)std::min(200, std::max(16, zl_env("PRJ_ZLINE_SMEM_KB", 72))) * 1024;
-    const bool wide = zl_env("PRJ_ZLINE_WIDE", 0) != 0;  // two-stage ring only
-    if (ns < 2 || ns > 4 || wide) ns = 2;
+    // planes per stage and stage count: the plan's z_planes / z_stages tuning, else 4 x 2;
+    // the planes per stage shrink until the ring fits 72 KB (three CTAs per SM).  Measured
+    // at 768x384x384 and not kept: deeper rings at fewer CTAs per SM, and one line per
+    // thread (twice the threads, spilling at the register budget of three CTAs per SM).
+    int yb = pl->z_planes > 0 ? pl->z_planes : 4, ns = pl->z_stages > 0 ? pl->z_stages : 2;
+    const size_t cap = (size_t)72 * 1024;
+    if (ns < 2 || ns > 4) ns = 2;
     if (yb < 1) yb = 1;
     if (yb > g.ny) yb = g.ny;
     while (yb > 1 && zline_smem(g.nz, g.mzp, yb, ns) > cap) yb--;
@@ -285,7 +276,7 @@ cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st) {
     case N: {                                                                \
         using PL = PassList<__VA_ARGS__>;                                    \
         if (!same_radices<PL>(pl->zd.f)) return cudaErrorNotSupported;       \
-        return launch_zline_ns<PL>(a, ns, wide, smem, st);                   \
+        return launch_zline_ns<PL>(a, ns, smem, st);                         \
     }
         PRJ_PASS_PLANS(PRJ_ZL_CASE)
 #undef PRJ_ZL_CASE

@@ -244,13 +244,8 @@ cudaError_t launch_ppt(const ZPipeArgs& a, int ppt, int nthr, size_t smem, cudaS
 
 }  // namespace
 
-int env_int(const char* name, int dflt) {
-    const char* v = getenv(name);
-    return (v && *v) ? atoi(v) : dflt;
-}
-
 // Chooses the chunk size and ring depth for about 72 KB of shared memory (three
-// CTAs per SM; PRJ_ZSOLVE_YB / PRJ_ZSOLVE_NS override them for tuning) and
+// CTAs per SM; the plan's z_planes / z_stages tuning overrides them) and
 // returns cudaErrorNotSupported when even one plane per chunk with two stages
 // does not fit, so the caller can use the unpipelined kernel.
 cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStream_t st) {
@@ -266,7 +261,7 @@ cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStrea
         const size_t extra = dif ? ((size_t)g.nz * sizeof(int) + 15) / 16 * 16 : (size_t)yb * xrow;
         return (size_t)ns * yb * (xrow + prow) + extra + 8 * (size_t)ns;
     };
-    int yb = env_int("PRJ_ZSOLVE_YB", 0), ns = env_int("PRJ_ZSOLVE_NS", 0);
+    int yb = pl->z_planes, ns = pl->z_stages;
     if (yb < 1 || ns < 2 || ns > 8 || bytes(yb, ns) > 200 * 1024) {
         yb = 0;
         const int pref_ns = dif ? 2 : 3;

@@ -407,14 +407,10 @@ cudaError_t launch_zfft_pass_pl(ZfftArgs a, int rows_req, cudaStream_t st) {
     const size_t smem = (size_t)padded_len(a.rb * PL::n, true) * sizeof(double2);
     const unsigned grid = (unsigned)((a.nrow_total + a.rb - 1) / a.rb);
     if (grid == 0) return cudaSuccess;
-    // the inverse stages its slot-order rows through shared memory (coalesced copy-in);
-    // PRJ_ZINV_STAGE=0 reads them in its first pass instead (measured at 768x384x384:
-    // 0.33 ms staged against 0.37 ms direct; 0.093 / 0.113 ms at 512x256x256)
-    static const bool stage_inv = [] {
-        const char* v = getenv("PRJ_ZINV_STAGE");
-        return !(v && atoi(v) == 0);
-    }();
-    if (DIR > 0 && stage_inv) {
+    // the inverse stages its slot-order rows through shared memory (coalesced copy-in;
+    // measured at 768x384x384: 0.33 ms staged against 0.37 ms reading them in the first
+    // pass; 0.093 / 0.113 ms at 512x256x256)
+    if (DIR > 0) {
         cudaError_t e = allow_smem(k_zfft_pass<DIR, T, PL, true>, smem);
         if (e != cudaSuccess) return e;
         k_zfft_pass<DIR, T, PL, true><<<grid, kPassThreads, smem, st>>>(a);

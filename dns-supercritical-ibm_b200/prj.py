@@ -82,7 +82,9 @@ class Stats(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("x_rows", ctypes.c_int), ("z_rows", ctypes.c_int), ("z_mode", ctypes.c_int)]
+    _fields_ = [("x_rows", ctypes.c_int), ("z_rows", ctypes.c_int), ("z_mode", ctypes.c_int),
+                ("z_planes", ctypes.c_int), ("z_stages", ctypes.c_int), ("thomas_ring", ctypes.c_int),
+                ("mixed_iters", ctypes.c_int), ("mixed_tau", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -166,7 +168,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
-    L.prj_plan_schedule.argtypes = [_vp, i, ctypes.POINTER(i), ctypes.POINTER(i)]
+    L.prj_plan_schedule.argtypes = [_vp, i, ctypes.POINTER(i)]
     L.prj_projection_step_host_async.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.POINTER(StepParams), i]
     L.prj_host_async_wait.argtypes = [_vp]
     L.prj_selftest_wait_timeout.argtypes = [i, ctypes.c_longlong]
@@ -342,18 +344,11 @@ class Plan:
     def host_async_wait(self):
         _check(load_library().prj_host_async_wait(self.handle))
 
-    def schedule(self, mode=MODE_FP64):
-        """(kernel launches per projection step, overlapped y chunks) (prj_plan_schedule)."""
-        n, c = ctypes.c_int(), ctypes.c_int()
-        _check(load_library().prj_plan_schedule(self.handle, mode, ctypes.byref(n), ctypes.byref(c)))
-        return n.value, c.value
-
     def launches_per_step(self, mode=MODE_FP64):
-        return self.schedule(mode)[0]
-
-    @property
-    def overlap_chunks(self):
-        return self.schedule(MODE_FP64)[1]
+        """Kernel launches of one projection step of ``mode`` (prj_plan_schedule)."""
+        n = ctypes.c_int()
+        _check(load_library().prj_plan_schedule(self.handle, mode, ctypes.byref(n)))
+        return n.value
 
     def set_vd_metric(self, inv_dy_p_pad):
         """inv_dy_p_pad (ny+1) for projection_step_vd (prj_plan_set_vd_metric)."""
@@ -418,8 +413,17 @@ class Plan:
         _check(load_library().prj_plan_get_tuning(self.handle, ctypes.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, x_rows, z_rows=0, z_mode=0):
-        _check(load_library().prj_plan_set_tuning(self.handle, ctypes.byref(Tuning(x_rows, z_rows, z_mode))))
+    def set_tuning(self, x_rows=None, z_rows=None, z_mode=None, **kw):
+        """Change some fields of the plan's tuning (prj_plan_set_tuning); the others keep their
+        current values.  Fields: x_rows, z_rows, z_mode, z_planes, z_stages, thomas_ring,
+        mixed_iters, mixed_tau."""
+        t = self.tuning
+        for k, v in (("x_rows", x_rows), ("z_rows", z_rows), ("z_mode", z_mode), *kw.items()):
+            if k not in t:
+                raise TypeError(f"unknown tuning field {k!r}")
+            if v is not None:
+                t[k] = v
+        _check(load_library().prj_plan_set_tuning(self.handle, ctypes.byref(Tuning(**t))))
 
     # ---------------------------------------------------------------- solve
     def poisson_mixed(self, P, stream=None):

@@ -147,9 +147,8 @@ int prj_host_async_wait(prj_plan* plan);
  * refinement (the precision scheme of PRJ_MODE_FP32_REFINE): rows of
  * x-wavenumbers whose tridiagonals are badly conditioned stay FP64, the
  * residual b - A p of the pinned operator is formed in FP64.  One refinement
- * pass by default (environment variable PRJ_MIXED_ITERS, read at the plan's
- * first mixed call).  Needs in-place transform plans (radices 2, 3, 4, 5, 8 for
- * nx/2 and nz).  Asynchronous.
+ * pass by default (the tuning's mixed_iters).  Needs in-place transform plans
+ * (radices 2, 3, 4, 5, 6, 8 for nx/2 and nz).  Asynchronous.
  */
 int prj_poisson_mixed(prj_plan* plan, double* d_P, void* stream);
 
@@ -282,20 +281,45 @@ int prj_batch_launch(prj_batch* batch, void* stream);
 int prj_batch_destroy(prj_batch* batch);
 
 /*
- * Launch-shape tuning of a plan (read by the autotuner, which times
- * candidates and caches the winner per grid size):
- *   x_rows  x-rows per CTA of the x-transform kernels (power of two, 1..16);
- *   z_rows  spectral rows per CTA of the z-transform kernels (power of two, 1..16);
- *   z_mode  0 = z FFT / Thomas / inverse z FFT as three kernels, 1 = one fused
- *           pipelined kernel per x-wavenumber (runtime radices), 3 = one kernel per
- *           x-wavenumber on the compile-time pass plans (three kernels where nz has
- *           no pass plan).  The default is 3 when nx/2+1 >= 2 x the SM count, else 0.
- * prj_plan_set_tuning rejects shapes that do not fit shared memory.
+ * Tuning of a plan: launch shapes and kernel choices (read by the autotuner,
+ * which times candidates and caches the winner per grid size), and the
+ * parameters of the mixed path.  Every knob is a plan field: the launchers read
+ * nothing else.
+ *   x_rows      x-rows per CTA of the x-transform kernels (power of two, 1..16);
+ *   z_rows      spectral rows per CTA of the split z-transform kernels (0 = default,
+ *               else a power of two, 1..16);
+ *   z_mode      0 = z FFT / Thomas / inverse z FFT as three kernels, 1 = one fused
+ *               pipelined kernel per x wavenumber (runtime radices; the kernel of z
+ *               lengths with a prime factor above 5), 2 = its unpipelined form,
+ *               3 = one kernel per x wavenumber on the compile-time pass plans,
+ *               4 = the same on a thread-block cluster of R_0 CTAs per x wavenumber
+ *               (R_0 the plan's first radix); 3 and 4 run the three kernels where nz
+ *               has no pass plan.  The default is 3 when nx/2+1 >= 2 x the SM count,
+ *               else 0;
+ *   z_planes    planes per chunk of the per-wavenumber z kernels (0 = default);
+ *   z_stages    stages of their copy rings (0 = default, else 2..4; 2..8 for mode 1);
+ *   thomas_ring shared-memory ring of the split Thomas kernel: -1 = default (the
+ *               mixed storage only), 0 = none, 1..4 = shapes 4x4, 8x2, 2x8, 8x3
+ *               (planes x stages) for both storages;
+ *   mixed_iters refinement passes of PRJ_MODE_FP32_REFINE (default 1, 0..8);
+ *   mixed_tau   x-wavenumber rows with |a_x| < mixed_tau max|b| keep FP64 storage in
+ *               the mixed path (default 1e-3; must lie in (0, 1)).
+ * prj_plan_set_tuning rejects values out of range and shapes that do not fit
+ * shared memory; it may allocate (tables of z_mode 4, the mixed path's FP32
+ * spectrum after a change of mixed_tau), so call it outside stream capture.
+ * The environment variables PRJ_ZSOLVE (split|fused|basic|line|cluster),
+ * PRJ_FFT_KERNELS=runtime and PRJ_THOMAS_ASYNC are read once, at plan creation,
+ * as test hooks for the defaults.
  */
 typedef struct prj_tuning {
     int x_rows;
     int z_rows;
     int z_mode;
+    int z_planes;
+    int z_stages;
+    int thomas_ring;
+    int mixed_iters;
+    double mixed_tau;
 } prj_tuning;
 int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out);
 int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
@@ -317,13 +341,8 @@ int prj_selftest_division(int device, long long n, unsigned long long seed, long
                           double* first_u, double* first_d);
 
 /* Kernel launches one prj_projection_step of `mode` issues with the plan's current
- * configuration (statistics excluded), and the number of y chunks of the overlapped
- * FP64 schedule (0 when the kernels run one after another).  The overlapped
- * schedule (environment variable PRJ_OVERLAP_CHUNKS, default 0 = off) splits the planes
- * into chunks and overlaps the x transform, z transforms and correction of
- * neighbouring chunks on three streams forked from and joined back into the
- * caller's stream; stage timing switches it off. */
-int prj_plan_schedule(const prj_plan* plan, int mode, int* launches, int* chunks);
+ * configuration (statistics excluded). */
+int prj_plan_schedule(const prj_plan* plan, int mode, int* launches);
 
 /* band modes of prj_bands_from_yu */
 #define PRJ_BANDS_REFERENCE 0   /* the reference's mk_P_abc bands */

@@ -119,25 +119,6 @@ def test_projection_rejects_bad_params(cuda_device):
     torch.cuda.synchronize()
 
 
-@pytest.mark.parametrize("chunks", [2, 3, 5])
-def test_overlapped_schedule_is_bitwise_sequential(cuda_device, monkeypatch, chunks):
-    """The chunked three-stream schedule runs the same kernels on the same planes: the step's
-    outputs equal the sequential schedule's bit for bit (uneven chunk sizes included)."""
-    import prj
-    import workloads
-    nx, ny, nz = 96, 64, 48
-    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=4)
-    wall = (0.01, 0.0, -0.02, 0.03, 0.0, 0.04)
-    outs = []
-    for c in (0, chunks):
-        monkeypatch.setenv("PRJ_OVERLAP_CHUNKS", str(c))
-        with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
-            assert plan.overlap_chunks == c and plan.launches_per_step() == (5 * c + 1 if c else 6)
-            outs.append(run_engine(plan, Uh, Vh, Wh, 0.9, wall))
-    for a, b in zip(outs[0][:4], outs[1][:4]):
-        np.testing.assert_array_equal(a, b)
-
-
 def test_pipelined_host_steps_match_sync(cuda_device):
     """Three pipelined host-buffer steps (alternating staging slots) give the synchronous call's
     outputs bit for bit."""
@@ -165,25 +146,6 @@ def test_pipelined_host_steps_match_sync(cuda_device):
             plan.projection_step(Uh, Vh, Wh, *want, 0.8, stats=False)
             for a, b in zip(o, want):
                 np.testing.assert_array_equal(a, b)
-
-
-@pytest.mark.parametrize("threads", [128, 256])
-def test_staged_x_forward_matches_oracle(cuda_device, oracle, monkeypatch, threads):
-    """PRJ_X_STAGED selects the persistent divergence x kernel (k_fwd_xs) whose halo'd rows
-    arrive by bulk copies on mbarriers with bounded waits: same step as the oracle."""
-    import prj
-    import workloads
-    monkeypatch.setenv("PRJ_X_STAGED", str(threads))
-    nx, ny, nz = 128, 96, 64
-    Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=6)
-    wall = (0.01, 0.0, -0.02, 0.03, 0.0, 0.04)
-    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
-        U, V, W, P, st = run_engine(plan, Uh, Vh, Wh, 0.5, wall)
-    Uo, Vo, Wo, Po = oracle.projection(Uh, Vh, Wh, dx, dz, 0.5, yu, "consistent", wall)
-    assert rel_l2(P, Po) <= 1e-12
-    for a, b in ((U, Uo), (V, Vo), (W, Wo)):
-        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
-    assert st["div_maxabs"] <= 1e-10
 
 
 @pytest.mark.parametrize("shape", [(64, 48, 32), (30, 17, 21)])

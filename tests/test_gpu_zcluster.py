@@ -17,17 +17,18 @@ from gpu_util import from_dev, to_dev
 pytestmark = pytest.mark.gpu
 
 
-def _solve(monkeypatch, env, nx, ny, nz, seed):
+def _solve(monkeypatch, env, nx, ny, nz, seed, **tuning):
     import prj
     import workloads
-    for k in ("PRJ_ZSOLVE", "PRJ_ZCL_YB", "PRJ_ZCL_NS"):
-        monkeypatch.delenv(k, raising=False)
+    monkeypatch.delenv("PRJ_ZSOLVE", raising=False)
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=seed)
     with prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent")) as plan:
         if env.get("PRJ_ZSOLVE") == "cluster":
             assert plan.tuning["z_mode"] == 4
+        if tuning:
+            plan.set_tuning(**tuning)
         t = to_dev(rhs)
         plan.poisson_fp64(t)
         plan.check_error()
@@ -46,8 +47,7 @@ def test_cluster_kernel_is_bitwise_split_every_plan(cuda_device, monkeypatch, nz
 def test_cluster_kernel_chunk_shapes(cuda_device, monkeypatch, yb, ns):
     nx, ny, nz = 64, 61, 384
     split = _solve(monkeypatch, {"PRJ_ZSOLVE": "split"}, nx, ny, nz, seed=32)
-    clus = _solve(monkeypatch, {"PRJ_ZSOLVE": "cluster", "PRJ_ZCL_YB": str(yb), "PRJ_ZCL_NS": str(ns)},
-                  nx, ny, nz, seed=32)
+    clus = _solve(monkeypatch, {"PRJ_ZSOLVE": "cluster"}, nx, ny, nz, seed=32, z_planes=yb, z_stages=ns)
     np.testing.assert_array_equal(split, clus)
 
 

@@ -14,13 +14,15 @@ from gpu_util import from_dev, to_dev
 pytestmark = pytest.mark.gpu
 
 
-def _solve(monkeypatch, env, nx, ny, nz, seed):
+def _solve(monkeypatch, env, nx, ny, nz, seed, **tuning):
     import prj
     import workloads
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=seed)
     with prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent")) as plan:
+        if tuning:
+            plan.set_tuning(**tuning)
         t = to_dev(rhs)
         plan.poisson_fp64(t)
         return from_dev(t)
@@ -39,8 +41,7 @@ def test_line_kernel_is_bitwise_split(cuda_device, monkeypatch, shape):
 def test_line_kernel_ring_shapes(cuda_device, monkeypatch, yb, ns):
     nx, ny, nz = 64, 61, 384
     split = _solve(monkeypatch, {"PRJ_ZSOLVE": "split"}, nx, ny, nz, seed=22)
-    line = _solve(monkeypatch, {"PRJ_ZSOLVE": "line", "PRJ_ZLINE_YB": str(yb), "PRJ_ZLINE_NS": str(ns)},
-                  nx, ny, nz, seed=22)
+    line = _solve(monkeypatch, {"PRJ_ZSOLVE": "line"}, nx, ny, nz, seed=22, z_planes=yb, z_stages=ns)
     np.testing.assert_array_equal(split, line)
 
 
