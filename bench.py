@@ -480,20 +480,51 @@ def run_vd(device, nx, ny, nz, steps, warmup):
             "stages_ms_per_launch": {k: v[0] / v[1] for k, v in stages.items()}}
 
 
-def run_served(device, seconds, rate, budget):
+def run_served(device, seconds, rate, budget, io="device"):
     """Open-loop Poisson arrivals (rate per second, default_rng(3)) of projection requests of
-    sizes (128,96,64)/(256,128,128)/(384,192,192)/(768,384,384) with p = 0.4/0.3/0.2/0.1."""
+    sizes (128,96,64)/(256,128,128)/(384,192,192)/(768,384,384) with p = 0.4/0.3/0.2/0.1.
+    io "device": every request's predictor is produced on the device from its own seed and its
+    U, V, W, P are left on the device for the caller (a result handle); io "host": every
+    request's predictor is copied in from pinned host memory (a pool of one field set per
+    size, the requests of a size taking turns) and its U, V, W, P are copied back to pinned
+    host memory, both inside the request's latency."""
+    import torch
     import serve
+    import workloads
     arrivals = serve.poisson_arrivals(rate, seconds, seed=3)
+    reqs = [serve.Request(i, size, t, seed=1000 + i) for i, (t, size) in enumerate(arrivals)]
+    h2d = d2h = 0
+    if io == "host":
+        pin = lambda shape: torch.empty(tuple(reversed(shape)), dtype=torch.float64).pin_memory().numpy().T
+        pool = {}
+        for size in sorted({r.size for r in reqs}):
+            nx, ny, nz = size
+            Uh, Vh, Wh, *_ = workloads.projection_inputs(nx, ny, nz, seed=17)
+            hs = (nx + 2, nz + 2, ny + 2)
+            ins = tuple(pin(hs) for _ in range(3))
+            for dst, src in zip(ins, (Uh, Vh, Wh)):
+                dst[...] = src
+            pool[size] = (ins, tuple(pin(hs) for _ in range(3)) + (pin((nx, nz, ny)),))
+        for r in reqs:
+            r.fields, r.out = pool[r.size]
+            r.want = "host"
+            nx, ny, nz = r.size
+            h2d += 3 * 8 * (nx + 2) * (nz + 2) * (ny + 2)
+            d2h += 3 * 8 * (nx + 2) * (nz + 2) * (ny + 2) + 8 * nx * ny * nz
     srv = serve.ProjectionServer(device=device.index or 0, hbm_budget=budget)
     t0 = time.perf_counter()
-    done = srv.run(arrivals)
+    done = srv.run(None, requests=reqs)
     wall = time.perf_counter() - t0
     out = serve.summarize(done, seconds)
     offered = sum(a * b * c for _, (a, b, c) in arrivals) / seconds / 1e9
     out.update({"rate_hz": rate, "offered_gpts_per_s": offered, "wall_s": wall,
                 "max_inflight": srv.max_inflight, "peak_resident_gb": srv.peak_used / 1e9,
-                "sustained": bool(out["drain_s"] is not None and out["drain_s"] < 0.05 * seconds)})
+                "sustained": bool(out["drain_s"] is not None and out["drain_s"] < 0.05 * seconds),
+                "io": ("predictor produced on the device per request from its seed; U, V, W, P left on the "
+                       "device (result handle)") if io == "device" else
+                      ("predictor copied in from pinned host memory and U, V, W, P copied back to pinned host "
+                       "memory inside each request"),
+                "h2d_bytes_per_request": h2d / max(1, len(reqs)), "d2h_bytes_per_request": d2h / max(1, len(reqs))})
     srv.close()
     return out
 
@@ -690,6 +721,11 @@ def main():
             # the same request mix at a rate one GPU sustains: latency without queue growth
             extra["served_sustainable"] = run_served(device, min(10.0, args.served_seconds), 1000.0,
                                                      args.served_budget_gb * 1e9)
+            torch.cuda.empty_cache()
+            # requests that bring their fields from host memory and take their results back there
+            # (PCIe-bound: about 0.9 GB of copies per request of the mix)
+            extra["served_host_io"] = run_served(device, min(10.0, args.served_seconds), 40.0,
+                                                 args.served_budget_gb * 1e9, io="host")
             torch.cuda.empty_cache()
         extra["variable_density"] = run_vd(device, NX, NY, NZ, steps=max(3, args.steps // 4), warmup=args.warmup)
         torch.cuda.empty_cache()

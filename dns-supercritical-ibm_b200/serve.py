@@ -1,25 +1,40 @@
 """Served projection solves: a continuous-batching request loop on one GPU.
 
-Requests (one projection step of a channel case of some size) arrive on an
-open-loop schedule.  The server keeps, per grid size, a pool of resident
-*slots*: a solver plan plus the device fields of one request (predictor u_hat,
-outputs u, v, w, p) and a CUDA stream.  A queued request is admitted as soon as
-a slot of its size is idle; if none exists, a new slot is created when it fits
-the HBM budget, evicting idle slots of other sizes (least recently used) when
-needed.  Admitted requests run asynchronously on their slot's stream, so
-requests of different sizes overlap on the device; completion is detected with
-CUDA events.  Latency is completion time minus arrival time (host clock).
+Requests arrive on an open-loop schedule.  Each request is one projection step of
+a channel case of some size and carries its own predictor field, in one of two
+forms:
 
-Predictor fields are synthetic (a channel profile plus seeded noise), generated
-once per slot; a request uses its slot's field, so a result can be replayed
-alone and compared bit for bit (see tests/test_gpu_serve.py).
+* ``seed``: the predictor u_hat is produced on the device from the request's
+  seed (a channel profile plus seeded N(0, 0.1) noise, v = 0 at the walls).  This
+  is how a DNS time loop hands the projection its input: the momentum step leaves
+  u_hat in device memory (src/main.f90:386-393 calls the projection on it);
+* ``fields``: host arrays (Uh, Vh, Wh) in the reference's halo'd Fortran layout,
+  copied to the device inside the request's timed work (pinned memory makes the
+  copy asynchronous).
+
+The result is handed back either as a device handle (``want="device"``: the
+completion callback reads the slot's U, V, W, P while the slot is still held for
+it) or copied into host arrays the request brings (``want="host"``: the
+device-to-host copies are part of the request's work and latency).
+
+The server keeps, per grid size, a pool of resident *slots*: a solver plan, the
+device fields of one request and a CUDA stream.  A queued request is admitted as
+soon as a slot of its size is idle; if none exists, a new slot is created when it
+fits the HBM budget, evicting idle slots of other sizes (least recently used)
+when needed.  Admitted requests run asynchronously on their slot's stream (input,
+projection, output), so requests of different sizes overlap on the device.  One
+waiter thread per slot blocks on the slot's completion event (a blocking-sync
+event, so the thread sleeps) and stamps the completion time; the admission loop
+sleeps on the completion queue between arrivals instead of polling.  Latency is
+completion time minus arrival time (host clock).
 """
 from __future__ import annotations
 
 import collections
-import math
+import queue
+import threading
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -36,6 +51,10 @@ class Request:
     rid: int
     size: tuple
     arrival: float           # seconds since the start of the run
+    seed: int = 0            # predictor produced on the device from this seed (when fields is None)
+    fields: tuple = None     # or host (Uh, Vh, Wh), halo'd Fortran-ordered [x+2, z+2, y+2]
+    want: str = "device"     # "device": result handle; "host": U, V, W, P copied into `out`
+    out: tuple = None        # host (U, V, W, P) for want == "host" (P Fortran-ordered [x, z, y])
     start: float = -1.0
     done: float = -1.0
     slot: object = None
@@ -49,10 +68,12 @@ class Slot:
     stream: object
     event: object
     nbytes: int
-    seed: int
+    yp: object               # cell-centre coordinates (device) of the predictor profile
     busy: bool = False
     last_used: float = 0.0
     current: Request = None
+    waiter: object = None
+    jobs: object = None
 
 
 def poisson_arrivals(rate_hz: float, duration_s: float, seed: int = 3, sizes=SERVED_SIZES, probs=SERVED_PROBS):
@@ -65,6 +86,23 @@ def poisson_arrivals(rate_hz: float, duration_s: float, seed: int = 3, sizes=SER
             break
         out.append((t, sizes[int(rng.choice(len(sizes), p=probs))]))
     return out
+
+
+def device_predictor(Uh, Vh, Wh, yp, seed):
+    """The channel predictor of one request in place on the device, deterministic in
+    `seed`: U = 1.5 (1 - (y-1)^2) + N(0, 0.1), V, W = N(0, 0.1) (drawn in the order U,
+    V, W), V = 0 on the bottom wall face; halo'd [y+2, z+2, x+2] tensors, interior only
+    (the projection reads no halo of its inputs)."""
+    import torch
+    ny, nz, nx = Uh.shape[0] - 2, Uh.shape[1] - 2, Uh.shape[2] - 2
+    g = torch.Generator(device=Uh.device)
+    g.manual_seed(int(seed))
+    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+    Uh[inner] = torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=Uh.device).mul_(0.1).add_(
+        1.5 * (1 - (yp.view(-1, 1, 1) - 1) ** 2))
+    Vh[inner] = torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=Uh.device).mul_(0.1)
+    Wh[inner] = torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=Uh.device).mul_(0.1)
+    Vh[1] = 0.0
 
 
 class ProjectionServer:
@@ -83,7 +121,8 @@ class ProjectionServer:
         self.used = 0
         self.peak_used = 0
         self.max_inflight = 0
-        self.seed = 100
+        self._done_q = queue.Queue()
+        self._t0 = time.perf_counter()
 
     # ------------------------------------------------------------------ slots
     def _slot_bytes(self, size):
@@ -93,6 +132,17 @@ class ProjectionServer:
         plan = 16 * (nx // 2 + 1) * nz * ny + 8 * (nx // 2 + 1) * (nz // 2 + 2) * ny
         return fields + plan
 
+    def _waiter_loop(self, slot):
+        """Blocks on the slot's completion events in order; stamps and reports completions."""
+        while True:
+            job = slot.jobs.get()
+            if job is None:
+                return
+            req, ev = job
+            ev.synchronize()
+            req.done = time.perf_counter() - self._t0
+            self._done_q.put(req)
+
     def _new_slot(self, size):
         torch = self.torch
         nx, ny, nz = size
@@ -100,30 +150,29 @@ class ProjectionServer:
         yu = workloads.tanh_faces(ny, 2.0)
         dx, dz = workloads.channel_spacing(nx, nz)
         plan = prj.Plan.from_yu(nx, nz, dx, dz, yu, self.band_mode, device=self.device)
-        self.seed += 1
-        g = torch.Generator(device=dev)
-        g.manual_seed(self.seed)
         hs = (ny + 2, nz + 2, nx + 2)
-        yp = torch.tensor((yu[:-1] + yu[1:]) / 2, dtype=torch.float64, device=dev)
         Uh = torch.zeros(hs, dtype=torch.float64, device=dev)
-        Vh = torch.zeros_like(Uh)
-        Wh = torch.zeros_like(Uh)
-        inner = (slice(1, -1), slice(1, -1), slice(1, -1))
-        Uh[inner] = 1.5 * (1 - (yp.view(-1, 1, 1) - 1) ** 2) + 0.1 * torch.randn((ny, nz, nx), generator=g,
-                                                                                dtype=torch.float64, device=dev)
-        Vh[inner] = 0.1 * torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=dev)
-        Wh[inner] = 0.1 * torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=dev)
-        Vh[1] = 0.0
+        Vh, Wh = torch.zeros_like(Uh), torch.zeros_like(Uh)
         U, V, W = (torch.empty_like(Uh) for _ in range(3))
         P = torch.empty((ny, nz, nx), dtype=torch.float64, device=dev)
+        yp = torch.tensor((yu[:-1] + yu[1:]) / 2, dtype=torch.float64, device=dev)
         s = torch.cuda.Stream(device=dev)
         torch.cuda.synchronize(dev)
         nbytes = plan.device_bytes + 8 * (6 * Uh.numel() + P.numel())
-        slot = Slot(size, plan, (Uh, Vh, Wh, U, V, W, P), s, torch.cuda.Event(), nbytes, self.seed)
+        slot = Slot(size, plan, (Uh, Vh, Wh, U, V, W, P), s, None, nbytes, yp)
+        slot.jobs = queue.Queue()
+        slot.waiter = threading.Thread(target=self._waiter_loop, args=(slot,), daemon=True)
+        slot.waiter.start()
         self.slots.append(slot)
         self.used += nbytes
         self.peak_used = max(self.peak_used, self.used)
         return slot
+
+    def _drop(self, s):
+        s.jobs.put(None)
+        s.waiter.join()
+        s.plan.close()
+        s.fields = None
 
     def _evict_for(self, need):
         """Free idle slots of least recent use until `need` more bytes fit."""
@@ -133,8 +182,7 @@ class ProjectionServer:
                 break
             self.slots.remove(s)
             self.used -= s.nbytes
-            s.plan.close()
-            s.fields = None
+            self._drop(s)
         return self.used + need <= self.budget
 
     def _acquire(self, size, now):
@@ -156,14 +204,31 @@ class ProjectionServer:
         return self._new_slot(size)
 
     def launch(self, slot, req):
+        """The request's work on the slot's stream: its input, the projection step, its output."""
+        torch = self.torch
         Uh, Vh, Wh, U, V, W, P = slot.fields
+        with torch.cuda.stream(slot.stream):
+            if req.fields is not None:
+                for d, h in zip((Uh, Vh, Wh), req.fields):
+                    d.copy_(torch.from_numpy(h.T), non_blocking=True)
+            else:
+                device_predictor(Uh, Vh, Wh, slot.yp, req.seed)
         slot.plan.projection_step(Uh, Vh, Wh, U, V, W, P, self.dt, mode=self.mode, stats=False, stream=slot.stream)
-        slot.event.record(slot.stream)
+        if req.want == "host":
+            with torch.cuda.stream(slot.stream):
+                for h, d in zip(req.out, (U, V, W, P)):
+                    torch.from_numpy(h.T).copy_(d, non_blocking=True)
+        ev = torch.cuda.Event(blocking=True)
+        ev.record(slot.stream)
+        slot.jobs.put((req, ev))
 
     # ------------------------------------------------------------------- loop
-    def run(self, arrivals, on_complete=None, warm=True):
-        """Serve `arrivals` [(t, size)], return the list of completed requests."""
-        sizes = sorted({s for _, s in arrivals})
+    def run(self, arrivals, on_complete=None, warm=True, requests=None):
+        """Serve `arrivals` [(t, size)] (or ready Request objects in arrival order); return the
+        completed requests.  Requests made from `arrivals` carry seed = 1000 + index."""
+        if requests is None:
+            requests = [Request(i, size, t, seed=1000 + i) for i, (t, size) in enumerate(arrivals)]
+        sizes = sorted({r.size for r in requests})
         if warm:  # the per-size slots that fit the budget, created before the clock starts
             for k in range(self.slots_per_size):
                 for size in sizes:
@@ -173,31 +238,33 @@ class ProjectionServer:
                         self.slots[-1].busy = True  # keep _acquire from returning it again
             for sl in self.slots:
                 sl.busy = False
-        reqs = [Request(i, size, t) for i, (t, size) in enumerate(arrivals)]
         queues = {size: collections.deque() for size in sizes}
         queued = 0
-        inflight = []
+        inflight = 0
         done = []
         nxt = 0
-        t0 = time.perf_counter()
-        while nxt < len(reqs) or queued or inflight:
+        self._t0 = t0 = time.perf_counter()
+
+        def finish(r):
+            nonlocal inflight
+            inflight -= 1
+            if on_complete:
+                on_complete(r)  # the slot stays held while the callback reads its outputs
+            r.slot.busy = False
+            r.slot.last_used = r.done
+            done.append(r)
+
+        while nxt < len(requests) or queued or inflight:
             now = time.perf_counter() - t0
-            while nxt < len(reqs) and reqs[nxt].arrival <= now:
-                queues[reqs[nxt].size].append(reqs[nxt])
+            while nxt < len(requests) and requests[nxt].arrival <= now:
+                queues[requests[nxt].size].append(requests[nxt])
                 queued += 1
                 nxt += 1
-            still = []
-            for r in inflight:
-                if r.slot.event.query():
-                    r.done = time.perf_counter() - t0
-                    r.slot.busy = False
-                    r.slot.last_used = r.done
-                    if on_complete:
-                        on_complete(r)
-                    done.append(r)
-                else:
-                    still.append(r)
-            inflight = still
+            while True:
+                try:
+                    finish(self._done_q.get_nowait())
+                except queue.Empty:
+                    break
             # admit the oldest waiting request of each size while that size has a free slot;
             # sizes go in order of their oldest request, and a size without a slot blocks no other
             blocked = False
@@ -214,17 +281,26 @@ class ProjectionServer:
                     r.slot = slot
                     r.start = time.perf_counter() - t0
                     self.launch(slot, r)
-                    inflight.append(r)
-                    self.max_inflight = max(self.max_inflight, len(inflight))
+                    inflight += 1
+                    self.max_inflight = max(self.max_inflight, inflight)
             if blocked and not inflight:
                 raise RuntimeError("requests cannot be admitted within the HBM budget")
-            if nxt < len(reqs) and not inflight and not queued:
-                time.sleep(max(0.0, min(1e-3, reqs[nxt].arrival - (time.perf_counter() - t0))))
+            # sleep until the next completion or the next arrival
+            wait = 0.05
+            if nxt < len(requests):
+                wait = max(0.0, requests[nxt].arrival - (time.perf_counter() - t0))
+            if inflight:
+                try:
+                    finish(self._done_q.get(timeout=wait if wait > 0 else 1e-4))
+                except queue.Empty:
+                    pass
+            elif wait > 0 and not queued:
+                time.sleep(wait)
         return done
 
     def close(self):
         for s in self.slots:
-            s.plan.close()
+            self._drop(s)
         self.slots = []
         self.used = 0
 
