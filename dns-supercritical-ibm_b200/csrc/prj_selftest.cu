@@ -32,8 +32,9 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
     return z ^ (z >> 31);
 }
 
-// a double with a random sign and mantissa and an exponent in [-span, span] about 1;
-// every eighth value has an all-ones or all-zeros mantissa (the rounding edges)
+// a double with a random sign and mantissa and an exponent in [-span, span] about 1
+// (span <= 1022: normal numbers); every eighth value has an all-ones or all-zeros
+// mantissa (the rounding edges)
 __device__ __forceinline__ double random_double(unsigned long long w, unsigned long long w2, int span) {
     unsigned long long mant = w & 0xfffffffffffffull;
     const int sel = (int)(w2 & 7);
@@ -44,13 +45,46 @@ __device__ __forceinline__ double random_double(unsigned long long w, unsigned l
     return __longlong_as_double((long long)bits);
 }
 
+// a double with a random sign and mantissa and any exponent field 0 .. 2047 (zeros,
+// subnormals, normals across the whole range, infinities and NaNs)
+__device__ __forceinline__ double any_double(unsigned long long w, unsigned long long w2) {
+    unsigned long long mant = w & 0xfffffffffffffull;
+    const int sel = (int)(w2 & 7);
+    if (sel == 0) mant = 0xfffffffffffffull;
+    if (sel == 1) mant = 0;
+    const unsigned long long ex = (w2 >> 8) % 2048ull;
+    return __longlong_as_double((long long)(((w >> 63) << 63) | (ex << 52) | mant));
+}
+
+// pairs of three kinds by index: u within 2^+-200 and D within 2^+-100 of 1 (the pivots
+// and spectra of a solve), both anywhere in the double range, and one of them near the
+// edges of the fast path's exponent window
 __global__ void k_div_selftest(long long n, unsigned long long seed, unsigned long long* bad, double* first) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = seed * 0x100000000ull + (unsigned long long)i * 4;
-        const unsigned long long wu = mix64(k), wu2 = mix64(k + 1);
-        double u = random_double(wu, wu2, 200);
+        const unsigned long long wu = mix64(k), wu2 = mix64(k + 1), wd = mix64(k + 2), wd2 = mix64(k + 3);
+        double u, D;
+        switch (i % 4) {
+        case 0:
+        case 1:
+            u = random_double(wu, wu2, 200);
+            D = random_double(wd, wd2, 100);
+            break;
+        case 2:
+            u = any_double(wu, wu2);
+            D = any_double(wd, wd2);
+            break;
+        default: {
+            // exponents within 40 of the window's bounds: u near 2^-960 or 2^1020, D near
+            // 2^-1000 or 2^1000 (ldexp rounds to subnormals or infinities past the range)
+            const int eu = ((wu2 >> 40) & 1 ? 1020 : -960) + (int)((wu2 >> 41) % 81ull) - 40;
+            const int ed = ((wd2 >> 40) & 1 ? 1000 : -1000) + (int)((wd2 >> 41) % 81ull) - 40;
+            u = ldexp(random_double(wu, wu2, 0), eu);
+            D = ldexp(random_double(wd, wd2, 0), ed);
+            break;
+        }
+        }
         if (((wu2 >> 20) & 31) == 0) u = (wu >> 63) ? -0.0 : 0.0;  // signed zero numerators
-        const double D = random_double(mix64(k + 2), mix64(k + 3), 100);
         const double want = __ddiv_rn(u, D);
         const double got = div_by_recip(u, D, __drcp_rn(D));
         if (__double_as_longlong(want) != __double_as_longlong(got)) {

@@ -332,7 +332,9 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
 int prj_selftest_wait_timeout(int device, long long budget_cycles);
 
 /* Diagnostic of the division the Thomas forward sweeps use: n pseudo-random pairs
- * (u, D) from `seed` (exponents within 2^+-200 and 2^+-100 of 1, random and edge
+ * (u, D) from `seed` (half with exponents within 2^+-200 and 2^+-100 of 1, a quarter
+ * anywhere in the double range -- zeros, subnormals, infinities and NaNs included -- and
+ * a quarter near the bounds of the fast path's exponent window; random and edge
  * mantissas), each divided both by __ddiv_rn and by the reciprocal-and-correction form
  * of div_rn.cuh; *mismatches counts the pairs whose two results differ in any bit
  * (the first such pair in first_u, first_d when not NULL).  No counterpart in the
