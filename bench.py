@@ -264,10 +264,11 @@ def timed_steps(fn, stream, steps):
 
 
 def run_batched(device, steps, warmup, rank=0, world=1, dist=None):
-    """64 independent Poisson solves of uneven sizes in one CUDA graph launch: sizes from
-    default_rng(2) (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]),
-    uniform[-1,1] right-hand sides minus their dy-weighted mean; launch shapes from the
-    autotuner.  FP64 and FP32-storage + FP64-refinement graphs."""
+    """64 independent Poisson solves of uneven sizes in one launch: sizes from default_rng(2)
+    (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]), uniform[-1,1]
+    right-hand sides minus their dy-weighted mean; launch shapes from the autotuner.  FP64: the
+    persistent work-queue kernel (one kernel per batch); FP32-storage + FP64 refinement: one CUDA
+    graph of the per-case kernels."""
     import numpy as np
     import torch
     import autotune
@@ -330,8 +331,12 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None):
             if dist is not None:
                 dist.barrier()
             total = sharding.max_over_ranks(total, dist, device)
+            info = batch.info
             out[name] = {"gpts_per_s": pts * steps / (total / 1e3) / 1e9, "ms_per_batch": total / steps,
-                         "graph_launches": steps}
+                         "launches": steps, "persistent_kernel": info["persistent"],
+                         "kernels_per_launch": info["kernels_per_launch"], "work_items": info["work_items"]}
+            if info["persistent"]:
+                batch.check_error(stream)
     for p in plans:
         p.close()
     return out

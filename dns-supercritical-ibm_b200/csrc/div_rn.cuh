@@ -12,33 +12,33 @@
 // not depend on the previous step), the dependent work per step is one multiply, two
 // fused multiply-adds and a select.
 //
-// The correction step is exact only while u, D and q stay inside the normal range with
-// room to spare: y = RN(1/D) must be normal, u - D q must be representable (it is about
-// 2^-53 |u|, so u must lie well above the subnormal range) and q must neither overflow
-// nor underflow.  Outside the window |u| in [2^-960, 2^1020] (or u = 0), |D| and |q| in
-// [2^-1000, 2^1000] -- subnormal, huge, infinite or NaN operands, a zero divisor -- the
-// quotient is taken from __ddiv_rn instead, so the result is RN(u / D) for every pair of
-// doubles.  The window tests are integer compares on the exponent fields; the D test does
-// not depend on the recurrence, and the q test runs beside the residual's multiply-add.
-// prj_selftest_division compares the function with __ddiv_rn bit for bit on random
-// pairs in and around the window (subnormals, infinities, NaNs and zeros included).
+// The correction step is exact only while the operands and the quotient stay inside the
+// normal range with room to spare: y = RN(1/D) must be normal, u - D q must be
+// representable (it is about 2^-53 |u|, so u must lie well above the subnormal range)
+// and q must neither overflow nor underflow.  The divisors here are Thomas pivots, and
+// plan creation checks that every pivot satisfies 2^-40 <= |D| <= 2^1000
+// (PRJ_ERR_NUMERIC otherwise).  With D in that range, |q| in [2^-900, 2^1000) implies
+// |u| >= 2^-941, so all three conditions hold; the function tests only the quotient's
+// exponent (its high word: a mask, a subtraction and a compare) and takes the quotient
+// from __ddiv_rn outside that window, unless u = 0 (then q = +-0 is exact).  So for every
+// u -- zeros, subnormals, infinities and NaNs included -- and every D in the pivot range,
+// the result is RN(u / D).  prj_selftest_division compares it with __ddiv_rn bit for
+// bit on random pairs of that domain, with the window's edges weighted.
 #pragma once
 
 namespace prj {
 
-// lo <= unbiased exponent of x <= hi (subnormals and zeros count as -1023, infinities
-// and NaNs as 1024)
-__device__ __forceinline__ bool exp_within(double x, int lo, int hi) {
-    const int e = (int)((unsigned long long)__double_as_longlong(x) >> 52 & 0x7ffull) - 1023;
-    return (unsigned)(e - lo) <= (unsigned)(hi - lo);
-}
+// smallest and largest |D| for which div_by_recip is correctly rounded for every u
+constexpr double kDivRecipMinD = 0x1p-40;
+constexpr double kDivRecipMaxD = 0x1p1000;
 
 __device__ __forceinline__ double div_by_recip(double u, double D, double y) {
     const double q = __dmul_rn(u, y);
     const double r = __fma_rn(-D, q, u);
-    const bool in_window =
-        exp_within(D, -1000, 1000) && (u == 0.0 || (exp_within(u, -960, 1020) && exp_within(q, -1000, 1000)));
-    if (!in_window) return __ddiv_rn(u, D);
+    // 2^-900 <= |q| < 2^1000: the biased exponent of q in [123, 2023)
+    const unsigned hq = (unsigned)__double2hiint(q) & 0x7fffffffu;
+    const bool q_in = hq - 0x07B00000u < 0x7E700000u - 0x07B00000u;
+    if (!q_in && u != 0.0) return __ddiv_rn(u, D);
     return r == 0.0 ? q : __fma_rn(r, y, q);
 }
 

@@ -16,6 +16,7 @@
 
 #include "../../include/projection.h"
 #include "fft_host.h"
+#include "div_rn.cuh"
 #include "prj_internal.h"
 
 namespace {
@@ -165,7 +166,6 @@ int make_slot_table(int n, int** d_out, size_t* bytes) {
 // nx/2+1 = 385 / 513 / 769, but 0.30 / 0.45 ms against 0.21 / 0.37 ms for 193 / 257.
 int z_mode(bool split_ok, bool line_pref) {
     const char* v = getenv("PRJ_ZSOLVE");
-    if (v && !strcmp(v, "cluster")) return split_ok ? 4 : 1;
     if (v && !strcmp(v, "fused")) return 1;
     if (v && !strcmp(v, "basic")) return 2;
     if (v && !strcmp(v, "line")) return split_ok ? 3 : 1;
@@ -190,9 +190,6 @@ void free_plan_buffers(prj_plan* pl) {
     dfree(pl->zd.tw);
     dfree(pl->zd.pos);
     dfree(pl->kz_of_slot);
-    dfree(pl->zcl_dcls);
-    dfree(pl->zcl_ccls);
-    dfree(pl->zcl_pos);
     dfree(pl->spec32);
     dfree(pl->pbar);
     dfree(pl->psum);
@@ -405,7 +402,7 @@ int run_mixed_solve(prj_plan* pl, const double* Uh, const double* Vh, const doub
 }
 
 int mixed_supported(const prj_plan* pl) {
-    if ((pl->zmode != 0 && pl->zmode != 3 && pl->zmode != 4) || !pl->xd.ok)
+    if ((pl->zmode != 0 && pl->zmode != 3) || !pl->xd.ok)
         return fail(PRJ_ERR_UNSUPPORTED, "the mixed-precision path needs in-place plans for nx/2 and nz (radices 2, 3, 4, 5, 8)");
     return PRJ_OK;
 }
@@ -428,15 +425,7 @@ int run_mixed_poisson(prj_plan* pl, double* P, cudaStream_t st) {
 
 // z transforms + Thomas: three kernels (split) or one fused kernel
 int run_zsolve(prj_plan* pl, cudaStream_t st) {
-    if (pl->zmode == 4) {
-        StageTimer tm(pl, prj::kStZSolve, st);
-        const cudaError_t e = prj::launch_zcl(pl, st);
-        if (e != cudaErrorNotSupported) {
-            CK(e, "z transform + Thomas (cluster kernel)");
-            return PRJ_OK;
-        }
-    }
-    if (pl->zmode == 3 || pl->zmode == 4) {
+    if (pl->zmode == 3) {
         StageTimer tm(pl, prj::kStZSolve, st);
         const cudaError_t e = prj::launch_zline(pl, st);
         if (e != cudaErrorNotSupported) {
@@ -444,7 +433,7 @@ int run_zsolve(prj_plan* pl, cudaStream_t st) {
             return PRJ_OK;
         }
     }
-    if (pl->zmode == 0 || pl->zmode == 3 || pl->zmode == 4) {
+    if (pl->zmode == 0 || pl->zmode == 3) {
         {
             StageTimer tm(pl, prj::kStZfftFwd, st);
             CK(prj::launch_zfft(pl, -1, st), "z transform");
@@ -505,6 +494,9 @@ struct BatchImpl {
     int ncases = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    bool persistent = false;   // one persistent kernel over a work queue (FP64 cases of the
+    prj::BatchKernel bk;       // kernel's pass-plan lengths); else the per-case graph
+    int graph_kernels = 0;     // kernel launches per replay of the graph
 };
 
 }  // namespace
@@ -513,6 +505,7 @@ struct prj_batch : BatchImpl {};
 
 namespace {
 void batch_release(prj_batch* b) {
+    prj::batchk_free(&b->bk);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -724,18 +717,19 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
     if ((e = cudaMemset(pl->stat_buf, 0, 8 * sizeof(double))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMemset(stats)"));
     if ((e = prj::launch_build_pivots(pl, 0)) != cudaSuccess) return bail(cuda_fail(e, "pivot table"));
-    double mp = 0;
-    if ((e = cudaMemcpy(&mp, pl->stat_buf, sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess)
+    double mm[2] = {0, 0};
+    if ((e = cudaMemcpy(mm, pl->stat_buf, sizeof(mm), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return bail(cuda_fail(e, "pivot table"));
+    const double mp = mm[0];
     pl->min_pivot = mp;
     if (!(mp > 0) || !std::isfinite(mp))
         return bail(fail(PRJ_ERR_NUMERIC, "zero or non-finite Thomas pivot (min_abs_div_bacp = %g)", mp));
+    if (!(mp >= prj::kDivRecipMinD) || !(mm[1] <= prj::kDivRecipMaxD))
+        return bail(fail(PRJ_ERR_NUMERIC,
+                         "Thomas pivots |D| in [%g, %g] leave the range [2^-40, 2^1000] of the forward sweeps' "
+                         "correctly rounded division (a nearly singular wall-normal operator)",
+                         mp, mm[1]));
     pl->device_bytes = bytes;
-    if (pl->zmode == 4) {
-        if (!prj::zcl_supported(pl)) pl->zmode = 3;
-        else if ((e = prj::zcl_prepare(pl, 0)) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess)
-            return bail(cuda_fail(e, "cluster z kernel tables"));
-    }
     *out = pl;
     return PRJ_OK;
 }
@@ -1143,8 +1137,7 @@ bool x_pass_active(const prj_plan* pl) {
 int prj_plan_schedule(const prj_plan* plan, int mode, int* launches) {
     if (!plan || !launches) return fail(PRJ_ERR_ARG, "NULL argument");
     if (mode == PRJ_MODE_FP64) {
-        const bool one_z = (plan->zmode == 1 || plan->zmode == 2) || (plan->zmode == 3 && prj::zline_supported(plan)) ||
-                           (plan->zmode == 4 && (prj::zcl_supported(plan) || prj::zline_supported(plan)));
+        const bool one_z = (plan->zmode == 1 || plan->zmode == 2) || (plan->zmode == 3 && prj::zline_supported(plan));
         *launches = one_z ? 4 : 6;
     } else {
         // forward x, z transforms of the FP64 and FP32 rows, one Thomas launch, inverse z of both,
@@ -1176,8 +1169,8 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
     auto pow2 = [](int v) { return v >= 1 && v <= 16 && (v & (v - 1)) == 0; };
     if (!pow2(t->x_rows)) return fail(PRJ_ERR_ARG, "x_rows=%d must be a power of two in [1, 16]", t->x_rows);
     if (t->z_rows != 0 && !pow2(t->z_rows)) return fail(PRJ_ERR_ARG, "z_rows=%d must be 0 or a power of two in [1, 16]", t->z_rows);
-    if (t->z_mode < 0 || t->z_mode > 4) return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1, 2, 3 or 4", t->z_mode);
-    if ((t->z_mode == 0 || t->z_mode == 3 || t->z_mode == 4) && !(plan->zd.ok && plan->kz_of_slot))
+    if (t->z_mode < 0 || t->z_mode > 3) return fail(PRJ_ERR_ARG, "z_mode=%d must be 0, 1, 2 or 3", t->z_mode);
+    if ((t->z_mode == 0 || t->z_mode == 3) && !(plan->zd.ok && plan->kz_of_slot))
         return fail(PRJ_ERR_UNSUPPORTED, "no in-place z plan for nz=%d", plan->g.nz);
     if (t->z_planes < 0 || t->z_planes > 64) return fail(PRJ_ERR_ARG, "z_planes=%d must lie in [0, 64]", t->z_planes);
     if (t->z_stages != 0 && (t->z_stages < 2 || t->z_stages > (t->z_mode == 1 ? 8 : 4)))
@@ -1190,15 +1183,7 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
         return fail(PRJ_ERR_ARG, "x_rows=%d does not fit shared memory for nx=%d", t->x_rows, plan->g.nx);
     if (t->z_rows && (size_t)prj::padded_len(t->z_rows * plan->g.nz, true) * sizeof(double2) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "z_rows=%d does not fit shared memory for nz=%d", t->z_rows, plan->g.nz);
-    if (t->z_mode == 4 && t->z_planes && prj::zcl_supported(plan) &&
-        prj::zcl_smem(plan->g.nz, t->z_planes, t->z_stages ? t->z_stages : 3) > (size_t)200 * 1024)
-        return fail(PRJ_ERR_ARG, "z_planes=%d does not fit shared memory for nz=%d", t->z_planes, plan->g.nz);
     DeviceGuard dg(plan->device);
-    if (t->z_mode == 4 && prj::zcl_supported(plan)) {
-        cudaError_t e = prj::zcl_prepare(plan, 0);
-        if (e == cudaSuccess) e = cudaDeviceSynchronize();
-        if (e != cudaSuccess) return cuda_fail(e, "cluster z kernel tables");
-    }
     if (t->mixed_tau != plan->mixed_tau && (plan->spec32 || plan->kxs_mixed)) {
         // the FP64 row count follows mixed_tau: the mixed set-up runs again at the next mixed call
         cudaDeviceSynchronize();
@@ -1238,6 +1223,23 @@ int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int
         if (mode == PRJ_MODE_FP32_REFINE && (rc = mixed_supported(plans[i]))) return rc;
     }
     DeviceGuard dg(dev);
+    bool persistent = (mode == PRJ_MODE_FP64);
+    for (int i = 0; i < ncases && persistent; i++) persistent = prj::batchk_supported(plans[i]);
+    if (persistent) {
+        prj_batch* b = new prj_batch();
+        b->device = dev;
+        b->ncases = ncases;
+        b->persistent = true;
+        cudaError_t e = prj::batchk_build(plans, d_P, ncases, &b->bk);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            batch_release(b);
+            delete b;
+            return cuda_fail(e, "persistent batch kernel set-up");
+        }
+        *out = b;
+        return PRJ_OK;
+    }
     // eager pass: lazy buffers, kernel attributes, and a check that every case runs
     std::vector<cudaStream_t> streams((size_t)ncases, nullptr);
     std::vector<cudaEvent_t> joins((size_t)ncases, nullptr);
@@ -1291,6 +1293,17 @@ int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int
     }
     for (int i = 0; i < ncases; i++) plans[i]->timing = timing[i];
     if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (!rc && e == cudaSuccess) {
+        size_t nn = 0;
+        if (cudaGraphGetNodes(b->graph, nullptr, &nn) == cudaSuccess && nn) {
+            std::vector<cudaGraphNode_t> nodes(nn);
+            cudaGraphGetNodes(b->graph, nodes.data(), &nn);
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) b->graph_kernels++;
+            }
+        }
+    }
     if (rc || e != cudaSuccess) {
         if (!rc) rc = cuda_fail(e, "batch graph capture");
         batch_release(b);
@@ -1303,9 +1316,35 @@ int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int
 }
 
 int prj_batch_launch(prj_batch* batch, void* stream) {
-    if (!batch || !batch->exec) return fail(PRJ_ERR_ARG, "batch is NULL or empty");
+    if (!batch || (!batch->exec && !batch->persistent)) return fail(PRJ_ERR_ARG, "batch is NULL or empty");
     DeviceGuard dg(batch->device);
+    if (batch->persistent) {
+        CK(prj::batchk_launch(batch->bk, (cudaStream_t)stream), "persistent batch kernel");
+        return PRJ_OK;
+    }
     CK(cudaGraphLaunch(batch->exec, (cudaStream_t)stream), "batch graph launch");
+    return PRJ_OK;
+}
+
+int prj_batch_info(const prj_batch* batch, int* persistent, int* kernels_per_launch, long long* work_items) {
+    if (!batch) return fail(PRJ_ERR_ARG, "batch is NULL");
+    if (persistent) *persistent = batch->persistent ? 1 : 0;
+    if (kernels_per_launch) *kernels_per_launch = batch->persistent ? 1 : batch->graph_kernels;
+    if (work_items) *work_items = batch->persistent ? batch->bk.nitems : 0;
+    return PRJ_OK;
+}
+
+int prj_batch_check_error(prj_batch* batch, void* stream) {
+    if (!batch) return fail(PRJ_ERR_ARG, "batch is NULL");
+    if (!batch->persistent) return PRJ_OK;
+    DeviceGuard dg(batch->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int* word = prj::batchk_err_word(batch->bk);
+    int dev_err = 0;
+    CK(cudaMemcpyAsync(&dev_err, word, sizeof(int), cudaMemcpyDeviceToHost, st), "batch error word");
+    CK(cudaMemsetAsync(word, 0, sizeof(int), st), "batch error word");
+    CK(cudaStreamSynchronize(st), "batch error word");
+    if (dev_err) return fail(PRJ_ERR_TIMEOUT, "a bounded wait of the persistent batch kernel gave up (code %d)", dev_err);
     return PRJ_OK;
 }
 

@@ -1,0 +1,267 @@
+// prj_batchk.cu -- many FP64 Poisson solves of uneven sizes in one persistent kernel.
+//
+// A batch of independent solves (the reference solves one grid per run and plans it
+// once, poisson_solver_multigpu.f90:77-129; here every case keeps its own plan) is a
+// list of work items (case, stage, tile).  The five stages of a solve are the split
+// path's kernels -- forward x transform, forward z transform, Thomas sweeps, inverse z
+// transform, inverse x transform -- and a tile is what one CTA of that kernel does.
+// The host orders the items stage-major (every case's forward x tiles, then every
+// case's forward z tiles, ...), largest cases first within a stage, and one launch of
+// k_batch runs them all:
+//
+//   a CTA takes the next item index from a global counter (atomicAdd), waits until the
+//   case's previous stage has completed all its tiles (a per-case, per-stage counter,
+//   read with acquire semantics), runs the tile with the same device function as the
+//   per-case kernel (xfft_tiles.cuh, zsplit_tiles.cuh), and counts the tile done
+//   (release);
+//   items are taken in order, and an item depends only on items before it, all of which
+//   are held by running CTAs that wait only on earlier items, so the queue cannot
+//   deadlock, whatever number of CTAs is resident;
+//   every wait is bounded (a clock budget): a CTA that gives up raises the batch's
+//   error word, counts its tile done without running it (so later waits end too) and
+//   continues; prj_batch_check_error reports PRJ_ERR_TIMEOUT.
+//
+// The tiles run the per-case kernels' code on the same elements, so every case's P
+// equals its own prj_poisson_fp64 bit for bit.  One launch replaces ncases x 5 small
+// kernels, their launch gaps and their tails.  Counters are reset by a memset issued
+// with the launch, so the pair can be captured in a CUDA graph.
+#include <algorithm>
+#include <vector>
+
+#include "prj_internal.h"
+#include "tma_util.cuh"
+#include "xfft_tiles.cuh"
+#include "zsplit_tiles.cuh"
+
+namespace prj {
+
+// stages of one solve
+enum BatchStage { kBFwdX = 0, kBZFwd = 1, kBThomas = 2, kBZInv = 3, kBBwdX = 4, kBNumStages = 5 };
+
+struct BatchCaseDev {
+    XArgs x;          // forward (source P) and inverse (P out) x transforms of the case
+    ZfftArgs z;       // its z rows (ny nh rows of nz)
+    ThomasArgs t;     // its Thomas lines
+    int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in kBatchPlans
+    int ntz;          // x tiles per y plane
+    int tiles[kBNumStages];
+};
+
+// a run of items: tiles tile0 .. tile0+count-1 of one stage of one case
+struct BatchSeg {
+    long long item0;
+    int case_id, stage, tile0, count;
+};
+
+namespace {
+
+// lengths the persistent kernel dispatches (the pass plans up to 256 points)
+#define PRJ_BATCH_PLANS(X) \
+    X(0, 16, 4, 4)         \
+    X(1, 24, 6, 4)         \
+    X(2, 32, 8, 4)         \
+    X(3, 48, 6, 8)         \
+    X(4, 64, 8, 8)         \
+    X(5, 96, 2, 6, 8)      \
+    X(6, 128, 4, 4, 8)     \
+    X(7, 192, 3, 8, 8)     \
+    X(8, 256, 8, 4, 8)
+
+constexpr int kBatchThreads = kPassThreads;  // = kThomasTile
+static_assert(kPassThreads == kThomasTile, "one CTA shape for every stage");
+
+__device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    const int bx = tile % c.ntz, by = tile / c.ntz;
+    switch (c.xplan) {
+#define PRJ_BX(I, N, ...) \
+    case I: fwd_xp_tile<0, PassList<__VA_ARGS__>>(c.x, sm, bx, by); break;
+        PRJ_BATCH_PLANS(PRJ_BX)
+#undef PRJ_BX
+    default: break;
+    }
+}
+
+__device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    const int bx = tile % c.ntz, by = tile / c.ntz;
+    switch (c.xplan) {
+#define PRJ_BX(I, N, ...) \
+    case I: bwd_xp_tile<PassList<__VA_ARGS__>>(c.x, sm, bx, by, c.ntz); break;
+        PRJ_BATCH_PLANS(PRJ_BX)
+#undef PRJ_BX
+    default: break;
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ void run_z(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    double2* zp = reinterpret_cast<double2*>(sm);
+    switch (c.zplan) {
+#define PRJ_BZ(I, N, ...) \
+    case I: zfft_pass_tile<DIR, double2, PassList<__VA_ARGS__>, (DIR > 0)>(c.z, zp, tile); break;
+        PRJ_BATCH_PLANS(PRJ_BZ)
+#undef PRJ_BZ
+    default: break;
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 4)
+    k_batch(const BatchCaseDev* __restrict__ cases, const BatchSeg* __restrict__ segs, int nseg, long long nitems,
+            unsigned long long* counter, int* done, int* err) {
+    extern __shared__ __align__(16) unsigned char bsm[];
+    __shared__ long long s_item;
+    __shared__ int s_seg, s_skip;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long it = (long long)atomicAdd(counter, 1ull);
+            int sg = -1, skip = 0;
+            if (it < nitems) {
+                int lo = 0, hi = nseg - 1;  // last segment with item0 <= it
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) / 2;
+                    if (segs[mid].item0 <= it) lo = mid;
+                    else hi = mid - 1;
+                }
+                sg = lo;
+                const BatchSeg& g = segs[sg];
+                if (g.stage > 0) {
+                    const int need = cases[g.case_id].tiles[g.stage - 1];
+                    const volatile int* d = done + g.case_id * kBNumStages + g.stage - 1;
+                    const long long t0 = clock64();
+                    while (*d < need) {
+                        if (clock64() - t0 > kWaitBudgetCycles) {
+                            atomicExch(err, 4);
+                            skip = 1;
+                            break;
+                        }
+                        __nanosleep(128);
+                    }
+                    __threadfence();  // acquire: the previous stage's results before this tile's reads
+                }
+            }
+            s_item = it;
+            s_seg = sg;
+            s_skip = skip;
+        }
+        __syncthreads();
+        const long long it = s_item;
+        if (it >= nitems) break;
+        const BatchSeg g = segs[s_seg];
+        const BatchCaseDev& c = cases[g.case_id];
+        const int tile = g.tile0 + (int)(it - g.item0);
+        if (!s_skip) {
+            switch (g.stage) {
+            case kBFwdX: run_x_fwd(c, tile, bsm); break;
+            case kBZFwd: run_z<-1>(c, tile, bsm); break;
+            case kBThomas: thomas_line<double2>(c.t, tile); break;
+            case kBZInv: run_z<+1>(c, tile, bsm); break;
+            default: run_x_bwd(c, tile, bsm); break;
+            }
+        }
+        __syncthreads();  // every thread's stores of the tile, and bsm free for the next one
+        if (threadIdx.x == 0) {
+            __threadfence();  // release: the tile's stores before its count
+            atomicAdd(done + g.case_id * kBNumStages + g.stage, 1);
+        }
+    }
+}
+
+int batch_plan_index(int n, const DifDev& f) {
+    switch (n) {
+#define PRJ_BI(I, N, ...) \
+    case N: return same_radices<PassList<__VA_ARGS__>>(f) ? I : -1;
+        PRJ_BATCH_PLANS(PRJ_BI)
+#undef PRJ_BI
+    default:
+        return -1;
+    }
+}
+
+}  // namespace
+
+bool batchk_supported(const prj_plan* pl) {
+    return pl->use_pass && pl->fx64.even && pl->xd.ok && pl->zd.ok && pl->kz_of_slot && pl->t.pivc &&
+           batch_plan_index(pl->fx64.m, pl->xd.f) >= 0 && batch_plan_index(pl->g.nz, pl->zd.f) >= 0 &&
+           pl->kxs == pl->g.nxh;
+}
+
+cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases, BatchKernel* out) {
+    std::vector<BatchCaseDev> cs((size_t)ncases);
+    size_t smem = 0;
+    for (int i = 0; i < ncases; i++) {
+        const prj_plan* pl = plans[i];
+        const Geometry& g = pl->g;
+        BatchCaseDev& c = cs[i];
+        c.x = batch_x_args(pl, d_P[i]);
+        c.z = batch_z_args(pl);
+        c.t = thomas_args(pl, pl->spec, 0, g.nxh);
+        c.xplan = batch_plan_index(pl->fx64.m, pl->xd.f);
+        c.zplan = batch_plan_index(g.nz, pl->zd.f);
+        c.ntz = (g.nz + c.x.tz - 1) / c.x.tz;
+        c.tiles[kBFwdX] = c.tiles[kBBwdX] = c.ntz * g.ny;
+        c.tiles[kBZFwd] = c.tiles[kBZInv] = (c.z.nrow_total + c.z.rb - 1) / c.z.rb;
+        c.tiles[kBThomas] = g.nxh * c.t.tiles;
+        smem = std::max(smem, pass_x_smem(pl->fx64.m, c.x.tz));
+        smem = std::max(smem, (size_t)padded_len(c.z.rb * g.nz, true) * sizeof(double2));
+    }
+    // stage-major order; within a stage the cases with the most tiles first
+    std::vector<int> order((size_t)ncases);
+    for (int i = 0; i < ncases; i++) order[i] = i;
+    std::vector<BatchSeg> segs;
+    long long items = 0;
+    for (int s = 0; s < kBNumStages; s++) {
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cs[a].tiles[s] > cs[b].tiles[s]; });
+        for (int i : order) {
+            if (cs[i].tiles[s] <= 0) continue;
+            segs.push_back(BatchSeg{items, i, s, 0, cs[i].tiles[s]});
+            items += cs[i].tiles[s];
+        }
+    }
+    if (smem > (size_t)200 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1));
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch, kBatchThreads, smem)) != cudaSuccess) return e;
+    if (per < 1) return cudaErrorInvalidConfiguration;
+    out->grid = (int)std::min<long long>((long long)per * sms, items);
+    out->smem = smem;
+    out->nseg = (int)segs.size();
+    out->nitems = items;
+    out->ncases = ncases;
+    const size_t cb = cs.size() * sizeof(BatchCaseDev), sb = segs.size() * sizeof(BatchSeg);
+    const size_t wb = sizeof(unsigned long long) + (size_t)ncases * kBNumStages * sizeof(int) + sizeof(int);
+    if ((e = cudaMalloc(&out->d_cases, cb)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&out->d_segs, sb)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&out->d_work, wb)) != cudaSuccess) return e;
+    out->work_bytes = wb - sizeof(int);  // the error word after the counters is cleared by its check
+    if ((e = cudaMemcpy(out->d_cases, cs.data(), cb, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(out->d_segs, segs.data(), sb, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    return cudaMemset(out->d_work, 0, wb);
+}
+
+cudaError_t batchk_launch(const BatchKernel& k, cudaStream_t st) {
+    unsigned char* w = static_cast<unsigned char*>(k.d_work);
+    cudaError_t e = cudaMemsetAsync(w, 0, k.work_bytes, st);
+    if (e != cudaSuccess) return e;
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(w);
+    int* done = reinterpret_cast<int*>(w + sizeof(unsigned long long));
+    int* err = done + (size_t)k.ncases * kBNumStages;
+    k_batch<<<k.grid, kBatchThreads, k.smem, st>>>(static_cast<const BatchCaseDev*>(k.d_cases),
+                                                   static_cast<const BatchSeg*>(k.d_segs), k.nseg, k.nitems, counter,
+                                                   done, err);
+    return cudaGetLastError();
+}
+
+int* batchk_err_word(const BatchKernel& k) {
+    return reinterpret_cast<int*>(static_cast<unsigned char*>(k.d_work) + k.work_bytes);
+}
+
+void batchk_free(BatchKernel* k) {
+    if (k->d_cases) cudaFree(k->d_cases);
+    if (k->d_segs) cudaFree(k->d_segs);
+    if (k->d_work) cudaFree(k->d_work);
+    *k = BatchKernel{};
+}
+
+}  // namespace prj

@@ -127,9 +127,6 @@ struct prj_plan {
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
     double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
     double* vd_ih = nullptr;      // 0.5 / rho (halo'd) of the variable-density step (scratch)
-    double* zcl_dcls = nullptr;   // class tables of the pivots for the cluster z kernel (prj_zcluster.cu)
-    double* zcl_ccls = nullptr;   // class tables of the back-substitution factors
-    int* zcl_pos = nullptr;       // position of each slot's line in its class row
     int z_planes = 0;             // planes per chunk of the per-wavenumber z kernels (0: their default)
     int z_stages = 0;             // stages of their copy rings (0: their default)
     double mixed_tau = 1e-3;      // FP64-row threshold of the mixed path
@@ -173,12 +170,6 @@ cudaError_t launch_zsolve_pipelined(const prj_plan* pl, int* err_word, cudaStrea
 // butterflies (prj_zline.cu); cudaErrorNotSupported when nz has no pass plan
 cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st);
 bool zline_supported(const prj_plan* pl);  // launch_zline would run (not fall back)
-// the same on a thread-block cluster of R_0 CTAs per x wavenumber (prj_zcluster.cu);
-// zcl_prepare builds its pivot class tables once (allocates; not under capture)
-bool zcl_supported(const prj_plan* pl);
-cudaError_t zcl_prepare(prj_plan* pl, cudaStream_t st);
-cudaError_t launch_zcl(const prj_plan* pl, cudaStream_t st);
-size_t zcl_smem(int nz, int yb, int ns);
 
 // x transforms with the in-place DIF FFT (prj_xfft.cu); used when pl->xd.ok
 // bout: also store the source field (divergence) there; accum: P += result; sq: norms of
@@ -237,6 +228,22 @@ cudaError_t launch_vd_correction(const prj_plan* pl, const double* P, const doub
                                  const double* Wh, const VdFields& f, const StepScalars& sc,
                                  const unsigned long long* slot, double* U, double* V, double* W, cudaStream_t st);
 double vd_rho_min_host(unsigned long long o);
+
+// Persistent batch kernel (prj_batchk.cu): FP64 solves of many plans from one work queue.
+struct BatchKernel {
+    void* d_cases = nullptr;   // per-case arguments
+    void* d_segs = nullptr;    // runs of work items in execution order
+    void* d_work = nullptr;    // item counter, per-case stage counters, error word
+    size_t work_bytes = 0;     // bytes of d_work reset before every launch (all but the error word)
+    size_t smem = 0;
+    int grid = 0, nseg = 0, ncases = 0;
+    long long nitems = 0;
+};
+bool batchk_supported(const prj_plan* pl);   // the plan's lengths are among the kernel's pass plans
+cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases, BatchKernel* out);
+cudaError_t batchk_launch(const BatchKernel& k, cudaStream_t st);
+int* batchk_err_word(const BatchKernel& k);
+void batchk_free(BatchKernel* k);
 
 // Sets the calling thread's prj_last_error_string() message and returns code.
 int record_error(int code, const char* msg);

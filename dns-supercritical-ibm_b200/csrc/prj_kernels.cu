@@ -273,7 +273,8 @@ __global__ void __launch_bounds__(512) k_zsolve(const ZArgs a) {
 // Thomas pivots of every (kx, kzs) line, poisson_solver_multigpu.f90:164-179:
 // D_0 = b_0 + lambda, D_k = (b_k + lambda) - a_k c'_{k-1}, c'_k = c_k / D_k.
 // Also reduces min |D| (min_abs_div_bacp, :181-197) into *minpiv (as bits).
-// pivc (may be null): the back-substitution factors c'_y = c_y / D_y of every line, the
+// minpiv[0] / minpiv[1] receive the smallest / largest |pivot| (as the bits of a
+// non-negative double).  pivc (may be null): the back-substitution factors c'_y = c_y / D_y of every line, the
 // quotients the backward sweep would otherwise form
 __global__ void k_build_pivots(int nh, int nzh, int mzp, int ny, const double* __restrict__ bands,
                                const double* __restrict__ ax, const double* __restrict__ az, double* piv,
@@ -295,18 +296,22 @@ __global__ void k_build_pivots(int nh, int nzh, int mzp, int ny, const double* _
     const double lam = __dadd_rn(ax[kx], az[t]);
     double D = __dadd_rn(Bb[0], lam);
     double cp = __ddiv_rn(C[0], D);
-    double mn = fabs(D);
+    double mn = fabs(D), mx = fabs(D);
     piv[((size_t)0 * nh + kx) * mzp + t] = D;
     if (pivc) pivc[((size_t)0 * nh + kx) * mzp + t] = cp;
     for (int y = 1; y < ny; y++) {
         D = __dsub_rn(__dadd_rn(Bb[y], lam), __dmul_rn(A[y], cp));
         cp = __ddiv_rn(C[y], D);
         mn = fmin(mn, fabs(D));
+        mx = fmax(mx, fabs(D));
         piv[((size_t)y * nh + kx) * mzp + t] = D;
         if (pivc) pivc[((size_t)y * nh + kx) * mzp + t] = cp;
     }
     if (mn == mn) atomicMin(minpiv, (unsigned long long)__double_as_longlong(mn));
     else atomicMin(minpiv, 0ull);  // NaN pivot: report 0
+    // the largest |pivot| (slot 1): the division of the forward sweeps needs every pivot
+    // within [2^-40, 2^1000] (div_rn.cuh); an infinite or NaN pivot reports +inf
+    atomicMax(minpiv + 1, (unsigned long long)__double_as_longlong(mx == mx ? mx : __longlong_as_double(0x7ff0000000000000ll)));
 }
 
 struct CorrArgs {
@@ -482,8 +487,8 @@ cudaError_t launch_build_pivots(const prj_plan* pl, cudaStream_t st) {
     const Geometry& g = pl->g;
     const int tot = g.nxh * g.mzp;
     unsigned long long* mp = reinterpret_cast<unsigned long long*>(pl->stat_buf);
-    const double big = 1e300;
-    cudaError_t e = cudaMemcpyAsync(mp, &big, sizeof(double), cudaMemcpyHostToDevice, st);
+    const double init[2] = {1e300, 0.0};  // running min and max of |pivot|
+    cudaError_t e = cudaMemcpyAsync(mp, init, sizeof(init), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
     k_build_pivots<<<(tot + 127) / 128, 128, 0, st>>>(g.nxh, g.nzh, g.mzp, g.ny, pl->t.bands, pl->t.ax, pl->t.az,
                                                       pl->t.piv, pl->t.pivc, mp);

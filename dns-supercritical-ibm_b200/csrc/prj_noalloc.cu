@@ -26,6 +26,7 @@
 #include <mutex>
 
 #include "../../include/projection.h"
+#include "div_rn.cuh"
 #include "prj_internal.h"
 
 namespace {
@@ -216,12 +217,16 @@ extern "C" int prj_poisson_fp64_noalloc(int nx, int nz, int ny, double dx, doubl
     // pivot table; its launcher also resets the min-pivot slot
     if ((e = prj::launch_build_pivots(&pl, st)) != cudaSuccess)
         return na_fail(PRJ_ERR_CUDA, "pivot table: %s", cudaGetErrorString(e));
-    double minpiv = 0.0;
-    if ((e = cudaMemcpyAsync(&minpiv, pl.stat_buf, sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+    double mm[2] = {0.0, 0.0};  // smallest and largest |pivot|
+    if ((e = cudaMemcpyAsync(mm, pl.stat_buf, sizeof(mm), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return na_fail(PRJ_ERR_CUDA, "pivot table: %s", cudaGetErrorString(e));
+    const double minpiv = mm[0];
     if (!(minpiv > 0) || !std::isfinite(minpiv))
         return na_fail(PRJ_ERR_NUMERIC, "zero or non-finite Thomas pivot (min_abs_div_bacp = %g)", minpiv);
+    if (!(minpiv >= prj::kDivRecipMinD) || !(mm[1] <= prj::kDivRecipMaxD))
+        return na_fail(PRJ_ERR_NUMERIC, "Thomas pivots |D| in [%g, %g] leave the range [2^-40, 2^1000] of the "
+                                        "correctly rounded division", minpiv, mm[1]);
     // the error word of the bounded device waits (the z kernel's copy pipeline): cleared
     // here, because the array keeps whatever the previous call left, and read back below
     int* err_word = reinterpret_cast<int*>(pl.stat_buf + prj::kStatErrSlot);

@@ -56,9 +56,20 @@ __device__ __forceinline__ double any_double(unsigned long long w, unsigned long
     return __longlong_as_double((long long)(((w >> 63) << 63) | (ex << 52) | mant));
 }
 
-// pairs of three kinds by index: u within 2^+-200 and D within 2^+-100 of 1 (the pivots
-// and spectra of a solve), both anywhere in the double range, and one of them near the
-// edges of the fast path's exponent window
+// a divisor anywhere in the pivot range of div_by_recip, |D| in [2^-40, 2^1000]: exponent
+// uniform in [-40, 999], one value in 32 exactly at a bound
+__device__ __forceinline__ double pivot_range_double(unsigned long long w, unsigned long long w2) {
+    const int sel = (int)((w2 >> 50) & 31);
+    const double sgn = (w >> 63) ? -1.0 : 1.0;
+    if (sel == 0) return sgn * kDivRecipMinD;
+    if (sel == 1) return sgn * kDivRecipMaxD;
+    return ldexp(random_double(w, w2, 0), -40 + (int)((w2 >> 8) % 1040ull));
+}
+
+// pairs of three kinds by index: u within 2^+-200 and D within 2^+-40 of 1 (the spectra
+// and pivots of a solve); u anywhere in the double range (zeros, subnormals, infinities,
+// NaNs) with D anywhere in the pivot range; and quotients near the bounds 2^-900 and
+// 2^1000 of the fast path's window
 __global__ void k_div_selftest(long long n, unsigned long long seed, unsigned long long* bad, double* first) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = seed * 0x100000000ull + (unsigned long long)i * 4;
@@ -68,19 +79,20 @@ __global__ void k_div_selftest(long long n, unsigned long long seed, unsigned lo
         case 0:
         case 1:
             u = random_double(wu, wu2, 200);
-            D = random_double(wd, wd2, 100);
+            D = random_double(wd, wd2, 40);
             break;
         case 2:
             u = any_double(wu, wu2);
-            D = any_double(wd, wd2);
+            D = pivot_range_double(wd, wd2);
             break;
         default: {
-            // exponents within 40 of the window's bounds: u near 2^-960 or 2^1020, D near
-            // 2^-1000 or 2^1000 (ldexp rounds to subnormals or infinities past the range)
-            const int eu = ((wu2 >> 40) & 1 ? 1020 : -960) + (int)((wu2 >> 41) % 81ull) - 40;
-            const int ed = ((wd2 >> 40) & 1 ? 1000 : -1000) + (int)((wd2 >> 41) % 81ull) - 40;
-            u = ldexp(random_double(wu, wu2, 0), eu);
-            D = ldexp(random_double(wd, wd2, 0), ed);
+            // u / D within 2^40 of 2^-900 or of 2^1000 (ldexp rounds to subnormals, zero or
+            // infinity past the double range)
+            D = pivot_range_double(wd, wd2);
+            int eD = 0;
+            frexp(D, &eD);
+            const int eq = ((wu2 >> 40) & 1 ? 1000 : -900) + (int)((wu2 >> 41) % 81ull) - 40;
+            u = ldexp(random_double(wu, wu2, 0), eq + eD - 1);
             break;
         }
         }

@@ -13,6 +13,7 @@
 #include "fft_dif.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
+#include "xfft_tiles.cuh"
 
 // minimum resident CTAs per SM requested for the shared-memory FFT kernels
 #ifndef PRJ_FFT_MINB
@@ -22,51 +23,6 @@
 namespace prj {
 
 namespace {
-
-#ifndef PRJ_X_UNROLL
-#define PRJ_X_UNROLL 4
-#endif
-constexpr int kUnroll = PRJ_X_UNROLL;  // items whose global loads are in flight per thread in the load phases
-// items per thread whose five field-row loads the divergence phase issues together
-constexpr int kDivUnroll = 2;
-
-__device__ __forceinline__ size_t hidx_d(int nx, int nz, int i, int j, int k) {
-    return (size_t)(i + 1) + (size_t)(nx + 2) * ((size_t)(j + 1) + (size_t)(nz + 2) * (size_t)(k + 1));
-}
-
-struct XArgs {
-    int nx, nz, ny, nh, m, tz, rs, even;
-    DifDev f;
-    const double2* tw;
-    const int* pos;
-    const double2* post;
-    const double* P;
-    const double* Uh;
-    const double* Vh;
-    const double* Wh;
-    const double* inv_dy_p;
-    double inv_dx, inv_dz, inv_dt, vbot, vtop, scale;
-    double2* X;      // FP64 rows kx < kxs: X[(y kxs + kx) nz + z]
-    float2* X32;     // FP32 rows kx >= kxs: X32[(y (nh - kxs) + kx - kxs) nz + z]
-    int kxs;         // nh on the FP64 path
-    int y0;          // first y plane of this launch (grid.y planes from y0)
-    double* psum;    // k_bwd_xp: per-CTA sums of the written P values, [y][blockIdx.x], or null
-    double* Pout;
-    double* Bout;    // k_fwd_xd: copy of the source field (P layout), or null
-    int accum;       // k_bwd_xd: Pout += result instead of Pout = result
-    double* sq;      // k_bwd_xd with accum: sq[0] += sum(update^2), sq[1] += sum(result^2), or null
-};
-
-__device__ __forceinline__ void spec_store(const XArgs& a, int y, int kx, int z, double2 v) {
-    if (kx < a.kxs) a.X[((size_t)y * a.kxs + kx) * a.nz + z] = v;
-    else a.X32[((size_t)y * (a.nh - a.kxs) + (kx - a.kxs)) * a.nz + z] = make_float2((float)v.x, (float)v.y);
-}
-
-__device__ __forceinline__ double2 spec_load(const XArgs& a, int y, int kx, int z) {
-    if (kx < a.kxs) return a.X[((size_t)y * a.kxs + kx) * a.nz + z];
-    const float2 f = a.X32[((size_t)y * (a.nh - a.kxs) + (kx - a.kxs)) * a.nz + z];
-    return make_double2(f.x, f.y);
-}
 
 // divergence at cell (i, j, k), mod_cfd_subroutines.f90:532-534 (periodic wrap in x and z,
 // V_hat walls from the step parameters); reference operation order, no contraction
@@ -268,219 +224,17 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_bwd_xd(const XArgs a) {
 // Rows at stride pass_row_stride(m) in shared memory.  nr = rows present in this
 // CTA (the last CTA may hold fewer).
 
-// k_fwd_xp: source (P, or the divergence of u_hat) -> packed complex -> DIF
-// passes -> split X_k, X_{m-k} -> transposed store.  SRC 0 reads P in the first
-// pass; SRC 1 stages the divergence in shared memory first.
+// k_fwd_xp / k_bwd_xp: one CTA per tile of the pass-plan x transforms (xfft_tiles.cuh)
 template <int SRC, class PL>
 __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_fwd_xp(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
-    double2* A = reinterpret_cast<double2*>(sm);
-    constexpr int m = PL::n, nx = 2 * m, rs = pass_row_stride(m);
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
-    const int nr = min(a.tz, a.nz - z0);
-    const double2* tw = a.tw;
-    if (SRC == 1) {
-        // divergence of the x pair (2e, 2e+1) of row z0 + r, as packed complex element e
-        // (the operation order of div_at).  Each field row is read as the aligned pair
-        // (interior 2e+1, 2e+2) -- halo'd positions 2e+2, 2e+3, 16-byte aligned because
-        // the halo'd row length nx + 2 is even -- and interior 2e comes from the lane
-        // holding item e-1 by shuffle (a scalar load where that lane holds another row
-        // or is outside the warp).  The periodic wrap u(nx) = u(0) is a scalar load.
-        const size_t hrow = (size_t)nx + 2, hplane = hrow * (size_t)(a.nz + 2);
-        const double idy = a.inv_dy_p[y];
-        const bool wb = (y == 0), wt = (y + 1 == a.ny);
-        const int total = nr * m;
-        const int lane = tid & 31;
-        const unsigned full = 0xffffffffu;
-        // all field loads of a group of kDivUnroll items are issued before any shuffle or
-        // arithmetic (measured at 768x384x384: 0.88 ms against 0.98 ms for loads interleaved
-        // with the arithmetic at 4 items, and 1.19 / 1.45 ms with 3 / 4 items grouped, which
-        // spill)
-        for (int base = tid - lane; base < total; base += kDivUnroll * nthr) {
-            double2 pu[kDivUnroll], pw0[kDivUnroll], pw1[kDivUnroll], pv0[kDivUnroll], pv1[kDivUnroll];
-#pragma unroll
-            for (int u = 0; u < kDivUnroll; u++) {
-                const int idx = base + u * nthr + lane;
-                const bool in = idx < total;
-                const int r = in ? idx / m : 0, e = in ? idx - r * m : 0;
-                const int z = z0 + r, zp = (z + 1 == a.nz) ? 0 : z + 1;
-                const size_t c0 = (size_t)(y + 1) * hplane + (size_t)(z + 1) * hrow + 1;
-                const size_t cz = (size_t)(y + 1) * hplane + (size_t)(zp + 1) * hrow + 1;
-                const size_t c1 = c0 + hplane;
-                pu[u] = pw0[u] = pw1[u] = pv0[u] = pv1[u] = make_double2(0.0, 0.0);
-                if (in) {
-                    pu[u] = *reinterpret_cast<const double2*>(a.Uh + c0 + 2 * e + 1);
-                    pw0[u] = *reinterpret_cast<const double2*>(a.Wh + c0 + 2 * e + 1);
-                    pw1[u] = *reinterpret_cast<const double2*>(a.Wh + cz + 2 * e + 1);
-                    if (!wb) pv0[u] = *reinterpret_cast<const double2*>(a.Vh + c0 + 2 * e + 1);
-                    if (!wt) pv1[u] = *reinterpret_cast<const double2*>(a.Vh + c1 + 2 * e + 1);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kDivUnroll; u++) {
-                const int idx = base + u * nthr + lane;
-                const bool in = idx < total;
-                const int r = in ? idx / m : 0, e = in ? idx - r * m : 0;
-                const int z = z0 + r, zp = (z + 1 == a.nz) ? 0 : z + 1;
-                const size_t c0 = (size_t)(y + 1) * hplane + (size_t)(z + 1) * hrow + 1;
-                const size_t cz = (size_t)(y + 1) * hplane + (size_t)(zp + 1) * hrow + 1;
-                const size_t c1 = c0 + hplane;
-                double u0 = __shfl_up_sync(full, pu[u].y, 1), w00 = __shfl_up_sync(full, pw0[u].y, 1);
-                double w10 = __shfl_up_sync(full, pw1[u].y, 1), v00 = __shfl_up_sync(full, pv0[u].y, 1);
-                double v10 = __shfl_up_sync(full, pv1[u].y, 1);
-                if (!in) continue;
-                if (lane == 0 || e == 0) {
-                    u0 = a.Uh[c0 + 2 * e];
-                    w00 = a.Wh[c0 + 2 * e];
-                    w10 = a.Wh[cz + 2 * e];
-                    if (!wb) v00 = a.Vh[c0 + 2 * e];
-                    if (!wt) v10 = a.Vh[c1 + 2 * e];
-                }
-                if (wb) v00 = a.vbot;
-                const double v01 = wb ? a.vbot : pv0[u].x;
-                if (wt) v10 = a.vtop;
-                const double v11 = wt ? a.vtop : pv1[u].x;
-                const double u1 = pu[u].x;
-                const double u2 = (e == m - 1) ? a.Uh[c0] : pu[u].y;
-                double s0 = __dmul_rn(__dsub_rn(u1, u0), a.inv_dx);
-                s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(w10, w00), a.inv_dz));
-                s0 = __dadd_rn(s0, __dmul_rn(__dsub_rn(v10, v00), idy));
-                double s1 = __dmul_rn(__dsub_rn(u2, u1), a.inv_dx);
-                s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(pw1[u].x, pw0[u].x), a.inv_dz));
-                s1 = __dadd_rn(s1, __dmul_rn(__dsub_rn(v11, v01), idy));
-                const double2 vv = make_double2(__dmul_rn(a.inv_dt, s0), __dmul_rn(a.inv_dt, s1));
-                if (a.Bout) {
-                    double* b = a.Bout + ((size_t)y * a.nz + z) * nx + 2 * e;
-                    b[0] = vv.x;
-                    b[1] = vv.y;
-                }
-                A[sidx<true>(r * rs + e)] = vv;
-            }
-        }
-        __syncthreads();
-        dif_passes_shared<-1, PL, 0, PL::P>(A, nr, rs, tw);
-    } else {
-        const double2* src = reinterpret_cast<const double2*>(a.P) + ((size_t)y * a.nz + z0) * m;
-        double2* bout = a.Bout ? reinterpret_cast<double2*>(a.Bout) + ((size_t)y * a.nz + z0) * m : nullptr;
-        dif_first_pass<-1, PL>(A, nr, rs, tw, [&](int r, int e) {
-            const double2 v = src[(size_t)r * m + e];
-            if (bout) bout[(size_t)r * m + e] = v;
-            return v;
-        });
-        __syncthreads();
-        dif_passes_shared<-1, PL, 1, PL::P>(A, nr, rs, tw);
-    }
-    // split: X_k = E_k + W^k O_k, X_{m-k} = conj(E_k) + W^{m-k} conj(O_k); row index fastest
-    constexpr int half = m / 2;
-    for (int idx = tid; idx < nr * (half + 1); idx += nthr) {
-        const int k = idx / nr, r = idx - k * nr;
-        const int base = r * rs;
-        const int z = z0 + r;
-        if (k == 0) {
-            const double2 c = A[sidx<true>(base)];
-            spec_store(a, y, 0, z, make_double2(c.x + c.y, 0.0));
-            spec_store(a, y, m, z, make_double2(c.x - c.y, 0.0));
-        } else {
-            const int kk = m - k;
-            const double2 zk = A[sidx<true>(base + pass_slot<PL>(k))];
-            const double2 zm = cconj(A[sidx<true>(base + pass_slot<PL>(kk))]);
-            const double2 e = cscale(cadd(zk, zm), 0.5);
-            const double2 d = csub(zk, zm);
-            const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
-            spec_store(a, y, k, z, cadd(e, cmul(a.post[k], o)));
-            if (kk != k) spec_store(a, y, kk, z, cadd(cconj(e), cmul(a.post[kk], cconj(o))));
-        }
-    }
+    fwd_xp_tile<SRC, PL>(a, sm, blockIdx.x, blockIdx.y);
 }
 
-// k_bwd_xp: transposed load of X_k, X_{m-k} -> inverse split (scaled) into slot
-// order -> DIT passes -> P rows (x pairs as double2), optionally accumulated.
 template <class PL>
 __global__ void __launch_bounds__(kPassThreads, PRJ_PASS_MINB) k_bwd_xp(const XArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
-    double2* A = reinterpret_cast<double2*>(sm);
-    constexpr int m = PL::n, rs = pass_row_stride(m), half = m / 2;
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int y = a.y0 + (int)blockIdx.y, z0 = blockIdx.x * a.tz;
-    const int nr = min(a.tz, a.nz - z0);
-    const double s = a.scale;
-    const int total = nr * (half + 1);
-    // X_k and X_{m-k} of kUnroll items loaded together (independent loads in flight)
-    for (int base0 = tid; base0 < total; base0 += kUnroll * nthr) {
-        double2 xa[kUnroll], xb[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-            const int idx = base0 + u * nthr;
-            if (idx < total) {
-                const int k = idx / nr, r = idx - k * nr;
-                xa[u] = spec_load(a, y, k, z0 + r);
-                xb[u] = spec_load(a, y, m - k, z0 + r);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-            const int idx = base0 + u * nthr;
-            if (idx >= total) continue;
-            const int k = idx / nr, r = idx - k * nr;
-            const int base = r * rs;
-            if (k == 0) {
-                const double x0 = xa[u].x, xm = xb[u].x;
-                A[sidx<true>(base)] = make_double2((x0 + xm) * s, (x0 - xm) * s);
-            } else {
-                const int kk = m - k;
-                const double2 xk = xa[u], xkk = xb[u];
-                const double2 e1 = cadd(xk, cconj(xkk));
-                const double2 o1 = cmulc(csub(xk, cconj(xkk)), a.post[k]);
-                A[sidx<true>(base + pass_slot<PL>(k))] = cscale(make_double2(e1.x - o1.y, e1.y + o1.x), s);
-                if (kk != k) {
-                    const double2 e2 = cadd(xkk, cconj(xk));
-                    const double2 o2 = cmulc(csub(xkk, cconj(xk)), a.post[kk]);
-                    A[sidx<true>(base + pass_slot<PL>(kk))] = cscale(make_double2(e2.x - o2.y, e2.y + o2.x), s);
-                }
-            }
-        }
-    }
-    __syncthreads();
-    dit_passes_shared<+1, PL, PL::P - 1, 0>(A, nr, rs, a.tw);
-    double2* out = reinterpret_cast<double2*>(a.Pout) + ((size_t)y * a.nz + z0) * m;
-    double sq0 = 0.0, sq1 = 0.0, ps = 0.0;
-    dit_last_pass<+1, PL>(A, nr, rs, a.tw, [&](int r, int e, double2 v) {
-        double2* o = out + (size_t)r * m + e;
-        if (a.accum) {
-            const double2 old = *o;
-            const double2 nv = make_double2(old.x + v.x, old.y + v.y);
-            sq0 += v.x * v.x + v.y * v.y;
-            sq1 += nv.x * nv.x + nv.y * nv.y;
-            ps += nv.x + nv.y;
-            *o = nv;
-        } else {
-            ps += v.x + v.y;
-            *o = v;
-        }
-    });
-    if (a.psum) {
-        // the tile's sum in a fixed order (per thread, then warp butterfly, then warps in order)
-        __shared__ double wsum[kPassThreads / 32];
-        for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
-        if ((tid & 31) == 0) wsum[tid >> 5] = ps;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < nthr / 32; w++) t += wsum[w];
-            a.psum[(size_t)y * gridDim.x + blockIdx.x] = t;
-        }
-    }
-    if (a.sq) {
-        for (int o = 16; o > 0; o >>= 1) {
-            sq0 += __shfl_xor_sync(0xffffffffu, sq0, o);
-            sq1 += __shfl_xor_sync(0xffffffffu, sq1, o);
-        }
-        if ((tid & 31) == 0) {
-            atomicAdd(a.sq, sq0);
-            atomicAdd(a.sq + 1, sq1);
-        }
-    }
+    bwd_xp_tile<PL>(a, sm, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 XArgs make_args(const prj_plan* pl) {
@@ -497,6 +251,20 @@ XArgs make_args(const prj_plan* pl) {
     a.kxs = pl->kxs;
     return a;
 }
+
+}  // namespace
+
+XArgs batch_x_args(const prj_plan* pl, double* P) {
+    XArgs a = make_args(pl);
+    a.tz = pl->tz_xp;
+    a.y0 = 0;
+    a.P = P;
+    a.Pout = P;
+    a.scale = 1.0 / ((double)pl->g.nx * (double)pl->g.nz + 0.0);
+    return a;
+}
+
+namespace {
 
 size_t smem_bytes(const XArgs& a) {
     return (size_t)padded_len(a.tz * a.rs, true) * sizeof(double2) + (size_t)a.m * sizeof(int);

@@ -21,6 +21,7 @@
 #include "div_rn.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
+#include "zsplit_tiles.cuh"
 
 // minimum resident CTAs per SM requested for the shared-memory FFT kernels
 #ifndef PRJ_FFT_MINB
@@ -31,18 +32,12 @@ namespace prj {
 
 namespace {
 
-struct ZfftArgs {
-    int nrow_total;  // rows of length nz in this buffer (ny * rows per plane)
-    int nz, rb;      // rows per CTA
-    DifDev f;
-    const double2* tw;
-    void* X;         // double2 (FP64 storage) or float2 (FP32 storage) rows
-};
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
-__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
-__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
-__device__ __forceinline__ void from_d2(double2& o, double2 v) { o = v; }
-__device__ __forceinline__ void from_d2(float2& o, double2 v) { o = make_float2((float)v.x, (float)v.y); }
 
 // T: storage type of the spectrum rows (arithmetic is FP64 in shared memory)
 template <int DIR, typename T>
@@ -74,140 +69,11 @@ __global__ void __launch_bounds__(256, PRJ_FFT_MINB) k_zfft(const ZfftArgs a) {
     for (int i = tid; i < tot; i += nthr) from_d2(dst[i], zs[sidx<true>(i)]);
 }
 
-// Pass-plan z transform (fft_pass.cuh): the first pass reads the rows from global
-// memory, the last writes them back; rb rows per CTA, kPassThreads threads.
-// resident CTAs per SM asked of the pass-plan z kernels (measured at 768x384x384: 5 gives
-// the forward z 0.300 ms against 0.345 ms at 6, the x kernels' setting)
-#ifndef PRJ_ZPASS_MINB
-#define PRJ_ZPASS_MINB 5
-#endif
-
+// k_zfft_pass: one CTA per group of rb rows (zsplit_tiles.cuh)
 template <int DIR, typename T, class PL, bool STAGE_INV = false>
 __global__ void __launch_bounds__(kPassThreads, PRJ_ZPASS_MINB) k_zfft_pass(const ZfftArgs a) {
     extern __shared__ __align__(16) double2 zp[];
-    constexpr int n = PL::n;
-    const size_t row0 = (size_t)blockIdx.x * a.rb;
-    const int nr = (int)min((size_t)a.rb, (size_t)a.nrow_total - row0);
-    T* X = static_cast<T*>(a.X) + row0 * n;
-    const double2* tw = a.tw;
-    // the forward transform's slot-order rows leave shared memory in whole coalesced
-    // rows (its last pass would store R contiguous elements per thread: half-sector
-    // writes per instruction); the inverse copies them in whole rows the same way
-    // (STAGE_INV) or reads them in its first pass
-    const int tot = nr * n;
-    if (DIR < 0) {
-        dif_first_pass<-1, PL>(zp, nr, n, tw, [&](int r, int e) { return to_d2(X[(size_t)r * n + e]); });
-        __syncthreads();
-        dif_passes_shared<-1, PL, 1, PL::P>(zp, nr, n, tw);
-        for (int i = threadIdx.x; i < tot; i += blockDim.x) from_d2(X[i], zp[sidx<true>(i)]);
-    } else {
-        if (STAGE_INV) {
-            // slot-order rows copied in whole (coalesced), every pass in shared memory
-#pragma unroll 4
-            for (int i = threadIdx.x; i < tot; i += blockDim.x) zp[sidx<true>(i)] = to_d2(X[i]);
-            __syncthreads();
-            dit_passes_shared<+1, PL, PL::P - 1, 0>(zp, nr, n, tw);
-        } else {
-            dit_first_pass<+1, PL>(zp, nr, n, [&](int r, int q) { return to_d2(X[(size_t)r * n + q]); });
-            __syncthreads();
-            dit_passes_shared<+1, PL, PL::P - 2, 0>(zp, nr, n, tw);
-        }
-        dit_last_pass<+1, PL>(zp, nr, n, tw, [&](int r, int e, double2 v) { from_d2(X[(size_t)r * n + e], v); });
-    }
-}
-
-struct ThomasArgs {
-    int nz, ny, nh, mzp, tiles;  // tiles of kThomasTile slots per kx
-    int nhb, kx0;                // rows per plane in this buffer; its first kx
-    const double* bands;         // a, b, c, a00, b00, c00
-    const double* piv;           // D[y][kx][kzs], kx over all nh rows
-    const double* pivc;          // c'[y][kx][kzs] = c_y / D_y, same layout
-    const int* kz_of_slot;       // wavenumber held by each slot
-    void* X;                     // T rows [y][kx - kx0][slot]
-};
-
-constexpr int kThomasTile = 128;
-#ifndef PRJ_THOMAS_BLOCK
-#define PRJ_THOMAS_BLOCK 8
-#endif
-constexpr int kBlock = PRJ_THOMAS_BLOCK;  // planes loaded together (independent loads in flight)
-
-// One line: the CTA's block index `blk` within the buffer a.X (T storage).
-template <typename T>
-__device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
-    const int kb = blk / a.tiles;  // row within this buffer
-    const int kx = a.kx0 + kb;
-    const int slot = (blk - kb * a.tiles) * kThomasTile + threadIdx.x;
-    if (slot >= a.nz) return;
-    const int nz = a.nz, ny = a.ny, nh = a.nh, mzp = a.mzp;
-    const int kz = a.kz_of_slot[slot];
-    const int kzs = kz <= nz - kz ? kz : nz - kz;
-    const bool is00 = (kx == 0 && kz == 0);
-    const double* A = a.bands + (is00 ? 3 : 0) * ny;
-    const size_t rstride = (size_t)a.nhb * nz;  // X: next y plane
-    const size_t pstride = (size_t)nh * mzp;     // D: next y plane
-    T* x = static_cast<T*>(a.X) + (size_t)kb * nz + slot;
-    const double* d = a.piv + (size_t)kx * mzp + kzs;
-    const double* dc = a.pivc + (size_t)kx * mzp + kzs;
-
-    // forward sweep, y ascending
-    double2 prev = make_double2(0.0, 0.0);
-    for (int y0 = 0; y0 < ny; y0 += kBlock) {
-        double2 v[kBlock];
-        double D[kBlock], av[kBlock];
-#pragma unroll
-        for (int u = 0; u < kBlock; u++) {
-            const int y = y0 + u;
-            if (y < ny) {
-                v[u] = to_d2(x[(size_t)y * rstride]);
-                D[u] = d[(size_t)y * pstride];
-                av[u] = A[y];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kBlock; u++) {
-            const int y = y0 + u;
-            if (y < ny) {
-                double2 r = v[u];
-                const double rD = __drcp_rn(D[u]);  // off the recurrence's chain
-                if (y == 0) {
-                    r.x = div_by_recip(r.x, D[u], rD);
-                    r.y = div_by_recip(r.y, D[u], rD);
-                } else {
-                    r.x = div_by_recip(__dsub_rn(r.x, __dmul_rn(av[u], prev.x)), D[u], rD);
-                    r.y = div_by_recip(__dsub_rn(r.y, __dmul_rn(av[u], prev.y)), D[u], rD);
-                }
-                prev = r;
-                if (y < ny - 1) from_d2(x[(size_t)y * rstride], r);
-            }
-        }
-    }
-    // backward sweep, y descending; prev holds d'_{ny-1} = x_{ny-1}
-    from_d2(x[(size_t)(ny - 1) * rstride], prev);
-    for (int y1 = ny - 2; y1 >= 0; y1 -= kBlock) {
-        double2 v[kBlock];
-        double cp[kBlock];
-#pragma unroll
-        for (int u = 0; u < kBlock; u++) {
-            const int y = y1 - u;
-            if (y >= 0) {
-                v[u] = to_d2(x[(size_t)y * rstride]);
-                cp[u] = dc[(size_t)y * pstride];  // c_y / D_y, tabulated with the pivots
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kBlock; u++) {
-            const int y = y1 - u;
-            if (y >= 0) {
-                const double c = cp[u];
-                double2 r;
-                r.x = __dsub_rn(v[u].x, __dmul_rn(prev.x, c));
-                r.y = __dsub_rn(v[u].y, __dmul_rn(prev.y, c));
-                prev = r;
-                from_d2(x[(size_t)y * rstride], r);
-            }
-        }
-    }
+    zfft_pass_tile<DIR, T, PL, STAGE_INV>(a, zp, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,12 +250,6 @@ __global__ void __launch_bounds__(kThomasTile) k_thomas_mixed(const ThomasArgs a
     else thomas_line<float2>(a32, blockIdx.x - nblk64);
 }
 
-template <typename K>
-cudaError_t allow_smem(K kernel, size_t bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
 }  // namespace
 
 // rows per CTA of the pass-plan kernels: the requested count, else the largest
@@ -481,6 +341,18 @@ cudaError_t launch_zfft_t(const prj_plan* pl, int dir, void* X, int rows_per_pla
         k_zfft<+1, T><<<grid, 256, smem, st>>>(a);
     }
     return cudaGetLastError();
+}
+
+ZfftArgs batch_z_args(const prj_plan* pl) {
+    const Geometry& g = pl->g;
+    ZfftArgs a{};
+    a.nrow_total = g.ny * g.nxh;
+    a.nz = g.nz;
+    a.f = pl->zd.f;
+    a.tw = pl->zd.tw;
+    a.X = pl->spec;
+    a.rb = pass_rows(g.nz, pl->zfft_rows);
+    return a;
 }
 
 ThomasArgs thomas_args(const prj_plan* pl, void* X, int kx0, int rows_per_plane) {

@@ -50,7 +50,7 @@ EXPORTS = (
     "prj_bands_from_yu", "prj_metrics_from_yu",
     "prj_plan_enable_stage_timing", "prj_plan_stage_times", "prj_stage_name",
     "prj_poisson_fp64_noalloc", "prj_poisson_mixed",
-    "prj_batch_create", "prj_batch_launch", "prj_batch_destroy",
+    "prj_batch_create", "prj_batch_launch", "prj_batch_destroy", "prj_batch_info", "prj_batch_check_error",
     "prj_plan_get_tuning", "prj_plan_set_tuning",
     "prj_vd_metric_from_yu", "prj_plan_set_vd_metric", "prj_projection_step_vd",
     "prj_field_read_header", "prj_field_read", "prj_field_write", "prj_field_read_device",
@@ -165,6 +165,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.prj_batch_create.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(_vp), i, i, ctypes.POINTER(_vp)]
     L.prj_batch_launch.argtypes = [_vp, _vp]
     L.prj_batch_destroy.argtypes = [_vp]
+    L.prj_batch_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_longlong)]
+    L.prj_batch_check_error.argtypes = [_vp, _vp]
     L.prj_plan_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_plan_set_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.prj_vd_metric_from_yu.argtypes = [i, _dp, _dp]
@@ -593,8 +596,10 @@ def read_field(path, out=None, halo=False):
 
 
 class Batch:
-    """Many independent in-place Poisson solves replayed as one CUDA graph launch
-    (prj_batch_create / prj_batch_launch).  Case i solves plans[i] on tensors[i]."""
+    """Many independent in-place Poisson solves in one launch (prj_batch_create /
+    prj_batch_launch): one persistent kernel over a work queue for FP64 cases of the
+    pass-plan lengths up to 256, else one CUDA graph.  Case i solves plans[i] on
+    tensors[i]."""
 
     def __init__(self, plans, tensors, mode=MODE_FP64):
         if len(plans) != len(tensors) or not plans:
@@ -610,6 +615,18 @@ class Batch:
 
     def launch(self, stream=None):
         _check(load_library().prj_batch_launch(self._h, _stream_ptr(stream)))
+
+    @property
+    def info(self) -> dict:
+        """{"persistent", "kernels_per_launch", "work_items"} (prj_batch_info)."""
+        p, k, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        _check(load_library().prj_batch_info(self._h, ctypes.byref(p), ctypes.byref(k), ctypes.byref(w)))
+        return {"persistent": bool(p.value), "kernels_per_launch": k.value, "work_items": w.value}
+
+    def check_error(self, stream=None):
+        """Raise PrjError(PRJ_ERR_TIMEOUT) if a bounded wait of the persistent kernel gave up
+        (prj_batch_check_error; waits for the stream)."""
+        _check(load_library().prj_batch_check_error(self._h, _stream_ptr(stream)))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -184,6 +184,46 @@ def nccl_plane_exchange(dist, rank: int, world: int, stream=None):
     return ex
 
 
+def host_staged_exchange(dist, stream=None):
+    """The all-to-all of ``DistSolve`` through host memory: the device send buffer is copied
+    to the host, exchanged with ``all_to_all_single`` over the process group (gloo between
+    processes that may share a GPU, or hosts without a GPU interconnect), and the received
+    blocks are copied back; the copies are ordered on ``stream`` (the current stream if
+    None) and the collective waits for them on the host."""
+    import torch
+
+    def ex(out, inp, out_splits, in_splits):
+        s = stream or torch.cuda.current_stream(out.device)
+        with torch.cuda.stream(s):
+            h_in = inp[:sum(in_splits)].to("cpu")  # synchronous: the collective needs the data
+            h_out = torch.empty(sum(out_splits), dtype=out.dtype)
+            dist.all_to_all_single(h_out, h_in, out_splits, in_splits)
+            out[:sum(out_splits)].copy_(h_out)
+    return ex
+
+
+def host_staged_plane_exchange(dist, rank: int, world: int, stream=None):
+    """``nccl_plane_exchange`` through host memory (see ``host_staged_exchange``)."""
+    import torch
+
+    def ex(P_ext):
+        s = stream or torch.cuda.current_stream(P_ext.device)
+        with torch.cuda.stream(s):
+            h = P_ext[[0, -1]].to("cpu")
+            prev = h[0].clone()
+            ops = []
+            if rank + 1 < world:
+                ops.append(dist.P2POp(dist.isend, h[1].contiguous(), rank + 1))
+            if rank > 0:
+                ops.append(dist.P2POp(dist.irecv, prev, rank - 1))
+            if ops:
+                for w in dist.batch_isend_irecv(ops):
+                    w.wait()
+            if rank > 0:
+                P_ext[0].copy_(prev)
+    return ex
+
+
 def project_emulated(plans, Uh, Vh, Wh, U, V, W, P, params, world: int):
     """The projection step of ``world`` ranks emulated on one device (one plan per rank,
     in-process exchanges).  Halo'd tensors are (ny+2, nz+2, nx+2) with filled halos, P is

@@ -268,16 +268,30 @@ int prj_geom_read_metrics(const char* geom_dir, int ny, double* inv_dy_p, double
 int prj_geom_read_base_params(const char* path, prj_case_params* out);
 
 /*
- * Batched solves: one CUDA graph holding every case (case i solves plans[i] in
- * place on the device array d_P[i], FP64 or PRJ_MODE_FP32_REFINE), the cases
- * on parallel graph branches, replayed by one graph launch.  The plans must be
- * distinct (a plan's scratch serves one solve at a time) and outlive the batch;
- * the arrays are bound at creation.  No counterpart in the reference, which
- * solves one grid per run.
+ * Batched solves: case i solves plans[i] in place on the device array d_P[i].
+ * The plans must be distinct (a plan's scratch serves one solve at a time) and
+ * outlive the batch; the arrays are bound at creation; the plans' tuning must not
+ * change while the batch exists.  No counterpart in the reference, which solves
+ * one grid per run (and plans it once, poisson_solver_multigpu.f90:77-129).
+ *   FP64, every case with even nx, nx/2 and nz among the pass-plan lengths up to
+ *   256 (16, 24, 32, 48, 64, 96, 128, 192, 256): one persistent kernel runs all
+ *   cases from a work queue of (case, stage, tile) items in stage-major order,
+ *   with bounded waits on per-case stage counters; prj_batch_launch issues a
+ *   counter reset and that one kernel (both capturable in a CUDA graph).
+ *   Otherwise (FP32 + refinement, other lengths): one CUDA graph holding every
+ *   case's kernels on parallel branches, replayed by one graph launch.
+ * Each case's P equals its own prj_poisson_fp64 / prj_poisson_mixed bit for bit.
+ * prj_batch_info: whether the batch is persistent, its kernel launches per
+ * prj_batch_launch, and its work items.  prj_batch_check_error waits for
+ * `stream`, returns PRJ_ERR_TIMEOUT if a bounded wait of the persistent kernel
+ * gave up since the last check (that launch's results are not valid), and clears
+ * the word.
  */
 typedef struct prj_batch prj_batch;
 int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int mode, prj_batch** out);
 int prj_batch_launch(prj_batch* batch, void* stream);
+int prj_batch_info(const prj_batch* batch, int* persistent, int* kernels_per_launch, long long* work_items);
+int prj_batch_check_error(prj_batch* batch, void* stream);
 int prj_batch_destroy(prj_batch* batch);
 
 /*
@@ -291,11 +305,9 @@ int prj_batch_destroy(prj_batch* batch);
  *   z_mode      0 = z FFT / Thomas / inverse z FFT as three kernels, 1 = one fused
  *               pipelined kernel per x wavenumber (runtime radices; the kernel of z
  *               lengths with a prime factor above 5), 2 = its unpipelined form,
- *               3 = one kernel per x wavenumber on the compile-time pass plans,
- *               4 = the same on a thread-block cluster of R_0 CTAs per x wavenumber
- *               (R_0 the plan's first radix); 3 and 4 run the three kernels where nz
- *               has no pass plan.  The default is 3 when nx/2+1 >= 2 x the SM count,
- *               else 0;
+ *               3 = one kernel per x wavenumber on the compile-time pass plans (the
+ *               three kernels where nz has no pass plan).  The default is 3 when
+ *               nx/2+1 >= 2 x the SM count, else 0;
  *   z_planes    planes per chunk of the per-wavenumber z kernels (0 = default);
  *   z_stages    stages of their copy rings (0 = default, else 2..4; 2..8 for mode 1);
  *   thomas_ring shared-memory ring of the split Thomas kernel: -1 = default (the
@@ -305,9 +317,9 @@ int prj_batch_destroy(prj_batch* batch);
  *   mixed_tau   x-wavenumber rows with |a_x| < mixed_tau max|b| keep FP64 storage in
  *               the mixed path (default 1e-3; must lie in (0, 1)).
  * prj_plan_set_tuning rejects values out of range and shapes that do not fit
- * shared memory; it may allocate (tables of z_mode 4, the mixed path's FP32
- * spectrum after a change of mixed_tau), so call it outside stream capture.
- * The environment variables PRJ_ZSOLVE (split|fused|basic|line|cluster),
+ * shared memory; it may free and later reallocate the mixed path's FP32 spectrum
+ * (after a change of mixed_tau), so call it outside stream capture.
+ * The environment variables PRJ_ZSOLVE (split|fused|basic|line),
  * PRJ_FFT_KERNELS=runtime and PRJ_THOMAS_ASYNC are read once, at plan creation,
  * as test hooks for the defaults.
  */
@@ -332,11 +344,12 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
 int prj_selftest_wait_timeout(int device, long long budget_cycles);
 
 /* Diagnostic of the division the Thomas forward sweeps use: n pseudo-random pairs
- * (u, D) from `seed` (half with exponents within 2^+-200 and 2^+-100 of 1, a quarter
- * anywhere in the double range -- zeros, subnormals, infinities and NaNs included -- and
- * a quarter near the bounds of the fast path's exponent window; random and edge
- * mantissas), each divided both by __ddiv_rn and by the reciprocal-and-correction form
- * of div_rn.cuh; *mismatches counts the pairs whose two results differ in any bit
+ * (u, D) from `seed` -- half with u within 2^+-200 and D within 2^+-40 of 1, a quarter
+ * with u anywhere in the double range (zeros, subnormals, infinities and NaNs
+ * included), a quarter with quotients near the bounds of the fast path's exponent
+ * window; D always within the pivot range [2^-40, 2^1000] that plan creation enforces;
+ * random and edge mantissas -- each divided both by __ddiv_rn and by the
+ * reciprocal-and-correction form of div_rn.cuh; *mismatches counts the pairs whose two results differ in any bit
  * (the first such pair in first_u, first_d when not NULL).  No counterpart in the
  * reference. */
 int prj_selftest_division(int device, long long n, unsigned long long seed, long long* mismatches,

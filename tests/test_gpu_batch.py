@@ -1,5 +1,6 @@
-"""GPU tests of the batched form (many uneven solves in one CUDA graph launch)
-and of the launch-shape autotuner."""
+"""GPU tests of the batched form (many uneven solves in one launch: the persistent
+work-queue kernel for FP64 cases of the pass-plan lengths up to 256, else one CUDA
+graph) and of the launch-shape autotuner."""
 import numpy as np
 import pytest
 
@@ -48,6 +49,65 @@ def test_batch_equals_single_solves(cuda_device):
     for a, b, c in zip(first, (from_dev(t) for t in tensors), singles):
         np.testing.assert_array_equal(a, b)
         np.testing.assert_array_equal(a, from_dev(c))
+    for p in plans:
+        p.close()
+
+
+PERSISTENT_SHAPES = [(64, 48, 64), (96, 64, 128), (128, 96, 96), (256, 48, 64), (192, 128, 256), (32, 5, 16),
+                     (512, 21, 192), (48, 33, 24)]
+
+
+def _cases(shapes, seed):
+    import prj
+    import workloads
+    rng = np.random.default_rng(seed)
+    out = []
+    for nx, ny, nz in shapes:
+        rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, beta=rng.uniform(1.5, 2.5), seed=int(rng.integers(1 << 30)))
+        out.append((rhs, yu, dx, dz, prj.bands(yu, "reference")))
+    return out
+
+
+def test_persistent_batch_equals_single_solves(cuda_device, oracle):
+    """One kernel launch per batch; every case bitwise equal to its own solve, on two launches
+    in a row (the work counters reset with each launch), and within 1e-12 of the oracle."""
+    import prj
+    import torch
+    cases = _cases(PERSISTENT_SHAPES, 7)
+    plans = [prj.Plan(r.shape[0], r.shape[1], r.shape[2], dx, dz, b) for r, _, dx, dz, b in cases]
+    singles = []
+    for p, (r, *_rest) in zip(plans, cases):
+        t = to_dev(r)
+        p.poisson_fp64(t)
+        singles.append(from_dev(t))
+    tensors = [to_dev(r) for r, *_ in cases]
+    with prj.Batch(plans, tensors) as batch:
+        info = batch.info
+        assert info["persistent"] and info["kernels_per_launch"] == 1 and info["work_items"] > len(cases)
+        for rep in range(2):
+            for t, (r, *_rest) in zip(tensors, cases):
+                t.copy_(to_dev(r))
+            batch.launch()
+            batch.check_error()
+            for t, want in zip(tensors, singles):
+                np.testing.assert_array_equal(from_dev(t), want)
+    for (r, _, dx, dz, b), got in zip(cases, singles):
+        Po, _ = oracle.poisson(r, dx, dz, b)
+        assert rel_l2(got, Po) <= 1e-12
+    for p in plans:
+        p.close()
+    torch.cuda.synchronize()
+
+
+def test_graph_batch_for_other_lengths(cuda_device):
+    """A case outside the persistent kernel's lengths (nx/2 = 15) keeps the graph form."""
+    import prj
+    cases = make_cases()
+    plans = [prj.Plan(r.shape[0], r.shape[1], r.shape[2], dx, dz, b) for r, _, dx, dz, b in cases]
+    tensors = [to_dev(r) for r, *_ in cases]
+    with prj.Batch(plans, tensors) as batch:
+        info = batch.info
+        assert not info["persistent"] and info["kernels_per_launch"] >= len(cases)
     for p in plans:
         p.close()
 
