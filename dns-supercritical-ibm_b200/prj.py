@@ -59,6 +59,7 @@ EXPORTS = (
     "prj_dist_forward", "prj_dist_pack", "prj_dist_thomas", "prj_dist_unpack", "prj_dist_inverse",
     "prj_dist_divergence", "prj_dist_correct", "prj_selftest_division", "prj_plan_check_error",
     "prj_geom_read_column", "prj_geom_read_bands", "prj_geom_read_metrics", "prj_geom_read_base_params",
+    "prj_synth_channel_predictor",
 )
 
 BANDS_REFERENCE = 0
@@ -150,6 +151,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
                                            ctypes.POINTER(Stats)]
     L.prj_plan_min_pivot.argtypes = [_vp, _dp]
     L.prj_plan_check_error.argtypes = [_vp, _vp]
+    L.prj_synth_channel_predictor.argtypes = [i, i, i, _vp, ctypes.c_ulonglong, d, _vp, _vp, _vp, _vp]
     L.prj_geom_read_column.argtypes = [ctypes.c_char_p, i, i, i, _dp]
     L.prj_geom_read_bands.argtypes = [ctypes.c_char_p, i, _dp, _dp, _dp, _dp, _dp, _dp]
     L.prj_geom_read_metrics.argtypes = [ctypes.c_char_p, i, _dp, _dp, _dp]
@@ -252,6 +254,16 @@ def bands(yu, mode="reference"):
     m = {"reference": BANDS_REFERENCE, "consistent": BANDS_CONSISTENT}[mode]
     _check(load_library().prj_bands_from_yu(ny, _p(yu), m, *[_p(v) for v in out]))
     return tuple(out)
+
+
+def synth_predictor(Uh, Vh, Wh, yp, seed, sigma=0.1, stream=None):
+    """Channel predictor of `seed` in place on halo'd [y+2, z+2, x+2] CUDA tensors
+    (prj_synth_channel_predictor): Poiseuille profile over the cell centres yp (CUDA
+    tensor, ny values) plus N(0, sigma) noise, v = 0 on the bottom wall face."""
+    ny, nz, nx = Uh.shape[0] - 2, Uh.shape[1] - 2, Uh.shape[2] - 2
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    _check(load_library().prj_synth_channel_predictor(nx, nz, ny, p(yp), int(seed) & (2 ** 64 - 1), float(sigma),
+                                                      p(Uh), p(Vh), p(Wh), _stream_ptr(stream)))
 
 
 def vd_metric(yu):

@@ -5,7 +5,8 @@ a channel case of some size and carries its own predictor field, in one of two
 forms:
 
 * ``seed``: the predictor u_hat is produced on the device from the request's
-  seed (a channel profile plus seeded N(0, 0.1) noise, v = 0 at the walls).  This
+  seed in one pass (prj_synth_channel_predictor: a channel profile plus N(0, 0.1)
+  noise that is a fixed function of the seed, v = 0 on the bottom wall face).  This
   is how a DNS time loop hands the projection its input: the momentum step leaves
   u_hat in device memory (src/main.f90:386-393 calls the projection on it);
 * ``fields``: host arrays (Uh, Vh, Wh) in the reference's halo'd Fortran layout,
@@ -88,21 +89,12 @@ def poisson_arrivals(rate_hz: float, duration_s: float, seed: int = 3, sizes=SER
     return out
 
 
-def device_predictor(Uh, Vh, Wh, yp, seed):
-    """The channel predictor of one request in place on the device, deterministic in
-    `seed`: U = 1.5 (1 - (y-1)^2) + N(0, 0.1), V, W = N(0, 0.1) (drawn in the order U,
-    V, W), V = 0 on the bottom wall face; halo'd [y+2, z+2, x+2] tensors, interior only
-    (the projection reads no halo of its inputs)."""
-    import torch
-    ny, nz, nx = Uh.shape[0] - 2, Uh.shape[1] - 2, Uh.shape[2] - 2
-    g = torch.Generator(device=Uh.device)
-    g.manual_seed(int(seed))
-    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
-    Uh[inner] = torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=Uh.device).mul_(0.1).add_(
-        1.5 * (1 - (yp.view(-1, 1, 1) - 1) ** 2))
-    Vh[inner] = torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=Uh.device).mul_(0.1)
-    Wh[inner] = torch.randn((ny, nz, nx), generator=g, dtype=torch.float64, device=Uh.device).mul_(0.1)
-    Vh[1] = 0.0
+def device_predictor(Uh, Vh, Wh, yp, seed, stream=None):
+    """The channel predictor of one request in place on the device, a fixed function of
+    `seed` (prj_synth_channel_predictor: U = 1.5 (1 - (y-1)^2) + N(0, 0.1), V, W = N(0, 0.1),
+    V = 0 on the bottom wall face); halo'd [y+2, z+2, x+2] tensors, interior only (the
+    projection reads no halo of its inputs)."""
+    prj.synth_predictor(Uh, Vh, Wh, yp, seed, 0.1, stream=stream)
 
 
 class ProjectionServer:
@@ -207,12 +199,12 @@ class ProjectionServer:
         """The request's work on the slot's stream: its input, the projection step, its output."""
         torch = self.torch
         Uh, Vh, Wh, U, V, W, P = slot.fields
-        with torch.cuda.stream(slot.stream):
-            if req.fields is not None:
+        if req.fields is not None:
+            with torch.cuda.stream(slot.stream):
                 for d, h in zip((Uh, Vh, Wh), req.fields):
                     d.copy_(torch.from_numpy(h.T), non_blocking=True)
-            else:
-                device_predictor(Uh, Vh, Wh, slot.yp, req.seed)
+        else:
+            device_predictor(Uh, Vh, Wh, slot.yp, req.seed, stream=slot.stream)
         slot.plan.projection_step(Uh, Vh, Wh, U, V, W, P, self.dt, mode=self.mode, stats=False, stream=slot.stream)
         if req.want == "host":
             with torch.cuda.stream(slot.stream):

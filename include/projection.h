@@ -485,6 +485,17 @@ int prj_dist_correct(prj_plan* plan, const double* d_P_ext, const double* d_Uh_l
  * statistics performs the same check. */
 int prj_plan_check_error(prj_plan* plan, void* stream);
 
+/* Synthetic channel predictor on the device, for benchmarks, tests and served
+ * requests that name their field by a seed (no counterpart in the reference, whose
+ * predictor comes from its momentum step): on the interior of the halo'd arrays
+ * u_hat = 1.5 (1 - (yp_k - 1)^2) + sigma n, v_hat = sigma n, w_hat = sigma n, and
+ * v_hat = 0 on the bottom wall face k = 0, with yp (ny values, device) the cell
+ * centres and n standard normals that are a fixed function of (seed, field, point)
+ * (a counter hash and one single-precision Box-Muller step, stored as doubles).
+ * Halos are not written.  Asynchronous on `stream`. */
+int prj_synth_channel_predictor(int nx, int nz, int ny, const double* d_yp, unsigned long long seed, double sigma,
+                                double* d_Uh, double* d_Vh, double* d_Wh, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* prj_last_error_string(void);
 
