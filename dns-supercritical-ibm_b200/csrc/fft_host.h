@@ -12,26 +12,38 @@
 
 namespace prj {
 
-// radices of the lengths with a compile-time pass plan (fft_pass.cuh); 0 if none
-inline int pass_radices(int n, int* fac, int cap) {
+// radices of the compile-time pass plan of length n in radix order `order` (0: the
+// default of PRJ_PASS_PLANS, k >= 1: the k-th entry of n in PRJ_PASS_ALTS); 0 if none
+inline int pass_radices(int n, int* fac, int cap, int order = 0) {
+    int seen = 0;
 #define PRJ_PASS_RADICES(N, ...)                                  \
-    if (n == N) {                                                 \
+    if (n == N && seen++ == order) {                              \
         const int r[] = {__VA_ARGS__};                            \
         const int nr = (int)(sizeof(r) / sizeof(r[0]));           \
         if (nr > cap) return -1;                                  \
         for (int i = 0; i < nr; i++) fac[i] = r[i];               \
         return nr;                                                \
     }
-    PRJ_PASS_PLANS(PRJ_PASS_RADICES)
+    PRJ_PASS_ALL(PRJ_PASS_RADICES)
 #undef PRJ_PASS_RADICES
     return 0;
 }
 
-// radix sequence of a length-n transform: the pass plan's radices where one
-// exists, else 8 first, then 4, 2, 3, 5, then any remaining primes; returns the
-// number of stages or -1
-inline int fft_factorize(int n, int* fac, int cap) {
-    const int np = pass_radices(n, fac, cap);
+// radix orders compiled for length n (0 when n has no pass plan)
+inline int pass_orders(int n) {
+    int c = 0;
+#define PRJ_PASS_COUNT(N, ...) \
+    if (n == N) c++;
+    PRJ_PASS_ALL(PRJ_PASS_COUNT)
+#undef PRJ_PASS_COUNT
+    return c;
+}
+
+// radix sequence of a length-n transform: the pass plan's radices (in radix order
+// `order`) where one exists, else 8 first, then 4, 2, 3, 5, then any remaining primes;
+// returns the number of stages or -1
+inline int fft_factorize(int n, int* fac, int cap, int order = 0) {
+    const int np = pass_radices(n, fac, cap, order);
     if (np != 0) return np;
     int nf = 0, m = n;
     auto push = [&](int r) { if (nf < cap) fac[nf] = r; nf++; };
@@ -56,10 +68,11 @@ inline bool dif_supported(int n) {
     return true;
 }
 
-// fills the stage descriptor; returns the number of twiddles (>= 1) or -1
-inline long dif_plan(int n, DifDev* f) {
+// fills the stage descriptor (radix order `order` where n has a pass plan); returns the
+// number of twiddles (>= 1) or -1
+inline long dif_plan(int n, DifDev* f, int order = 0) {
     int fac[kMaxStages];
-    const int nf = fft_factorize(n, fac, kMaxStages);
+    const int nf = fft_factorize(n, fac, kMaxStages, order);
     if (nf < 0) return -1;
     std::memset(f, 0, sizeof(*f));
     f->n = n;
@@ -76,6 +89,13 @@ inline long dif_plan(int n, DifDev* f) {
         cnt += (long)(L / R) * (R - 1);
         L /= R;
     }
+    return cnt > 0 ? cnt : 1;
+}
+
+// twiddle entries of a stage descriptor (what dif_plan returned for it)
+inline long dif_twiddle_count(const DifDev& f) {
+    long cnt = 0;
+    for (int s = 0; s < f.nst; s++) cnt += (long)(f.span[s] / f.radix[s]) * (f.radix[s] - 1);
     return cnt > 0 ? cnt : 1;
 }
 

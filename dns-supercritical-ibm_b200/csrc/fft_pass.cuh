@@ -242,6 +242,24 @@ inline bool same_radices(const DifDev& f) {
     X(1024, 4, 8, 4, 8)         \
     X(1536, 4, 8, 6, 8)
 
+// Other radix orders of some of those lengths, compiled as well, that a plan's tuning
+// (x_order / z_order) can select: order k >= 1 of length n is the k-th entry of n below.
+// The autotuner times them against the default orders above.  Different orders round
+// differently (every one within the parity bounds); a given order gives the same bits in
+// every kernel family.
+#define PRJ_PASS_ALTS(X)        \
+    X(64, 4, 4, 4)              \
+    X(96, 8, 6, 2)              \
+    X(128, 8, 8, 2)             \
+    X(192, 6, 4, 8)             \
+    X(256, 4, 8, 8)             \
+    X(256, 8, 8, 4)             \
+    X(384, 8, 6, 8)             \
+    X(384, 8, 8, 6)
+
+// every compiled pass plan: the default orders, then the other orders
+#define PRJ_PASS_ALL(X) PRJ_PASS_PLANS(X) PRJ_PASS_ALTS(X)
+
 // Row stride (in elements) of the x kernels' shared-memory rows of m complex values:
 // a multiple of 8, so every row starts on a padding boundary and the passes of
 // consecutive rows see the same bank pattern; the +8 offsets consecutive rows by

@@ -126,11 +126,12 @@ void dfree(P*& p) {
     p = nullptr;
 }
 
-// in-place DIF tables of a length-n transform (left unset when a radix is unsupported)
-int make_dif(int n, prj::DifFft* d, size_t* bytes) {
+// in-place DIF tables of a length-n transform in radix order `order` (left unset when a
+// radix is unsupported)
+int make_dif(int n, prj::DifFft* d, size_t* bytes, int order = 0) {
     d->ok = false;
     if (!prj::dif_supported(n)) return PRJ_OK;
-    const long ntw = prj::dif_plan(n, &d->f);
+    const long ntw = prj::dif_plan(n, &d->f, order);
     if (ntw < 0) return PRJ_OK;
     std::vector<double2> tw((size_t)ntw);
     std::vector<int> pos((size_t)n);
@@ -145,9 +146,9 @@ int make_dif(int n, prj::DifFft* d, size_t* bytes) {
 }
 
 // slot -> wavenumber table of the length-n in-place plan (inverse of its position table)
-int make_slot_table(int n, int** d_out, size_t* bytes) {
+int make_slot_table(int n, int** d_out, size_t* bytes, int order = 0) {
     prj::DifDev f{};
-    const long ntw = prj::dif_plan(n, &f);
+    const long ntw = prj::dif_plan(n, &f, order);
     if (ntw < 0) return fail(PRJ_ERR_UNSUPPORTED, "no in-place plan for length %d", n);
     std::vector<double2> tw((size_t)ntw);
     std::vector<int> pos((size_t)n), kz((size_t)n);
@@ -1159,6 +1160,40 @@ int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out) {
     out->thomas_ring = plan->thomas_async;
     out->mixed_iters = plan->mixed_iters;
     out->mixed_tau = plan->mixed_tau;
+    out->x_order = plan->x_order;
+    out->z_order = plan->z_order;
+    return PRJ_OK;
+}
+
+// rebuilds the in-place x or z transform tables in another radix order (z: with its slot
+// table); the old tables are freed once the device is idle
+int reorder_dif(prj_plan* pl, bool x_axis, int order) {
+    const int n = x_axis ? pl->fx64.m : pl->g.nz;
+    prj::DifFft fresh{};
+    size_t bytes = 0;
+    int* kz = nullptr;
+    int rc = make_dif(n, &fresh, &bytes, order);
+    if (!rc && !x_axis && fresh.ok) rc = make_slot_table(n, &kz, &bytes, order);
+    if (rc || !fresh.ok) {
+        dfree(fresh.tw);
+        dfree(fresh.pos);
+        dfree(kz);
+        return rc ? rc : fail(PRJ_ERR_UNSUPPORTED, "no in-place plan of length %d in radix order %d", n, order);
+    }
+    cudaDeviceSynchronize();
+    prj::DifFft& d = x_axis ? pl->xd : pl->zd;
+    const size_t old = (size_t)prj::dif_twiddle_count(d.f) * sizeof(double2) + (size_t)n * sizeof(int) +
+                       (x_axis ? 0 : (size_t)n * sizeof(int));
+    dfree(d.tw);
+    dfree(d.pos);
+    d = fresh;
+    if (!x_axis) {
+        dfree(pl->kz_of_slot);
+        pl->kz_of_slot = kz;
+    }
+    pl->device_bytes += bytes;
+    pl->device_bytes -= std::min(old, pl->device_bytes);
+    (x_axis ? pl->x_order : pl->z_order) = order;
     return PRJ_OK;
 }
 
@@ -1178,12 +1213,19 @@ int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* t) {
     if (t->thomas_ring < -1 || t->thomas_ring > 4) return fail(PRJ_ERR_ARG, "thomas_ring=%d must lie in [-1, 4]", t->thomas_ring);
     if (t->mixed_iters < 0 || t->mixed_iters > 8) return fail(PRJ_ERR_ARG, "mixed_iters=%d must lie in [0, 8]", t->mixed_iters);
     if (!(t->mixed_tau > 0.0 && t->mixed_tau < 1.0)) return fail(PRJ_ERR_ARG, "mixed_tau=%g must lie in (0, 1)", t->mixed_tau);
+    const int nxo = std::max(1, prj::pass_orders(plan->fx64.m)), nzo = std::max(1, prj::pass_orders(plan->g.nz));
+    if (t->x_order < 0 || t->x_order >= nxo)
+        return fail(PRJ_ERR_ARG, "x_order=%d: length %d has %d compiled radix order(s)", t->x_order, plan->fx64.m, nxo);
+    if (t->z_order < 0 || t->z_order >= nzo)
+        return fail(PRJ_ERR_ARG, "z_order=%d: length %d has %d compiled radix order(s)", t->z_order, plan->g.nz, nzo);
     const int rs = plan->fx64.even ? plan->fx64.m + 1 : plan->fx64.m;
     if ((size_t)prj::padded_len(t->x_rows * rs, true) * sizeof(double2) + (size_t)plan->fx64.m * sizeof(int) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "x_rows=%d does not fit shared memory for nx=%d", t->x_rows, plan->g.nx);
     if (t->z_rows && (size_t)prj::padded_len(t->z_rows * plan->g.nz, true) * sizeof(double2) > 200 * 1024)
         return fail(PRJ_ERR_ARG, "z_rows=%d does not fit shared memory for nz=%d", t->z_rows, plan->g.nz);
     DeviceGuard dg(plan->device);
+    if (t->x_order != plan->x_order && plan->xd.ok && (rc = reorder_dif(plan, true, t->x_order))) return rc;
+    if (t->z_order != plan->z_order && plan->zd.ok && (rc = reorder_dif(plan, false, t->z_order))) return rc;
     if (t->mixed_tau != plan->mixed_tau && (plan->spec32 || plan->kxs_mixed)) {
         // the FP64 row count follows mixed_tau: the mixed set-up runs again at the next mixed call
         cudaDeviceSynchronize();

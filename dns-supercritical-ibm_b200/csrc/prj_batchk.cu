@@ -55,7 +55,8 @@ struct BatchSeg {
 
 namespace {
 
-// lengths the persistent kernel dispatches (the pass plans up to 256 points)
+// plans the persistent kernel dispatches, indexed: the pass plans up to 256 points in
+// every compiled radix order (fft_pass.cuh PRJ_PASS_PLANS and PRJ_PASS_ALTS)
 #define PRJ_BATCH_PLANS(X) \
     X(0, 16, 4, 4)         \
     X(1, 24, 6, 4)         \
@@ -65,7 +66,13 @@ namespace {
     X(5, 96, 2, 6, 8)      \
     X(6, 128, 4, 4, 8)     \
     X(7, 192, 3, 8, 8)     \
-    X(8, 256, 8, 4, 8)
+    X(8, 256, 8, 4, 8)     \
+    X(9, 64, 4, 4, 4)      \
+    X(10, 96, 8, 6, 2)     \
+    X(11, 128, 8, 8, 2)    \
+    X(12, 192, 6, 4, 8)    \
+    X(13, 256, 4, 8, 8)    \
+    X(14, 256, 8, 8, 4)
 
 constexpr int kBatchThreads = kPassThreads;  // = kThomasTile
 static_assert(kPassThreads == kThomasTile, "one CTA shape for every stage");
@@ -166,14 +173,11 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
 }
 
 int batch_plan_index(int n, const DifDev& f) {
-    switch (n) {
 #define PRJ_BI(I, N, ...) \
-    case N: return same_radices<PassList<__VA_ARGS__>>(f) ? I : -1;
-        PRJ_BATCH_PLANS(PRJ_BI)
+    if (n == N && same_radices<PassList<__VA_ARGS__>>(f)) return I;
+    PRJ_BATCH_PLANS(PRJ_BI)
 #undef PRJ_BI
-    default:
-        return -1;
-    }
+    return -1;
 }
 
 }  // namespace

@@ -127,6 +127,8 @@ struct prj_plan {
     int tz_xp = 1;                // rows per CTA of the pass-plan x kernels
     double* vd_pad = nullptr;     // inv_dy_p_pad (ny+1) of the variable-density step
     double* vd_ih = nullptr;      // 0.5 / rho (halo'd) of the variable-density step (scratch)
+    int x_order = 0;              // radix order of the in-place x transform (fft_pass.cuh PRJ_PASS_ALTS)
+    int z_order = 0;              // radix order of the in-place z transform
     int z_planes = 0;             // planes per chunk of the per-wavenumber z kernels (0: their default)
     int z_stages = 0;             // stages of their copy rings (0: their default)
     double mixed_tau = 1e-3;      // FP64-row threshold of the mixed path

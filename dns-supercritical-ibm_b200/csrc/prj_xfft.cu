@@ -336,18 +336,14 @@ cudaError_t launch_xpass(const prj_plan* pl, bool fwd, FwdSource src, XArgs a, i
     if (!pl->use_pass || !a.even) return cudaErrorNotSupported;
     a.tz = pl->tz_xp;
     const dim3 grid((pl->g.nz + a.tz - 1) / a.tz, ny_launch);
-    switch (a.m) {
-#define PRJ_X_CASE(N, ...)                                                          \
-    case N: {                                                                       \
-        using PL = PassList<__VA_ARGS__>;                                           \
-        if (!same_radices<PL>(pl->xd.f)) return cudaErrorNotSupported;              \
-        return fwd ? launch_fwd_xp_pl<PL>(a, src, grid, st) : launch_bwd_xp_pl<PL>(a, grid, st); \
+#define PRJ_X_CASE(N, ...)                                                                          \
+    if (a.m == N && same_radices<PassList<__VA_ARGS__>>(pl->xd.f)) {                                \
+        using PL = PassList<__VA_ARGS__>;                                                           \
+        return fwd ? launch_fwd_xp_pl<PL>(a, src, grid, st) : launch_bwd_xp_pl<PL>(a, grid, st);    \
     }
-        PRJ_PASS_PLANS(PRJ_X_CASE)
+    PRJ_PASS_ALL(PRJ_X_CASE)
 #undef PRJ_X_CASE
-    default:
-        return cudaErrorNotSupported;
-    }
+    return cudaErrorNotSupported;
 }
 
 }  // namespace

@@ -240,14 +240,12 @@ cudaError_t launch_zline_ns(const ZLineArgs& a, int ns, size_t smem, cudaStream_
 
 bool zline_supported(const prj_plan* pl) {
     if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc) return false;
-    switch (pl->g.nz) {
-#define PRJ_ZL_HAS(N, ...) \
-    case N: return same_radices<PassList<__VA_ARGS__>>(pl->zd.f) && zline_smem(N, pl->g.mzp, 1, 2) <= (size_t)200 * 1024;
-        PRJ_PASS_PLANS(PRJ_ZL_HAS)
+#define PRJ_ZL_HAS(N, ...)                                                          \
+    if (pl->g.nz == N && same_radices<PassList<__VA_ARGS__>>(pl->zd.f))             \
+        return zline_smem(N, pl->g.mzp, 1, 2) <= (size_t)200 * 1024;
+    PRJ_PASS_ALL(PRJ_ZL_HAS)
 #undef PRJ_ZL_HAS
-    default:
-        return false;
-    }
+    return false;
 }
 
 // cudaErrorNotSupported when nz has no pass plan (the caller runs the split kernels)
@@ -271,18 +269,12 @@ cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st) {
     const size_t smem = zline_smem(g.nz, g.mzp, yb, ns);
     if (smem > (size_t)200 * 1024) return cudaErrorNotSupported;
     a.yb = yb;
-    switch (g.nz) {
 #define PRJ_ZL_CASE(N, ...)                                                  \
-    case N: {                                                                \
-        using PL = PassList<__VA_ARGS__>;                                    \
-        if (!same_radices<PL>(pl->zd.f)) return cudaErrorNotSupported;       \
-        return launch_zline_ns<PL>(a, ns, smem, st);                         \
-    }
-        PRJ_PASS_PLANS(PRJ_ZL_CASE)
+    if (g.nz == N && same_radices<PassList<__VA_ARGS__>>(pl->zd.f))          \
+        return launch_zline_ns<PassList<__VA_ARGS__>>(a, ns, smem, st);
+    PRJ_PASS_ALL(PRJ_ZL_CASE)
 #undef PRJ_ZL_CASE
-    default:
-        return cudaErrorNotSupported;
-    }
+    return cudaErrorNotSupported;
 }
 
 }  // namespace prj

@@ -294,19 +294,15 @@ cudaError_t launch_zfft_pass(const prj_plan* pl, int dir, void* X, int rows_per_
     a.f = pl->zd.f;
     a.tw = pl->zd.tw;
     a.X = X;
-    switch (g.nz) {
 #define PRJ_Z_CASE(N, ...)                                                                    \
-    case N: {                                                                                 \
+    if (g.nz == N && same_radices<PassList<__VA_ARGS__>>(pl->zd.f)) {                         \
         using PL = PassList<__VA_ARGS__>;                                                     \
-        if (!same_radices<PL>(pl->zd.f)) return cudaErrorNotSupported;                        \
         return dir < 0 ? launch_zfft_pass_pl<-1, T, PL>(a, pl->zfft_rows, st)                 \
                        : launch_zfft_pass_pl<+1, T, PL>(a, pl->zfft_rows, st);                \
     }
-        PRJ_PASS_PLANS(PRJ_Z_CASE)
+    PRJ_PASS_ALL(PRJ_Z_CASE)
 #undef PRJ_Z_CASE
-    default:
-        return cudaErrorNotSupported;
-    }
+    return cudaErrorNotSupported;
 }
 
 // in-place z FFT of every spectral row of one buffer: dir < 0 forward (natural ->

@@ -85,7 +85,8 @@ class Stats(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("x_rows", ctypes.c_int), ("z_rows", ctypes.c_int), ("z_mode", ctypes.c_int),
                 ("z_planes", ctypes.c_int), ("z_stages", ctypes.c_int), ("thomas_ring", ctypes.c_int),
-                ("mixed_iters", ctypes.c_int), ("mixed_tau", ctypes.c_double)]
+                ("mixed_iters", ctypes.c_int), ("mixed_tau", ctypes.c_double), ("x_order", ctypes.c_int),
+                ("z_order", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -431,7 +432,7 @@ class Plan:
     def set_tuning(self, x_rows=None, z_rows=None, z_mode=None, **kw):
         """Change some fields of the plan's tuning (prj_plan_set_tuning); the others keep their
         current values.  Fields: x_rows, z_rows, z_mode, z_planes, z_stages, thomas_ring,
-        mixed_iters, mixed_tau."""
+        mixed_iters, mixed_tau, x_order, z_order."""
         t = self.tuning
         for k, v in (("x_rows", x_rows), ("z_rows", z_rows), ("z_mode", z_mode), *kw.items()):
             if k not in t:

@@ -315,7 +315,13 @@ int prj_batch_destroy(prj_batch* batch);
  *               (planes x stages) for both storages;
  *   mixed_iters refinement passes of PRJ_MODE_FP32_REFINE (default 1, 0..8);
  *   mixed_tau   x-wavenumber rows with |a_x| < mixed_tau max|b| keep FP64 storage in
- *               the mixed path (default 1e-3; must lie in (0, 1)).
+ *               the mixed path (default 1e-3; must lie in (0, 1));
+ *   x_order,    radix order of the in-place x (length nx/2) and z (length nz)
+ *   z_order     transforms: 0 = the default pass plan, k >= 1 = the k-th other compiled
+ *               order of that length (64: 4x4x4; 96: 8x6x2; 128: 8x8x2; 192: 6x4x8;
+ *               256: 4x8x8, 8x8x4; 384: 8x6x8, 8x8x6).  Orders round differently (each
+ *               within the parity bounds); a given order gives the same bits in every
+ *               kernel family.  Changing an order rebuilds the transform's tables.
  * prj_plan_set_tuning rejects values out of range and shapes that do not fit
  * shared memory; it may free and later reallocate the mixed path's FP32 spectrum
  * (after a change of mixed_tau), so call it outside stream capture.
@@ -332,6 +338,8 @@ typedef struct prj_tuning {
     int thomas_ring;
     int mixed_iters;
     double mixed_tau;
+    int x_order;
+    int z_order;
 } prj_tuning;
 int prj_plan_get_tuning(const prj_plan* plan, prj_tuning* out);
 int prj_plan_set_tuning(prj_plan* plan, const prj_tuning* tuning);
