@@ -296,7 +296,7 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None):
             p.set_tuning(**tuned[(nx, ny, nz)])
         else:
             best = autotune.tune(p, reps=3)
-            tuned[(nx, ny, nz)] = {k: best[k] for k in ("x_rows", "z_rows", "z_mode")}
+            tuned[(nx, ny, nz)] = {k: best.get(k, 0) for k in autotune.FIELDS}
         plans.append(p)
         g = torch.Generator(device=device)
         g.manual_seed(seeds[i])

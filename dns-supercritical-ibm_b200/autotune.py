@@ -1,10 +1,14 @@
-"""Launch-shape autotuner of the pressure-Poisson engine.
+"""Autotuner of the pressure-Poisson engine: launch shapes and FFT radix plans.
 
-For one grid size it times candidate tunings of a plan -- x-rows per CTA of the
-x transforms, spectral rows per CTA of the z transforms, and split versus fused
-z kernels (prj_tuning, include/projection.h) -- on an in-place FP64 solve with
-CUDA events, keeps the fastest, and caches it in a JSON file keyed by grid size
-and device name (PRJ_AUTOTUNE_CACHE, default ~/.cache/prj_b200/autotune.json).
+For one grid size it times candidate tunings of a plan (prj_tuning,
+include/projection.h) on an in-place FP64 solve with CUDA events, in two phases:
+first the launch shapes -- x-rows per CTA of the x transforms, spectral rows per
+CTA of the z transforms, split versus fused z kernels -- in the default radix
+orders; then, with the best shapes, every compiled radix order of the x and z
+transform lengths (the pass plans of fft_pass.cuh, where the reference lets
+FFTW/cuFFT pick a factorisation at plan time, poisson_solver_multigpu.f90:77-129).
+The fastest is applied and cached in a JSON file keyed by grid size and device name
+(PRJ_AUTOTUNE_CACHE, default ~/.cache/prj_b200/autotune.json).
 """
 from __future__ import annotations
 
@@ -53,6 +57,18 @@ def candidates(plan):
     return out
 
 
+# compiled radix orders per transform length (fft_pass.cuh PRJ_PASS_PLANS + PRJ_PASS_ALTS)
+RADIX_ORDERS = {64: 2, 96: 2, 128: 2, 192: 2, 256: 3, 384: 3}
+
+
+def order_candidates(plan, shape):
+    """The best launch shape in every combination of the compiled radix orders."""
+    g = plan.grid
+    nxo = RADIX_ORDERS.get(g.nx // 2, 1) if g.nx % 2 == 0 else 1
+    nzo = RADIX_ORDERS.get(g.nz, 1)
+    return [dict(shape, x_order=xo, z_order=zo) for xo in range(nxo) for zo in range(nzo) if xo or zo]
+
+
 def time_solve(plan, P, reps):
     import torch
     s = torch.cuda.current_stream(plan.device)
@@ -67,6 +83,13 @@ def time_solve(plan, P, reps):
     return e0.elapsed_time(e1) / reps
 
 
+FIELDS = ("x_rows", "z_rows", "z_mode", "x_order", "z_order")
+
+
+def _apply(plan, t):
+    plan.set_tuning(**{k: t.get(k, 0) for k in FIELDS})
+
+
 def tune(plan, reps: int = 5, use_cache: bool = True) -> dict:
     """Apply the fastest tuning for this plan's grid (cached) and return it with its time."""
     import torch
@@ -74,24 +97,27 @@ def tune(plan, reps: int = 5, use_cache: bool = True) -> dict:
     cache = _load_cache() if use_cache else {}
     if k in cache:
         t = cache[k]
-        plan.set_tuning(t["x_rows"], t["z_rows"], t["z_mode"])
+        _apply(plan, t)
         return dict(t, cached=True)
     g = plan.grid
     P = torch.randn((g.ny, g.nz, g.nx), dtype=torch.float64, device=f"cuda:{plan.device}")
     best = None
     default = plan.tuning
-    for c in candidates(plan):
-        try:
-            plan.set_tuning(c["x_rows"], c["z_rows"], c["z_mode"])
-        except prj.PrjError:
-            continue
-        ms = time_solve(plan, P, reps)
-        if best is None or ms < best["ms"]:
-            best = dict(c, ms=ms)
-    if best is None:
-        plan.set_tuning(default["x_rows"], default["z_rows"], default["z_mode"])
-        return dict(default, ms=None, cached=False)
-    plan.set_tuning(best["x_rows"], best["z_rows"], best["z_mode"])
+    for phase in (0, 1):
+        cands = candidates(plan) if phase == 0 else order_candidates(plan, {f: best[f] for f in FIELDS})
+        for c in cands:
+            c = dict({"x_order": 0, "z_order": 0}, **c)
+            try:
+                _apply(plan, c)
+            except prj.PrjError:
+                continue
+            ms = time_solve(plan, P, reps)
+            if best is None or ms < best["ms"]:
+                best = dict(c, ms=ms)
+        if best is None:
+            _apply(plan, default)
+            return dict(default, ms=None, cached=False)
+    _apply(plan, best)
     if use_cache:
         cache = _load_cache()
         cache[k] = best
