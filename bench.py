@@ -263,7 +263,7 @@ def timed_steps(fn, stream, steps):
     return total
 
 
-def run_batched(device, steps, warmup, rank=0, world=1, dist=None):
+def run_batched(device, steps, warmup, rank=0, world=1, dist=None, tune=True):
     """64 independent Poisson solves of uneven sizes in one launch: sizes from default_rng(2)
     (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]), uniform[-1,1]
     right-hand sides minus their dy-weighted mean; launch shapes from the autotuner.  FP64: the
@@ -292,7 +292,9 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None):
         yu = workloads.tanh_faces(ny, beta)
         dx, dz = workloads.channel_spacing(nx, nz)
         p = prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent"), device=device.index or 0)
-        if (nx, ny, nz) in tuned:
+        if not tune:
+            tuned[(nx, ny, nz)] = {}
+        elif (nx, ny, nz) in tuned:
             p.set_tuning(**tuned[(nx, ny, nz)])
         else:
             best = autotune.tune(p, reps=3)
@@ -546,6 +548,10 @@ def main():
     ap.add_argument("--grid", default=f"{NX}x{NY}x{NZ}", help="nx x ny x nz (profiling of smaller cases)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the mixed, batched and served legs")
+    ap.add_argument("--legs", default="mixed,batched,served,vd,rough",
+                    help="comma list of the extra legs to run (mixed, batched, served, vd, rough)")
+    ap.add_argument("--batch-tune", default="auto", choices=["auto", "default"],
+                    help="batched leg: autotuned tunings, or the plans' defaults (profiling runs)")
     ap.add_argument("--served-seconds", type=float, default=30.0)
     ap.add_argument("--served-rate", type=float, default=2000.0)
     ap.add_argument("--served-budget-gb", type=float, default=150.0)
@@ -693,8 +699,9 @@ def main():
                                                                stream)
         del orc
 
+    legs = set() if args.no_extra else {v.strip() for v in args.legs.split(",") if v.strip()}
     extra = {}
-    if not args.no_extra:
+    if "mixed" in legs:
         # FP32 spectral storage + FP64 refinement on the same step
         other = prj.MODE_FP32_REFINE if mode == prj.MODE_FP64 else prj.MODE_FP64
         P_main = P.clone()
@@ -715,12 +722,12 @@ def main():
     plan.close()
     del Uh, Vh, Wh, U, V, W, P
     torch.cuda.empty_cache()
-    if not args.no_extra:
+    if "batched" in legs:
         extra["batched"] = run_batched(device, steps=max(3, args.steps // 4), warmup=args.warmup, rank=rank,
-                                       world=world, dist=dist)
+                                       world=world, dist=dist, tune=args.batch_tune == "auto")
         torch.cuda.empty_cache()
-    if not args.no_extra and world == 1:
-        if args.served_seconds > 0:  # --served-seconds 0 leaves the served legs out
+    if world == 1:
+        if "served" in legs and args.served_seconds > 0:  # --served-seconds 0 leaves the served legs out
             extra["served"] = run_served(device, args.served_seconds, args.served_rate, args.served_budget_gb * 1e9)
             torch.cuda.empty_cache()
             # the same request mix at a rate one GPU sustains: latency without queue growth
@@ -732,9 +739,11 @@ def main():
             extra["served_host_io"] = run_served(device, min(10.0, args.served_seconds), 40.0,
                                                  args.served_budget_gb * 1e9, io="host")
             torch.cuda.empty_cache()
-        extra["variable_density"] = run_vd(device, NX, NY, NZ, steps=max(3, args.steps // 4), warmup=args.warmup)
-        torch.cuda.empty_cache()
-        if args.rough_grid:
+        if "vd" in legs:
+            extra["variable_density"] = run_vd(device, NX, NY, NZ, steps=max(3, args.steps // 4),
+                                               warmup=args.warmup)
+            torch.cuda.empty_cache()
+        if "rough" in legs and args.rough_grid:
             rx, ry, rz = (int(v) for v in args.rough_grid.lower().split("x"))
             extra["rough_wall"] = run_rough(device, rx, ry, rz, steps=max(3, args.steps // 10), warmup=args.warmup)
             torch.cuda.empty_cache()
