@@ -38,11 +38,11 @@ namespace prj {
 // stages of one solve
 enum BatchStage { kBFwdX = 0, kBZFwd = 1, kBThomas = 2, kBZInv = 3, kBBwdX = 4, kBNumStages = 5 };
 
-struct BatchCaseDev {
+struct __align__(16) BatchCaseDev {
     XArgs x;          // forward (source P) and inverse (P out) x transforms of the case
     ZfftArgs z;       // its z rows (ny nh rows of nz)
     ThomasArgs t;     // its Thomas lines
-    int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in kBatchPlans
+    int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in PRJ_BATCH_PLANS
     int ntz;          // x tiles per y plane
     int tiles[kBNumStages];
 };
@@ -77,11 +77,30 @@ namespace {
 constexpr int kBatchThreads = kPassThreads;  // = kThomasTile
 static_assert(kPassThreads == kThomasTile, "one CTA shape for every stage");
 
+// Every (stage, plan) tile is its own non-inlined function: inlined into one switch, the
+// thirty plan variants' butterflies shared one register allocation and spilled (2 KB of
+// stack per thread); as calls, each tile function is allocated on its own, as in its
+// per-case kernel.
+template <class PL>
+__device__ __noinline__ void tile_x_fwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    fwd_xp_tile<0, PL>(c.x, sm, tile % c.ntz, tile / c.ntz);
+}
+template <class PL>
+__device__ __noinline__ void tile_x_bwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    bwd_xp_tile<PL, false>(c.x, sm, tile % c.ntz, tile / c.ntz, c.ntz);
+}
+template <int DIR, class PL>
+__device__ __noinline__ void tile_z(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    zfft_pass_tile<DIR, double2, PL, (DIR > 0)>(c.z, reinterpret_cast<double2*>(sm), tile);
+}
+// four planes per load block: the eight of k_thomas need more than the kernel's 128
+// registers per thread
+__device__ __noinline__ void tile_thomas(const BatchCaseDev& c, int tile) { thomas_line<double2, 4>(c.t, tile); }
+
 __device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    const int bx = tile % c.ntz, by = tile / c.ntz;
     switch (c.xplan) {
 #define PRJ_BX(I, N, ...) \
-    case I: fwd_xp_tile<0, PassList<__VA_ARGS__>>(c.x, sm, bx, by); break;
+    case I: tile_x_fwd<PassList<__VA_ARGS__>>(c, tile, sm); break;
         PRJ_BATCH_PLANS(PRJ_BX)
 #undef PRJ_BX
     default: break;
@@ -89,10 +108,9 @@ __device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int tile, unsig
 }
 
 __device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    const int bx = tile % c.ntz, by = tile / c.ntz;
     switch (c.xplan) {
 #define PRJ_BX(I, N, ...) \
-    case I: bwd_xp_tile<PassList<__VA_ARGS__>>(c.x, sm, bx, by, c.ntz); break;
+    case I: tile_x_bwd<PassList<__VA_ARGS__>>(c, tile, sm); break;
         PRJ_BATCH_PLANS(PRJ_BX)
 #undef PRJ_BX
     default: break;
@@ -101,10 +119,9 @@ __device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int tile, unsig
 
 template <int DIR>
 __device__ __forceinline__ void run_z(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    double2* zp = reinterpret_cast<double2*>(sm);
     switch (c.zplan) {
 #define PRJ_BZ(I, N, ...) \
-    case I: zfft_pass_tile<DIR, double2, PassList<__VA_ARGS__>, (DIR > 0)>(c.z, zp, tile); break;
+    case I: tile_z<DIR, PassList<__VA_ARGS__>>(c, tile, sm); break;
         PRJ_BATCH_PLANS(PRJ_BZ)
 #undef PRJ_BZ
     default: break;
@@ -117,6 +134,10 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
     extern __shared__ __align__(16) unsigned char bsm[];
     __shared__ long long s_item;
     __shared__ int s_seg, s_skip;
+    // the current case's arguments, copied once per change of case (items of one case and
+    // stage come in runs) so that the tile functions read them from shared memory
+    __shared__ __align__(16) BatchCaseDev s_case;
+    int loaded = -1;
     for (;;) {
         if (threadIdx.x == 0) {
             const long long it = (long long)atomicAdd(counter, 1ull);
@@ -153,13 +174,21 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
         const long long it = s_item;
         if (it >= nitems) break;
         const BatchSeg g = segs[s_seg];
-        const BatchCaseDev& c = cases[g.case_id];
+        if (g.case_id != loaded) {
+            static_assert(sizeof(BatchCaseDev) % 16 == 0, "16-byte copies");
+            const int4* src = reinterpret_cast<const int4*>(cases + g.case_id);
+            int4* dst = reinterpret_cast<int4*>(&s_case);
+            for (int w = threadIdx.x; w < (int)(sizeof(BatchCaseDev) / 16); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            loaded = g.case_id;
+        }
+        const BatchCaseDev& c = s_case;
         const int tile = g.tile0 + (int)(it - g.item0);
         if (!s_skip) {
             switch (g.stage) {
             case kBFwdX: run_x_fwd(c, tile, bsm); break;
             case kBZFwd: run_z<-1>(c, tile, bsm); break;
-            case kBThomas: thomas_line<double2>(c.t, tile); break;
+            case kBThomas: tile_thomas(c, tile); break;
             case kBZInv: run_z<+1>(c, tile, bsm); break;
             default: run_x_bwd(c, tile, bsm); break;
             }
@@ -197,6 +226,11 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
         BatchCaseDev& c = cs[i];
         c.x = batch_x_args(pl, d_P[i]);
         c.z = batch_z_args(pl);
+        // tile shapes within the per-case kernels' default shared-memory budgets (28-32 KB),
+        // so four CTAs fit per SM whatever the plans' own tuning; a tile's shape does not
+        // change its results
+        c.x.tz = std::min(c.x.tz, choose_tz_xp(pl->fx64.m));
+        c.z.rb = std::min(c.z.rb, batch_z_default_rows(g.nz));
         c.t = thomas_args(pl, pl->spec, 0, g.nxh);
         c.xplan = batch_plan_index(pl->fx64.m, pl->xd.f);
         c.zplan = batch_plan_index(g.nz, pl->zd.f);

@@ -339,6 +339,8 @@ cudaError_t launch_zfft_t(const prj_plan* pl, int dir, void* X, int rows_per_pla
     return cudaGetLastError();
 }
 
+int batch_z_default_rows(int nz) { return pass_rows(nz, 0); }
+
 ZfftArgs batch_z_args(const prj_plan* pl) {
     const Geometry& g = pl->g;
     ZfftArgs a{};

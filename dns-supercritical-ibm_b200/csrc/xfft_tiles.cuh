@@ -196,7 +196,9 @@ __device__ __forceinline__ void fwd_xp_tile(const XArgs& a, unsigned char* sm, i
 // bwd_xp_tile: transposed load of X_k, X_{m-k} -> inverse split (scaled) into slot
 // order -> DIT passes -> P rows (x pairs as double2), optionally accumulated; the
 // tile's partial sum of P goes to psum[y][bx] (tiles_per_plane entries per plane).
-template <class PL>
+// EXTRAS = false: plain P = result (no accumulation, partial sums or norms), the form of
+// the persistent batch kernel
+template <class PL, bool EXTRAS = true>
 __device__ __forceinline__ void bwd_xp_tile(const XArgs& a, unsigned char* sm, int bx, int by, int tiles_per_plane) {
     double2* A = reinterpret_cast<double2*>(sm);
     constexpr int m = PL::n, rs = pass_row_stride(m), half = m / 2;
@@ -244,6 +246,10 @@ __device__ __forceinline__ void bwd_xp_tile(const XArgs& a, unsigned char* sm, i
     dit_passes_shared<+1, PL, PL::P - 1, 0>(A, nr, rs, a.tw);
     double2* out = reinterpret_cast<double2*>(a.Pout) + ((size_t)y * a.nz + z0) * m;
     double sq0 = 0.0, sq1 = 0.0, ps = 0.0;
+    if constexpr (!EXTRAS) {
+        dit_last_pass<+1, PL>(A, nr, rs, a.tw, [&](int r, int e, double2 v) { out[(size_t)r * m + e] = v; });
+        return;
+    }
     dit_last_pass<+1, PL>(A, nr, rs, a.tw, [&](int r, int e, double2 v) {
         double2* o = out + (size_t)r * m + e;
         if (a.accum) {

@@ -85,8 +85,11 @@ constexpr int kThomasTile = 128;
 constexpr int kBlock = PRJ_THOMAS_BLOCK;  // planes loaded together (independent loads in flight)
 
 // One line: the CTA's block index `blk` within the buffer a.X (T storage).
-template <typename T>
+// B planes of a line are loaded together (independent loads in flight); the result does
+// not depend on B
+template <typename T, int B = kBlock>
 __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
+    constexpr int kBlock = B;
     const int kb = blk / a.tiles;  // row within this buffer
     const int kx = a.kx0 + kb;
     const int slot = (blk - kb * a.tiles) * kThomasTile + threadIdx.x;
@@ -165,6 +168,7 @@ __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
 // arguments of a plan's FP64 spectrum rows for zfft_pass_tile, and of its Thomas lines
 // kx0 .. kx0+rows-1 held in X as [y][kx - kx0][z] (prj_zsplit.cu)
 ZfftArgs batch_z_args(const prj_plan* pl);
+int batch_z_default_rows(int nz);  // rows per tile of the z kernels' default shape
 ThomasArgs thomas_args(const prj_plan* pl, void* X, int kx0, int rows_per_plane);
 
 }  // namespace prj
