@@ -2,23 +2,23 @@
 //
 // A batch of independent solves (the reference solves one grid per run and plans it
 // once, poisson_solver_multigpu.f90:77-129; here every case keeps its own plan) is a
-// list of work items (case, stage, tile).  The five stages of a solve are the split
+// list of work items (case, stage, tiles).  The five stages of a solve are the split
 // path's kernels -- forward x transform, forward z transform, Thomas sweeps, inverse z
-// transform, inverse x transform -- and a tile is what one CTA of that kernel does.
-// The host orders the items stage-major (every case's forward x tiles, then every
-// case's forward z tiles, ...), largest cases first within a stage, and one launch of
-// k_batch runs them all:
+// transform, inverse x transform -- and a tile is what one CTA of that kernel does; an
+// item is a run of up to 16 tiles of one stage of one case.  The host orders the items
+// stage-major (every case's forward x items, then every case's forward z items, ...),
+// largest cases first within a stage, and one launch of k_batch runs them all:
 //
 //   a CTA takes the next item index from a global counter (atomicAdd), waits until the
 //   case's previous stage has completed all its tiles (a per-case, per-stage counter,
-//   read with acquire semantics), runs the tile with the same device function as the
-//   per-case kernel (xfft_tiles.cuh, zsplit_tiles.cuh), and counts the tile done
+//   read with acquire semantics), runs the item's tiles with the same device functions as
+//   the per-case kernels (xfft_tiles.cuh, zsplit_tiles.cuh), and counts them done
 //   (release);
 //   items are taken in order, and an item depends only on items before it, all of which
 //   are held by running CTAs that wait only on earlier items, so the queue cannot
 //   deadlock, whatever number of CTAs is resident;
 //   every wait is bounded (a clock budget): a CTA that gives up raises the batch's
-//   error word, counts its tile done without running it (so later waits end too) and
+//   error word, counts its tiles done without running them (so later waits end too) and
 //   continues; prj_batch_check_error reports PRJ_ERR_TIMEOUT.
 //
 // The tiles run the per-case kernels' code on the same elements, so every case's P
@@ -47,9 +47,8 @@ struct __align__(16) BatchCaseDev {
     int tiles[kBNumStages];
 };
 
-// a run of items: tiles tile0 .. tile0+count-1 of one stage of one case
+// one work item: tiles tile0 .. tile0+count-1 of one stage of one case
 struct BatchSeg {
-    long long item0;
     int case_id, stage, tile0, count;
 };
 
@@ -129,28 +128,22 @@ __device__ __forceinline__ void run_z(const BatchCaseDev& c, int tile, unsigned 
 }
 
 __global__ void __launch_bounds__(kBatchThreads, 4)
-    k_batch(const BatchCaseDev* __restrict__ cases, const BatchSeg* __restrict__ segs, int nseg, long long nitems,
+    k_batch(const BatchCaseDev* __restrict__ cases, const BatchSeg* __restrict__ segs, int nseg,
             unsigned long long* counter, int* done, int* err) {
     extern __shared__ __align__(16) unsigned char bsm[];
-    __shared__ long long s_item;
-    __shared__ int s_seg, s_skip;
-    // the current case's arguments, copied once per change of case (items of one case and
-    // stage come in runs) so that the tile functions read them from shared memory
+    __shared__ BatchSeg s_seg;
+    __shared__ int s_skip;
+    // the current case's arguments, copied once per change of case (the items of one case
+    // and stage come in runs) so that the tile functions read them from shared memory
     __shared__ __align__(16) BatchCaseDev s_case;
     int loaded = -1;
     for (;;) {
         if (threadIdx.x == 0) {
             const long long it = (long long)atomicAdd(counter, 1ull);
-            int sg = -1, skip = 0;
-            if (it < nitems) {
-                int lo = 0, hi = nseg - 1;  // last segment with item0 <= it
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) / 2;
-                    if (segs[mid].item0 <= it) lo = mid;
-                    else hi = mid - 1;
-                }
-                sg = lo;
-                const BatchSeg& g = segs[sg];
+            BatchSeg g{-1, 0, 0, 0};
+            int skip = 0;
+            if (it < nseg) {
+                g = segs[it];
                 if (g.stage > 0) {
                     const int need = cases[g.case_id].tiles[g.stage - 1];
                     const volatile int* d = done + g.case_id * kBNumStages + g.stage - 1;
@@ -163,17 +156,15 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
                         }
                         __nanosleep(128);
                     }
-                    __threadfence();  // acquire: the previous stage's results before this tile's reads
+                    __threadfence();  // acquire: the previous stage's results before this item's reads
                 }
             }
-            s_item = it;
-            s_seg = sg;
+            s_seg = g;
             s_skip = skip;
         }
         __syncthreads();
-        const long long it = s_item;
-        if (it >= nitems) break;
-        const BatchSeg g = segs[s_seg];
+        const BatchSeg g = s_seg;
+        if (g.case_id < 0) break;
         if (g.case_id != loaded) {
             static_assert(sizeof(BatchCaseDev) % 16 == 0, "16-byte copies");
             const int4* src = reinterpret_cast<const int4*>(cases + g.case_id);
@@ -183,20 +174,22 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
             loaded = g.case_id;
         }
         const BatchCaseDev& c = s_case;
-        const int tile = g.tile0 + (int)(it - g.item0);
         if (!s_skip) {
-            switch (g.stage) {
-            case kBFwdX: run_x_fwd(c, tile, bsm); break;
-            case kBZFwd: run_z<-1>(c, tile, bsm); break;
-            case kBThomas: tile_thomas(c, tile); break;
-            case kBZInv: run_z<+1>(c, tile, bsm); break;
-            default: run_x_bwd(c, tile, bsm); break;
+            for (int tile = g.tile0; tile < g.tile0 + g.count; tile++) {
+                switch (g.stage) {
+                case kBFwdX: run_x_fwd(c, tile, bsm); break;
+                case kBZFwd: run_z<-1>(c, tile, bsm); break;
+                case kBThomas: tile_thomas(c, tile); break;
+                case kBZInv: run_z<+1>(c, tile, bsm); break;
+                default: run_x_bwd(c, tile, bsm); break;
+                }
+                __syncthreads();  // bsm free for the next tile
             }
         }
-        __syncthreads();  // every thread's stores of the tile, and bsm free for the next one
+        __syncthreads();  // every thread's stores of the item
         if (threadIdx.x == 0) {
-            __threadfence();  // release: the tile's stores before its count
-            atomicAdd(done + g.case_id * kBNumStages + g.stage, 1);
+            __threadfence();  // release: the item's stores before its count
+            atomicAdd(done + g.case_id * kBNumStages + g.stage, g.count);
         }
     }
 }
@@ -241,19 +234,23 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
         smem = std::max(smem, pass_x_smem(pl->fx64.m, c.x.tz));
         smem = std::max(smem, (size_t)padded_len(c.z.rb * g.nz, true) * sizeof(double2));
     }
-    // stage-major order; within a stage the cases with the most tiles first
+    // stage-major order; within a stage the cases with the most tiles first; each stage of a
+    // case cut into items of up to 16 tiles (about 64 items per stage where it has that
+    // many tiles), so one counter increment and one load start several tiles
     std::vector<int> order((size_t)ncases);
     for (int i = 0; i < ncases; i++) order[i] = i;
     std::vector<BatchSeg> segs;
-    long long items = 0;
+    long long tiles_total = 0;
     for (int s = 0; s < kBNumStages; s++) {
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cs[a].tiles[s] > cs[b].tiles[s]; });
         for (int i : order) {
-            if (cs[i].tiles[s] <= 0) continue;
-            segs.push_back(BatchSeg{items, i, s, 0, cs[i].tiles[s]});
-            items += cs[i].tiles[s];
+            const int T = cs[i].tiles[s];
+            const int chunk = std::max(1, std::min(16, T / 64));
+            for (int t0 = 0; t0 < T; t0 += chunk) segs.push_back(BatchSeg{i, s, t0, std::min(chunk, T - t0)});
+            tiles_total += T;
         }
     }
+    const long long items = (long long)segs.size();
     if (smem > (size_t)200 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1));
     if (e != cudaSuccess) return e;
@@ -266,6 +263,7 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
     out->smem = smem;
     out->nseg = (int)segs.size();
     out->nitems = items;
+    out->ntiles = tiles_total;
     out->ncases = ncases;
     const size_t cb = cs.size() * sizeof(BatchCaseDev), sb = segs.size() * sizeof(BatchSeg);
     const size_t wb = sizeof(unsigned long long) + (size_t)ncases * kBNumStages * sizeof(int) + sizeof(int);
@@ -286,8 +284,8 @@ cudaError_t batchk_launch(const BatchKernel& k, cudaStream_t st) {
     int* done = reinterpret_cast<int*>(w + sizeof(unsigned long long));
     int* err = done + (size_t)k.ncases * kBNumStages;
     k_batch<<<k.grid, kBatchThreads, k.smem, st>>>(static_cast<const BatchCaseDev*>(k.d_cases),
-                                                   static_cast<const BatchSeg*>(k.d_segs), k.nseg, k.nitems, counter,
-                                                   done, err);
+                                                   static_cast<const BatchSeg*>(k.d_segs), k.nseg, counter, done,
+                                                   err);
     return cudaGetLastError();
 }
 

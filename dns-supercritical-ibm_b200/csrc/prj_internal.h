@@ -239,7 +239,8 @@ struct BatchKernel {
     size_t work_bytes = 0;     // bytes of d_work reset before every launch (all but the error word)
     size_t smem = 0;
     int grid = 0, nseg = 0, ncases = 0;
-    long long nitems = 0;
+    long long nitems = 0;      // work items (runs of up to 16 tiles)
+    long long ntiles = 0;      // tiles over all cases and stages
 };
 bool batchk_supported(const prj_plan* pl);   // the plan's lengths are among the kernel's pass plans
 cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases, BatchKernel* out);

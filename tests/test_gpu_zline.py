@@ -87,3 +87,28 @@ def test_default_rule_and_tuning(cuda_device, monkeypatch):
             plan.poisson_fp64(d)
             out[zm] = from_dev(d)
     np.testing.assert_array_equal(out[0], out[3])
+
+
+@pytest.mark.parametrize("scale", [2.0 ** -960, 2.0 ** -1010])
+def test_line_kernel_outside_the_fast_division_window(cuda_device, monkeypatch, oracle, scale):
+    """Right-hand sides so small that the forward sweeps' quotients leave the window of the
+    reciprocal-and-correction division (|q| < 2^-900; subnormal inputs at 2^-1010): the
+    per-wavenumber kernel redoes those chunks with IEEE division, the split Thomas takes its
+    fallback per quotient, and both still agree bit for bit."""
+    import prj
+    import workloads
+    nx, ny, nz = 64, 21, 384
+    rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=23)
+    rhs = np.asfortranarray(rhs * scale)
+    b6 = prj.bands(yu, "consistent")
+    out = {}
+    for mode in ("split", "line"):
+        monkeypatch.setenv("PRJ_ZSOLVE", mode)
+        with prj.Plan(nx, nz, ny, dx, dz, b6) as plan:
+            t = to_dev(rhs)
+            plan.poisson_fp64(t)
+            out[mode] = from_dev(t)
+    np.testing.assert_array_equal(out["split"], out["line"])
+    if scale == 2.0 ** -960:  # normal inputs: the oracle's plain division agrees closely
+        Po, _ = oracle.poisson(rhs, dx, dz, b6)
+        assert np.linalg.norm(out["line"] - Po) <= 1e-12 * np.linalg.norm(Po)
