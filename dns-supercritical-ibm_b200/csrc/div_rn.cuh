@@ -42,16 +42,4 @@ __device__ __forceinline__ double div_by_recip(double u, double D, double y) {
     return r == 0.0 ? q : __fma_rn(r, y, q);
 }
 
-// The same quotient with the window test taken out of the control flow: returns the
-// correction step's result and sets `outside` when it may not be RN(u / D).  A caller that
-// keeps the inputs redoes the affected values with __ddiv_rn afterwards, so a hot loop
-// carries no branch; the redone values equal what div_by_recip returns.
-__device__ __forceinline__ double div_by_recip_flagged(double u, double D, double y, bool& outside) {
-    const double q = __dmul_rn(u, y);
-    const double r = __fma_rn(-D, q, u);
-    const unsigned hq = (unsigned)__double2hiint(q) & 0x7fffffffu;
-    outside |= (hq - 0x07B00000u >= 0x7E700000u - 0x07B00000u) & (u != 0.0);
-    return r == 0.0 ? q : __fma_rn(r, y, q);
-}
-
 }  // namespace prj

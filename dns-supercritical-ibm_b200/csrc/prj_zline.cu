@@ -145,16 +145,6 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
         double2* buf = ring + sidx<true>(s * yb * n);
         const double* dbuf = dring + (size_t)s * yb * mzs;
         dif_passes_shared<-1, PL, 0, PL::P>(buf, nr, n, a.tw);  // barrier after every pass
-        // the chunk's forward recurrence; a quotient outside the fast division's window only
-        // raises a flag, and the line's chunk is then redone with IEEE division from its
-        // inputs, still in the stage (div_rn.cuh)
-        double2 prev0[LPT];
-        bool outside[LPT];
-#pragma unroll
-        for (int q = 0; q < LPT; q++) {
-            prev0[q] = prev[q];
-            outside[q] = false;
-        }
         for (int r = 0; r < nr; r++) {
             const int y = y0 + r;
             double2* grow = a.X + ((size_t)y * nh + kx) * n;
@@ -165,36 +155,15 @@ __global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL:
                     const double D = dbuf[(size_t)r * mzs + kzs[q]];
                     const double rD = __drcp_rn(D);  // off the recurrence's chain
                     if (y == 0) {
-                        v.x = div_by_recip_flagged(v.x, D, rD, outside[q]);
-                        v.y = div_by_recip_flagged(v.y, D, rD, outside[q]);
+                        v.x = div_by_recip(v.x, D, rD);
+                        v.y = div_by_recip(v.y, D, rD);
                     } else {
                         const double av = is00[q] ? bA0[y] : bA[y];
-                        v.x = div_by_recip_flagged(__dsub_rn(v.x, __dmul_rn(av, prev[q].x)), D, rD, outside[q]);
-                        v.y = div_by_recip_flagged(__dsub_rn(v.y, __dmul_rn(av, prev[q].y)), D, rD, outside[q]);
+                        v.x = div_by_recip(__dsub_rn(v.x, __dmul_rn(av, prev[q].x)), D, rD);
+                        v.y = div_by_recip(__dsub_rn(v.y, __dmul_rn(av, prev[q].y)), D, rD);
                     }
                     prev[q] = v;
                     grow[slot[q]] = v;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < LPT; q++) {
-            if (outside[q]) {
-                prev[q] = prev0[q];
-                for (int r = 0; r < nr; r++) {
-                    const int y = y0 + r;
-                    double2 v = buf[sidx<true>(r * n + slot[q])];
-                    const double D = dbuf[(size_t)r * mzs + kzs[q]];
-                    if (y == 0) {
-                        v.x = __ddiv_rn(v.x, D);
-                        v.y = __ddiv_rn(v.y, D);
-                    } else {
-                        const double av = is00[q] ? bA0[y] : bA[y];
-                        v.x = __ddiv_rn(__dsub_rn(v.x, __dmul_rn(av, prev[q].x)), D);
-                        v.y = __ddiv_rn(__dsub_rn(v.y, __dmul_rn(av, prev[q].y)), D);
-                    }
-                    prev[q] = v;
-                    a.X[((size_t)y * nh + kx) * n + slot[q]] = v;
                 }
             }
         }

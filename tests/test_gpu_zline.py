@@ -92,9 +92,8 @@ def test_default_rule_and_tuning(cuda_device, monkeypatch):
 @pytest.mark.parametrize("scale", [2.0 ** -960, 2.0 ** -1010])
 def test_line_kernel_outside_the_fast_division_window(cuda_device, monkeypatch, oracle, scale):
     """Right-hand sides so small that the forward sweeps' quotients leave the window of the
-    reciprocal-and-correction division (|q| < 2^-900; subnormal inputs at 2^-1010): the
-    per-wavenumber kernel redoes those chunks with IEEE division, the split Thomas takes its
-    fallback per quotient, and both still agree bit for bit."""
+    reciprocal-and-correction division (|q| < 2^-900; subnormal inputs at 2^-1010): both
+    kernels take IEEE division for those quotients and still agree bit for bit."""
     import prj
     import workloads
     nx, ny, nz = 64, 21, 384
