@@ -267,8 +267,9 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None, tune=True):
     """64 independent Poisson solves of uneven sizes in one launch: sizes from default_rng(2)
     (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]), uniform[-1,1]
     right-hand sides minus their dy-weighted mean; launch shapes from the autotuner.  FP64: the
-    persistent work-queue kernel (one kernel per batch); FP32-storage + FP64 refinement: one CUDA
-    graph of the per-case kernels."""
+    persistent work-queue kernel (one kernel per batch), and beside it the CUDA-graph form of the
+    per-case kernels (fp64_graph); FP32-storage + FP64 refinement: one CUDA graph of the per-case
+    kernels."""
     import numpy as np
     import torch
     import autotune
@@ -311,14 +312,15 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None, tune=True):
     out = {"cases": 64, "points": pts, "distinct_sizes": len(tuned), "setup_s": t_tune,
            "sharding": f"{world} rank(s), cases partitioned by size"}
     stream = torch.cuda.current_stream(device)
-    for name, mode in (("fp64", prj.MODE_FP64), ("mixed", prj.MODE_FP32_REFINE)):
+    for name, mode, graph in (("fp64", prj.MODE_FP64, False), ("fp64_graph", prj.MODE_FP64, True),
+                              ("mixed", prj.MODE_FP32_REFINE, False)):
         if mode == prj.MODE_FP32_REFINE:  # the mixed path runs the split z kernels
             for p in plans:
                 t = p.tuning
                 if t["z_mode"] != 0:
                     p.set_tuning(t["x_rows"], 0, 0)
         work = [r.clone() for r in rhs]
-        with prj.Batch(plans, work, mode=mode) as batch:
+        with prj.Batch(plans, work, mode=mode, graph=graph) as batch:
             def reset():
                 for w_, r_ in zip(work, rhs):
                     w_.copy_(r_)
@@ -419,7 +421,8 @@ def run_rough(device, nx, ny, nz, steps, warmup):
     del Uf, Vf, Wf
     with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent", device=device.index or 0) as plan:
         P64 = None
-        for name, mode in (("fp64", prj.MODE_FP64), ("mixed", prj.MODE_FP32_REFINE)):
+        for name, mode, graph in (("fp64", prj.MODE_FP64, False), ("fp64_graph", prj.MODE_FP64, True),
+                              ("mixed", prj.MODE_FP32_REFINE, False)):
             fn = lambda: plan.projection_step(Uh, Vh, Wh, U, V, W, P, 1.0, mode=mode, stats=False, stream=stream)
             for _ in range(warmup):
                 fn()

@@ -1253,6 +1253,8 @@ int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int
     if (!out) return fail(PRJ_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (!plans || !d_P || ncases < 1) return fail(PRJ_ERR_ARG, "need ncases >= 1 plans and arrays");
+    const bool graph_form = (mode & PRJ_BATCH_GRAPH) != 0;
+    mode &= ~PRJ_BATCH_GRAPH;
     if (mode != PRJ_MODE_FP64 && mode != PRJ_MODE_FP32_REFINE) return fail(PRJ_ERR_ARG, "unknown mode %d", mode);
     const int dev = plans[0] ? plans[0]->device : 0;
     for (int i = 0; i < ncases; i++) {
@@ -1265,8 +1267,10 @@ int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int
         if (mode == PRJ_MODE_FP32_REFINE && (rc = mixed_supported(plans[i]))) return rc;
     }
     DeviceGuard dg(dev);
-    bool persistent = (mode == PRJ_MODE_FP64);
-    for (int i = 0; i < ncases && persistent; i++) persistent = prj::batchk_supported(plans[i]);
+    bool persistent = (mode == PRJ_MODE_FP64) && !graph_form;
+    // the persistent kernel reads P as 16-byte pairs (and copies it with 16-byte cp.async)
+    for (int i = 0; i < ncases && persistent; i++)
+        persistent = prj::batchk_supported(plans[i]) && ((uintptr_t)d_P[i] & 15u) == 0;
     if (persistent) {
         prj_batch* b = new prj_batch();
         b->device = dev;

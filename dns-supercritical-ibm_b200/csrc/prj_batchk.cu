@@ -44,6 +44,7 @@ struct __align__(16) BatchCaseDev {
     ThomasArgs t;     // its Thomas lines
     int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in PRJ_BATCH_PLANS
     int ntz;          // x tiles per y plane
+    int soff;         // byte offset in shared memory of the x tiles' staged input
     int tiles[kBNumStages];
 };
 
@@ -74,42 +75,74 @@ namespace {
     X(14, 256, 8, 8, 4)
 
 constexpr int kBatchThreads = kPassThreads;  // = kThomasTile
+#ifndef PRJ_BATCH_MINB
+#define PRJ_BATCH_MINB 6
+#endif
+// resident CTAs per SM the register allocation is held to (6: at most 80 registers per
+// thread, the per-case x and z kernels' own allocation)
+constexpr int kBatchMinBlocks = PRJ_BATCH_MINB;
 static_assert(kPassThreads == kThomasTile, "one CTA shape for every stage");
 
 // Every (stage, plan) tile is its own non-inlined function: inlined into one switch, the
 // thirty plan variants' butterflies shared one register allocation and spilled (2 KB of
 // stack per thread); as calls, each tile function is allocated on its own, as in its
 // per-case kernel.
+//
+// The x stages run an item's tiles as a pipeline: the next tile's input is copied into
+// shared memory (cp.async) while the current tile computes, so a CTA keeps loads in
+// flight through its FFT passes and stores instead of one round trip per tile.
 template <class PL>
-__device__ __noinline__ void tile_x_fwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    fwd_xp_tile<0, PL>(c.x, sm, tile % c.ntz, tile / c.ntz);
+__device__ __noinline__ void run_x_fwd_tiles(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
+    double2* S = reinterpret_cast<double2*>(sm + c.soff);
+    fwd_xp_stage<PL>(c.x, S, t0 % c.ntz, t0 / c.ntz);
+    for (int t = t0; t < t0 + count; t++) {
+        cp_async_wait<0>();
+        __syncthreads();  // S holds tile t for every thread; A is free
+        const int nt = t + 1;
+        fwd_xp_tile<2, PL>(c.x, sm, t % c.ntz, t / c.ntz, S, [&] {
+            if (nt < t0 + count) fwd_xp_stage<PL>(c.x, S, nt % c.ntz, nt / c.ntz);
+        });
+    }
 }
 template <class PL>
-__device__ __noinline__ void tile_x_bwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    bwd_xp_tile<PL, false>(c.x, sm, tile % c.ntz, tile / c.ntz, c.ntz);
+__device__ __noinline__ void run_x_bwd_tiles(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
+    double2* S = reinterpret_cast<double2*>(sm + c.soff);
+    bwd_xp_stage<PL>(c.x, S, t0 % c.ntz, t0 / c.ntz);
+    for (int t = t0; t < t0 + count; t++) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int nt = t + 1;
+        bwd_xp_tile<PL, false, true>(c.x, sm, t % c.ntz, t / c.ntz, c.ntz, S, [&] {
+            if (nt < t0 + count) bwd_xp_stage<PL>(c.x, S, nt % c.ntz, nt / c.ntz);
+        });
+    }
 }
 template <int DIR, class PL>
 __device__ __noinline__ void tile_z(const BatchCaseDev& c, int tile, unsigned char* sm) {
     zfft_pass_tile<DIR, double2, PL, (DIR > 0)>(c.z, reinterpret_cast<double2*>(sm), tile);
 }
-// four planes per load block: the eight of k_thomas need more than the kernel's 128
-// registers per thread
-__device__ __noinline__ void tile_thomas(const BatchCaseDev& c, int tile) { thomas_line<double2, 4>(c.t, tile); }
+// the lines streamed through a cp.async ring of kRingStages stages of kRingPlanes planes
+// (the per-case kernels' k_thomas_async; the plane loads wait in shared memory, not in
+// registers, so the tile fits the kernel's register cap)
+constexpr int kRingPlanes = 2, kRingStages = 4;
+__device__ __noinline__ void tile_thomas(const BatchCaseDev& c, int tile, unsigned char* sm) {
+    thomas_line_async<double2, kRingPlanes, kRingStages>(c.t, tile, sm);
+}
 
-__device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
+__device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
     switch (c.xplan) {
 #define PRJ_BX(I, N, ...) \
-    case I: tile_x_fwd<PassList<__VA_ARGS__>>(c, tile, sm); break;
+    case I: run_x_fwd_tiles<PassList<__VA_ARGS__>>(c, t0, count, sm); break;
         PRJ_BATCH_PLANS(PRJ_BX)
 #undef PRJ_BX
     default: break;
     }
 }
 
-__device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int tile, unsigned char* sm) {
+__device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
     switch (c.xplan) {
 #define PRJ_BX(I, N, ...) \
-    case I: tile_x_bwd<PassList<__VA_ARGS__>>(c, tile, sm); break;
+    case I: run_x_bwd_tiles<PassList<__VA_ARGS__>>(c, t0, count, sm); break;
         PRJ_BATCH_PLANS(PRJ_BX)
 #undef PRJ_BX
     default: break;
@@ -127,7 +160,7 @@ __device__ __forceinline__ void run_z(const BatchCaseDev& c, int tile, unsigned 
     }
 }
 
-__global__ void __launch_bounds__(kBatchThreads, 4)
+__global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
     k_batch(const BatchCaseDev* __restrict__ cases, const BatchSeg* __restrict__ segs, int nseg,
             unsigned long long* counter, int* done, int* err) {
     extern __shared__ __align__(16) unsigned char bsm[];
@@ -175,15 +208,19 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
         }
         const BatchCaseDev& c = s_case;
         if (!s_skip) {
-            for (int tile = g.tile0; tile < g.tile0 + g.count; tile++) {
-                switch (g.stage) {
-                case kBFwdX: run_x_fwd(c, tile, bsm); break;
-                case kBZFwd: run_z<-1>(c, tile, bsm); break;
-                case kBThomas: tile_thomas(c, tile); break;
-                case kBZInv: run_z<+1>(c, tile, bsm); break;
-                default: run_x_bwd(c, tile, bsm); break;
+            if (g.stage == kBFwdX) {
+                run_x_fwd(c, g.tile0, g.count, bsm);
+            } else if (g.stage == kBBwdX) {
+                run_x_bwd(c, g.tile0, g.count, bsm);
+            } else {
+                for (int tile = g.tile0; tile < g.tile0 + g.count; tile++) {
+                    switch (g.stage) {
+                    case kBZFwd: run_z<-1>(c, tile, bsm); break;
+                    case kBThomas: tile_thomas(c, tile, bsm); break;
+                    default: run_z<+1>(c, tile, bsm); break;
+                    }
+                    __syncthreads();  // bsm free for the next tile
                 }
-                __syncthreads();  // bsm free for the next tile
             }
         }
         __syncthreads();  // every thread's stores of the item
@@ -193,6 +230,10 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
         }
     }
 }
+
+// shared memory of an x tile's staged input (the inverse's m+1 spectrum rows of tz)
+size_t x_stage_bytes(int m, int tz) { return (size_t)(m + 1) * tz * sizeof(double2); }
+constexpr size_t kXStagedBytes = 32 * 1024;
 
 int batch_plan_index(int n, const DifDev& f) {
 #define PRJ_BI(I, N, ...) \
@@ -219,10 +260,13 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
         BatchCaseDev& c = cs[i];
         c.x = batch_x_args(pl, d_P[i]);
         c.z = batch_z_args(pl);
-        // tile shapes within the per-case kernels' default shared-memory budgets (28-32 KB),
-        // so four CTAs fit per SM whatever the plans' own tuning; a tile's shape does not
-        // change its results
-        c.x.tz = std::min(c.x.tz, choose_tz_xp(pl->fx64.m));
+        // tile shapes within the per-case kernels' default shared-memory budgets, the x
+        // tiles with their staged input within kXStagedBytes, so six CTAs fit per SM
+        // whatever the plans' own tuning; a tile's shape does not change its results
+        const int m = pl->fx64.m;
+        c.x.tz = std::min(c.x.tz, choose_tz_xp(m));
+        while (c.x.tz > 1 && pass_x_smem(m, c.x.tz) + x_stage_bytes(m, c.x.tz) > kXStagedBytes) c.x.tz /= 2;
+        c.soff = (int)pass_x_smem(m, c.x.tz);
         c.z.rb = std::min(c.z.rb, batch_z_default_rows(g.nz));
         c.t = thomas_args(pl, pl->spec, 0, g.nxh);
         c.xplan = batch_plan_index(pl->fx64.m, pl->xd.f);
@@ -231,8 +275,9 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
         c.tiles[kBFwdX] = c.tiles[kBBwdX] = c.ntz * g.ny;
         c.tiles[kBZFwd] = c.tiles[kBZInv] = (c.z.nrow_total + c.z.rb - 1) / c.z.rb;
         c.tiles[kBThomas] = g.nxh * c.t.tiles;
-        smem = std::max(smem, pass_x_smem(pl->fx64.m, c.x.tz));
+        smem = std::max(smem, pass_x_smem(m, c.x.tz) + x_stage_bytes(m, c.x.tz));
         smem = std::max(smem, (size_t)padded_len(c.z.rb * g.nz, true) * sizeof(double2));
+        smem = std::max(smem, thomas_async_smem<double2, kRingPlanes, kRingStages>());
     }
     // stage-major order; within a stage the cases with the most tiles first; each stage of a
     // case cut into items of up to 16 tiles (about 64 items per stage where it has that

@@ -2,10 +2,12 @@
 //
 // zfft_pass_tile: rb spectral z-rows of one buffer, in-place pass-plan FFT (forward:
 // natural z order -> slot order; inverse: slot order -> natural).  thomas_line: the
-// Thomas sweeps of one line (kx, slot) per thread, 128 lines per tile.  The kernels of
+// Thomas sweeps of one line (kx, slot) per thread, 128 lines per tile; thomas_line_async:
+// the same sweeps with the planes streamed through a cp.async shared-memory ring.  The kernels of
 // prj_zsplit.cu run one tile per CTA; the persistent batch kernel (prj_batchk.cu) runs
 // tiles of many cases from a work queue with the same code, so both give the same bits.
 #pragma once
+#include "cp_async.cuh"
 #include "div_rn.cuh"
 #include "fft_pass.cuh"
 
@@ -163,6 +165,124 @@ __device__ __forceinline__ void thomas_line(const ThomasArgs& a, int blk) {
             }
         }
     }
+}
+
+// The same line solve with the planes streamed through a ring of NS shared-memory
+// stages of B planes by cp.async (global -> shared, no register staging): while a
+// thread computes block b it already has blocks b+1 .. b+NS-1 in flight, so the
+// sequential recurrence no longer waits on one memory round trip per block.  Each
+// thread copies exactly the elements it consumes (its own line), so a thread only
+// waits for its own copy groups and no CTA barrier is needed.  Arithmetic and
+// order are those of thomas_line, so the results are bit-identical.
+template <typename T, int B, int NS>
+__device__ __forceinline__ void thomas_line_async(const ThomasArgs& a, int blk, unsigned char* sm) {
+    const int kb = blk / a.tiles;
+    const int kx = a.kx0 + kb;
+    const int slot = (blk - kb * a.tiles) * kThomasTile + threadIdx.x;
+    if (slot >= a.nz) return;  // a thread leaves only its own copy groups behind: none issued
+    const int nz = a.nz, ny = a.ny, nh = a.nh, mzp = a.mzp, tid = threadIdx.x;
+    const int kz = a.kz_of_slot[slot];
+    const int kzs = kz <= nz - kz ? kz : nz - kz;
+    const bool is00 = (kx == 0 && kz == 0);
+    const double* A = a.bands + (is00 ? 3 : 0) * ny;
+    const size_t rstride = (size_t)a.nhb * nz;
+    const size_t pstride = (size_t)nh * mzp;
+    T* x = static_cast<T*>(a.X) + (size_t)kb * nz + slot;
+    const double* d = a.piv + (size_t)kx * mzp + kzs;
+    const double* dc = a.pivc + (size_t)kx * mzp + kzs;
+    T* Xs = reinterpret_cast<T*>(sm);                                        // [NS][B][tile]
+    double* Ds = reinterpret_cast<double*>(sm + (size_t)NS * B * kThomasTile * sizeof(T));  // [NS][B][tile]
+    auto xs = [&](int st, int u) -> T& { return Xs[((size_t)st * B + u) * kThomasTile + tid]; };
+    auto ds = [&](int st, int u) -> double& { return Ds[((size_t)st * B + u) * kThomasTile + tid]; };
+    const int nb = (ny + B - 1) / B;
+
+    // forward sweep, y ascending: block b = planes b B .. b B + B - 1
+    auto issue_f = [&](int b) {
+        if (b < nb) {
+            const int st = b % NS;
+            for (int u = 0; u < B; u++) {
+                const int y = b * B + u;
+                if (y < ny) {
+                    cp_async(&xs(st, u), x + (size_t)y * rstride, (int)sizeof(T));
+                    cp_async(&ds(st, u), d + (size_t)y * pstride, 8);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int b = 0; b < NS - 1; b++) issue_f(b);
+    double2 prev = make_double2(0.0, 0.0);
+    for (int b = 0; b < nb; b++) {
+        issue_f(b + NS - 1);
+        cp_async_wait<NS - 1>();
+        const int st = b % NS;
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int y = b * B + u;
+            if (y < ny) {
+                double2 r = to_d2(xs(st, u));
+                const double D = ds(st, u);
+                const double rD = __drcp_rn(D);  // off the recurrence's chain
+                if (y == 0) {
+                    r.x = div_by_recip(r.x, D, rD);
+                    r.y = div_by_recip(r.y, D, rD);
+                } else {
+                    const double av = A[y];
+                    r.x = div_by_recip(__dsub_rn(r.x, __dmul_rn(av, prev.x)), D, rD);
+                    r.y = div_by_recip(__dsub_rn(r.y, __dmul_rn(av, prev.y)), D, rD);
+                }
+                prev = r;
+                if (y < ny - 1) from_d2(x[(size_t)y * rstride], r);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    // the backward sweep reads what this thread just stored: complete those stores first
+    __threadfence();
+    from_d2(x[(size_t)(ny - 1) * rstride], prev);
+    // backward sweep, y descending from ny-2: block b = planes ny-2 - b B - u
+    const int nbb = (ny - 1 + B - 1) / B;
+    auto issue_b = [&](int b) {
+        if (b < nbb) {
+            const int st = b % NS;
+            for (int u = 0; u < B; u++) {
+                const int y = ny - 2 - b * B - u;
+                if (y >= 0) {
+                    cp_async(&xs(st, u), x + (size_t)y * rstride, (int)sizeof(T));
+                    cp_async(&ds(st, u), dc + (size_t)y * pstride, 8);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int b = 0; b < NS - 1; b++) issue_b(b);
+    for (int b = 0; b < nbb; b++) {
+        issue_b(b + NS - 1);
+        cp_async_wait<NS - 1>();
+        const int st = b % NS;
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int y = ny - 2 - b * B - u;
+            if (y >= 0) {
+                const double c = ds(st, u);  // c_y / D_y, tabulated with the pivots
+                const double2 v = to_d2(xs(st, u));
+                double2 r;
+                r.x = __dsub_rn(v.x, __dmul_rn(prev.x, c));
+                r.y = __dsub_rn(v.y, __dmul_rn(prev.y, c));
+                prev = r;
+                from_d2(x[(size_t)y * rstride], r);
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// ring shape (planes per stage B x stages NS) of the streamed kernel
+template <typename T, int B, int NS>
+constexpr size_t thomas_async_smem() {
+    return (size_t)NS * B * kThomasTile * (sizeof(T) + sizeof(double));
 }
 
 // arguments of a plan's FP64 spectrum rows for zfft_pass_tile, and of its Thomas lines

@@ -41,6 +41,7 @@ PRJ_ERR_STATE = -7
 
 MODE_FP64 = 0
 MODE_FP32_REFINE = 1
+BATCH_GRAPH = 0x10  # or-ed into a batch's mode: the CUDA-graph form
 
 # every symbol include/projection.h declares
 EXPORTS = (
@@ -611,10 +612,10 @@ def read_field(path, out=None, halo=False):
 class Batch:
     """Many independent in-place Poisson solves in one launch (prj_batch_create /
     prj_batch_launch): one persistent kernel over a work queue for FP64 cases of the
-    pass-plan lengths up to 256, else one CUDA graph.  Case i solves plans[i] on
-    tensors[i]."""
+    pass-plan lengths up to 256, else (or with graph=True) one CUDA graph.  Case i
+    solves plans[i] on tensors[i]."""
 
-    def __init__(self, plans, tensors, mode=MODE_FP64):
+    def __init__(self, plans, tensors, mode=MODE_FP64, graph=False):
         if len(plans) != len(tensors) or not plans:
             raise ValueError("need one tensor per plan")
         L = load_library()
@@ -622,7 +623,7 @@ class Batch:
         hp = (_vp * n)(*[p.handle for p in plans])
         hd = (_vp * n)(*[ctypes.c_void_p(t.data_ptr()) for t in tensors])
         h = _vp()
-        _check(L.prj_batch_create(hp, hd, n, mode, ctypes.byref(h)))
+        _check(L.prj_batch_create(hp, hd, n, mode | (BATCH_GRAPH if graph else 0), ctypes.byref(h)))
         self._h = h
         self._keep = (list(plans), list(tensors))  # the graph holds their addresses
 

@@ -46,6 +46,8 @@ enum prj_status {
 /* precision modes of prj_projection_step */
 #define PRJ_MODE_FP64 0            /* plain FP64 path: the drop-in */
 #define PRJ_MODE_FP32_REFINE 1     /* FP32 spectral work + FP64 iterative refinement */
+/* or-ed into prj_batch_create's mode: the CUDA-graph form where the persistent kernel applies */
+#define PRJ_BATCH_GRAPH 0x10
 
 typedef struct prj_plan prj_plan;
 
@@ -274,12 +276,14 @@ int prj_geom_read_base_params(const char* path, prj_case_params* out);
  * change while the batch exists.  No counterpart in the reference, which solves
  * one grid per run (and plans it once, poisson_solver_multigpu.f90:77-129).
  *   FP64, every case with even nx, nx/2 and nz among the pass-plan lengths up to
- *   256 (16, 24, 32, 48, 64, 96, 128, 192, 256): one persistent kernel runs all
+ *   256 (16, 24, 32, 48, 64, 96, 128, 192, 256) and a 16-byte aligned array: one
+ *   persistent kernel runs all
  *   cases from a work queue of (case, stage, tile) items in stage-major order,
  *   with bounded waits on per-case stage counters; prj_batch_launch issues a
  *   counter reset and that one kernel (both capturable in a CUDA graph).
- *   Otherwise (FP32 + refinement, other lengths): one CUDA graph holding every
- *   case's kernels on parallel branches, replayed by one graph launch.
+ *   Otherwise (FP32 + refinement, other lengths, or mode | PRJ_BATCH_GRAPH): one
+ *   CUDA graph holding every case's kernels on parallel branches, replayed by one
+ *   graph launch.
  * Each case's P equals its own prj_poisson_fp64 / prj_poisson_mixed bit for bit.
  * prj_batch_info: whether the batch is persistent, its kernel launches per
  * prj_batch_launch, and its work items.  prj_batch_check_error waits for

@@ -99,6 +99,28 @@ def test_persistent_batch_equals_single_solves(cuda_device, oracle):
     torch.cuda.synchronize()
 
 
+def test_forced_graph_form_equals_persistent(cuda_device):
+    """mode | PRJ_BATCH_GRAPH keeps the CUDA-graph form for cases the persistent kernel could
+    run; both forms give the same bits."""
+    import prj
+    cases = _cases(PERSISTENT_SHAPES[:5], 11)
+    plans = [prj.Plan(r.shape[0], r.shape[1], r.shape[2], dx, dz, b) for r, _, dx, dz, b in cases]
+    outs = {}
+    for graph in (False, True):
+        tensors = [to_dev(r) for r, *_ in cases]
+        with prj.Batch(plans, tensors, graph=graph) as batch:
+            assert batch.info["persistent"] == (not graph)
+            for t, (r, *_rest) in zip(tensors, cases):
+                t.copy_(to_dev(r))
+            batch.launch()
+            batch.check_error()
+            outs[graph] = [from_dev(t) for t in tensors]
+    for a, b in zip(outs[False], outs[True]):
+        np.testing.assert_array_equal(a, b)
+    for p in plans:
+        p.close()
+
+
 def test_graph_batch_for_other_lengths(cuda_device):
     """A case outside the persistent kernel's lengths (nx/2 = 15) keeps the graph form."""
     import prj
@@ -165,3 +187,38 @@ def test_autotune_keeps_results(cuda_device, tmp_path, monkeypatch):
         assert again["cached"]
         with pytest.raises(prj.PrjError):
             plan.set_tuning(3, 0, 0)
+
+
+def test_misaligned_array_keeps_graph_form(cuda_device):
+    """An array that is not 16-byte aligned (the persistent kernel reads P in 16-byte pairs)
+    makes the batch use the graph form, with the bits of the per-case solve of the same
+    array."""
+    import prj
+    import torch
+    cases = _cases(PERSISTENT_SHAPES[:2], 13)
+    plans = [prj.Plan(r.shape[0], r.shape[1], r.shape[2], dx, dz, b) for r, _, dx, dz, b in cases]
+
+    def misaligned(r):
+        d = to_dev(r)
+        store = torch.zeros(d.numel() + 1, dtype=torch.float64, device=d.device)
+        t = store[1:].view(d.shape)  # 8 bytes past a 16-byte boundary
+        t.copy_(d)
+        assert t.data_ptr() % 16 == 8
+        return t
+
+    single0 = misaligned(cases[0][0])
+    plans[0].poisson_fp64(single0)
+    single1 = to_dev(cases[1][0])
+    plans[1].poisson_fp64(single1)
+    singles = [from_dev(single0), from_dev(single1)]
+    tensors = [misaligned(cases[0][0]), to_dev(cases[1][0])]
+    with prj.Batch(plans, tensors) as batch:
+        assert not batch.info["persistent"]
+        for t, (r, *_rest) in zip(tensors, cases):
+            t.copy_(to_dev(r))
+        batch.launch()
+        torch.cuda.synchronize()
+        for t, want in zip(tensors, singles):
+            np.testing.assert_array_equal(from_dev(t), want)
+    for p in plans:
+        p.close()
