@@ -267,8 +267,9 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None, tune=True):
     """64 independent Poisson solves of uneven sizes in one launch: sizes from default_rng(2)
     (Nx, Nz in {64,96,128,192,256}, Ny in {48,64,96,128}, tanh beta ~ U[1.5,2.5]), uniform[-1,1]
     right-hand sides minus their dy-weighted mean; launch shapes from the autotuner.  FP64: the
-    persistent work-queue kernel (one kernel per batch), and beside it the CUDA-graph form of the
-    per-case kernels (fp64_graph); FP32-storage + FP64 refinement: one CUDA graph of the per-case
+    persistent work-queue kernel (one kernel per batch; its plans at the default tuning, since it
+    sets its own tile shapes), and beside it the CUDA-graph form of the autotuned per-case
+    kernels (fp64_graph); FP32-storage + FP64 refinement: one CUDA graph of the per-case
     kernels."""
     import numpy as np
     import torch
@@ -286,13 +287,14 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None, tune=True):
     mine = sharding.partition_cases([a * b * c for a, b, c, _ in specs_all], world)[rank]
     specs = [specs_all[i] for i in mine]
     seeds = [1000 + i for i in mine]
-    plans, rhs = [], []
+    plans, rhs, defaults = [], [], []
     t_tune = time.perf_counter()
     tuned = {}
     for i, (nx, ny, nz, beta) in enumerate(specs):
         yu = workloads.tanh_faces(ny, beta)
         dx, dz = workloads.channel_spacing(nx, nz)
         p = prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent"), device=device.index or 0)
+        defaults.append(p.tuning)
         if not tune:
             tuned[(nx, ny, nz)] = {}
         elif (nx, ny, nz) in tuned:
@@ -312,8 +314,13 @@ def run_batched(device, steps, warmup, rank=0, world=1, dist=None, tune=True):
     out = {"cases": 64, "points": pts, "distinct_sizes": len(tuned), "setup_s": t_tune,
            "sharding": f"{world} rank(s), cases partitioned by size"}
     stream = torch.cuda.current_stream(device)
+    tuned_t = [p.tuning for p in plans]
     for name, mode, graph in (("fp64", prj.MODE_FP64, False), ("fp64_graph", prj.MODE_FP64, True),
                               ("mixed", prj.MODE_FP32_REFINE, False)):
+        # the persistent kernel sets its own tile shapes: its plans keep the default tuning
+        # (radix orders included); the graph forms run the autotuned per-case kernels
+        for p, t in zip(plans, defaults if name == "fp64" else tuned_t):
+            p.set_tuning(**t)
         if mode == prj.MODE_FP32_REFINE:  # the mixed path runs the split z kernels
             for p in plans:
                 t = p.tuning

@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
@@ -39,22 +40,39 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    """Compile every source to an object in parallel (one nvcc per source, up to the host's
+    cores), then link the shared library."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc_path(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp", *SOURCES, "-lcudart"]
+    flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(REPO, "include")]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
+        flags.insert(0, "-Xptxas=-v")
     if extra:
-        cmd[1:1] = list(extra)
+        flags[0:0] = list(extra)
     if os.environ.get("PRJ_NVCC_FLAGS"):  # experiments: extra -D options
-        cmd[1:1] = os.environ["PRJ_NVCC_FLAGS"].split()
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libprj_b200.so")
+        flags[0:0] = os.environ["PRJ_NVCC_FLAGS"].split()
+    with tempfile.TemporaryDirectory(prefix="prj_build_") as tmp:
+        objs = [os.path.join(tmp, os.path.basename(src)[:-3] + ".o") for src in SOURCES]
+        jobs = list(zip(SOURCES, objs))
+        width = max(1, min(len(jobs), os.cpu_count() or 1))
+        logs = []
+        while jobs:
+            batch, jobs = jobs[:width], jobs[width:]
+            procs = [(src, subprocess.Popen([nvcc_path(), *flags, "-c", src, "-o", obj], stdout=subprocess.PIPE,
+                                            stderr=subprocess.STDOUT, text=True)) for src, obj in batch]
+            for src, p in procs:
+                out, _ = p.communicate()
+                logs.append(out)
+                if p.returncode != 0:
+                    sys.stderr.write(out)
+                    raise RuntimeError(f"nvcc failed on {os.path.basename(src)}")
+        res = subprocess.run([nvcc_path(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"],
+                             capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("nvcc failed linking libprj_b200.so")
     if verbose:
-        sys.stderr.write(res.stderr)
+        sys.stderr.write("".join(logs))
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -16,4 +16,9 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// no action (the default hook of the tiles that can stage their next input)
+struct NoHook {
+    __device__ __forceinline__ void operator()() const {}
+};
+
 }  // namespace prj

@@ -160,19 +160,12 @@ int make_slot_table(int n, int** d_out, size_t* bytes, int order = 0) {
     return PRJ_OK;
 }
 
-// z-direction kernel choice: PRJ_ZSOLVE=split|fused|basic|line (split and line need the
-// in-place plan).  By default the per-wavenumber kernel when there are at least two x
-// wavenumbers (its CTAs) per SM, else the split kernels: measured on B200, the
-// per-wavenumber kernel took 1.12 / 1.41 / 6.91 ms against 1.31 / 1.49 / 7.87 ms for
-// nx/2+1 = 385 / 513 / 769, but 0.30 / 0.45 ms against 0.21 / 0.37 ms for 193 / 257.
-int z_mode(bool split_ok, bool line_pref) {
-    const char* v = getenv("PRJ_ZSOLVE");
-    if (v && !strcmp(v, "fused")) return 1;
-    if (v && !strcmp(v, "basic")) return 2;
-    if (v && !strcmp(v, "line")) return split_ok ? 3 : 1;
-    if (v && !strcmp(v, "split")) return split_ok ? 0 : 1;
-    return split_ok ? (line_pref ? 3 : 0) : 1;
-}
+// default z-direction kernels (prj_tuning.z_mode changes them; split and line need the
+// in-place plan): the per-wavenumber kernel when there are at least two x wavenumbers
+// (its CTAs) per SM, else the split kernels.  Measured on B200, the per-wavenumber kernel
+// took 1.12 / 1.41 / 6.91 ms against 1.31 / 1.49 / 7.87 ms for nx/2+1 = 385 / 513 / 769,
+// but 0.30 / 0.45 ms against 0.21 / 0.37 ms for 193 / 257.
+int z_mode(bool split_ok, bool line_pref) { return split_ok ? (line_pref ? 3 : 0) : 1; }
 
 void free_plan_buffers(prj_plan* pl) {
     dfree(pl->t.bands);
@@ -646,15 +639,10 @@ int prj_plan_create(int nx, int nz, int ny, double dx, double dz, const double* 
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, pl->device) != cudaSuccess) sms = 0;
         pl->zmode = z_mode(pl->zd.ok && pl->kz_of_slot, sms > 0 && g.nxh >= 2 * sms);
     }
-    {
-        // PRJ_FFT_KERNELS=runtime keeps the runtime-radix kernels for lengths with a pass plan
-        const char* v = getenv("PRJ_FFT_KERNELS");
-        pl->use_pass = !(v && !strcmp(v, "runtime"));
-        // PRJ_THOMAS_ASYNC: -1 (default) streams the mixed-storage Thomas only, 0 never,
-        // 1..4 always with ring shape 4x4, 8x2, 2x8, 8x3 (planes x stages)
-        const char* ta = getenv("PRJ_THOMAS_ASYNC");
-        pl->thomas_async = ta ? atoi(ta) : -1;
-    }
+    // pass-plan kernels wherever the length has a plan; the Thomas ring for the
+    // mixed-storage solve only (prj_tuning.thomas_ring changes it)
+    pl->use_pass = true;
+    pl->thomas_async = -1;
     pl->kxs = g.nxh;
     pl->tz_xd = prj::choose_tz_xd(pl->fx64.m, pl->fx64.even);
     pl->tz_xp = prj::choose_tz_xp(pl->fx64.m);

@@ -2,17 +2,18 @@
 //
 // A batch of independent solves (the reference solves one grid per run and plans it
 // once, poisson_solver_multigpu.f90:77-129; here every case keeps its own plan) is a
-// list of work items (case, stage, tiles).  The five stages of a solve are the split
-// path's kernels -- forward x transform, forward z transform, Thomas sweeps, inverse z
-// transform, inverse x transform -- and a tile is what one CTA of that kernel does; an
-// item is a run of up to 16 tiles of one stage of one case.  The host orders the items
-// stage-major (every case's forward x items, then every case's forward z items, ...),
-// largest cases first within a stage, and one launch of k_batch runs them all:
+// list of work items (case, stage, tiles).  The three stages of a solve are the forward
+// x transform (tiles of tz x-rows of one y plane), the z solve of one x wavenumber (z
+// FFT, both Thomas sweeps and inverse z FFT: k_zline's tile), and the inverse x
+// transform; an x item is a run of up to 16 tiles of one case, a z item one wavenumber.
+// The host orders the items stage-major (every case's forward x items, then every case's
+// z items, then the inverse x items), the largest tiles first within a stage, and one
+// launch of k_batch runs them all:
 //
 //   a CTA takes the next item index from a global counter (atomicAdd), waits until the
 //   case's previous stage has completed all its tiles (a per-case, per-stage counter,
 //   read with acquire semantics), runs the item's tiles with the same device functions as
-//   the per-case kernels (xfft_tiles.cuh, zsplit_tiles.cuh), and counts them done
+//   the per-case kernels (xfft_tiles.cuh, zline_tiles.cuh), and counts them done
 //   (release);
 //   items are taken in order, and an item depends only on items before it, all of which
 //   are held by running CTAs that wait only on earlier items, so the queue cannot
@@ -22,26 +23,28 @@
 //   continues; prj_batch_check_error reports PRJ_ERR_TIMEOUT.
 //
 // The tiles run the per-case kernels' code on the same elements, so every case's P
-// equals its own prj_poisson_fp64 bit for bit.  One launch replaces ncases x 5 small
-// kernels, their launch gaps and their tails.  Counters are reset by a memset issued
+// equals its own prj_poisson_fp64 bit for bit (the z solve of k_zline is bitwise that of
+// the split z kernels).  One launch replaces ncases x 3 to 5 small kernels, their launch
+// gaps and their tails, and the fused z solve moves the spectrum through HBM four times
+// where the split kernels move it eight.  Counters are reset by a memset issued
 // with the launch, so the pair can be captured in a CUDA graph.
 #include <algorithm>
+#include <array>
 #include <vector>
 
 #include "prj_internal.h"
 #include "tma_util.cuh"
 #include "xfft_tiles.cuh"
-#include "zsplit_tiles.cuh"
+#include "zline_tiles.cuh"
 
 namespace prj {
 
 // stages of one solve
-enum BatchStage { kBFwdX = 0, kBZFwd = 1, kBThomas = 2, kBZInv = 3, kBBwdX = 4, kBNumStages = 5 };
+enum BatchStage { kBFwdX = 0, kBZLine = 1, kBBwdX = 2, kBNumStages = 3 };
 
 struct __align__(16) BatchCaseDev {
     XArgs x;          // forward (source P) and inverse (P out) x transforms of the case
-    ZfftArgs z;       // its z rows (ny nh rows of nz)
-    ThomasArgs t;     // its Thomas lines
+    ZLineArgs zl;     // its z solves (one tile per x wavenumber)
     int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in PRJ_BATCH_PLANS
     int ntz;          // x tiles per y plane
     int soff;         // byte offset in shared memory of the x tiles' staged input
@@ -74,22 +77,21 @@ namespace {
     X(13, 256, 4, 8, 8)    \
     X(14, 256, 8, 8, 4)
 
-constexpr int kBatchThreads = kPassThreads;  // = kThomasTile
+constexpr int kBatchThreads = kPassThreads;
 #ifndef PRJ_BATCH_MINB
 #define PRJ_BATCH_MINB 6
 #endif
 // resident CTAs per SM the register allocation is held to (6: at most 80 registers per
-// thread, the per-case x and z kernels' own allocation)
+// thread, the per-case x kernels' own allocation)
 constexpr int kBatchMinBlocks = PRJ_BATCH_MINB;
-static_assert(kPassThreads == kThomasTile, "one CTA shape for every stage");
 
 // Every (stage, plan) tile is its own non-inlined function: inlined into one switch, the
 // thirty plan variants' butterflies shared one register allocation and spilled (2 KB of
 // stack per thread); as calls, each tile function is allocated on its own, as in its
 // per-case kernel.
 //
-// The x stages run an item's tiles as a pipeline: the next tile's input is copied into
-// shared memory (cp.async) while the current tile computes, so a CTA keeps loads in
+// The x and z stages run an item's tiles as a pipeline: the next tile's input is copied
+// into shared memory (cp.async) while the current tile computes, so a CTA keeps loads in
 // flight through its FFT passes and stores instead of one round trip per tile.
 template <class PL>
 __device__ __noinline__ void run_x_fwd_tiles(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
@@ -117,16 +119,13 @@ __device__ __noinline__ void run_x_bwd_tiles(const BatchCaseDev& c, int t0, int 
         });
     }
 }
-template <int DIR, class PL>
-__device__ __noinline__ void tile_z(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    zfft_pass_tile<DIR, double2, PL, (DIR > 0)>(c.z, reinterpret_cast<double2*>(sm), tile);
-}
-// the lines streamed through a cp.async ring of kRingStages stages of kRingPlanes planes
-// (the per-case kernels' k_thomas_async; the plane loads wait in shared memory, not in
-// registers, so the tile fits the kernel's register cap)
-constexpr int kRingPlanes = 2, kRingStages = 4;
-__device__ __noinline__ void tile_thomas(const BatchCaseDev& c, int tile, unsigned char* sm) {
-    thomas_line_async<double2, kRingPlanes, kRingStages>(c.t, tile, sm);
+// the z solve of one wavenumber: ring of kZlStages stages of c.zl.yb planes, lines
+// spread over the CTA's threads
+constexpr int kZlStages = 2;
+__host__ __device__ constexpr int batch_lpt(int n) { return (n + kBatchThreads - 1) / kBatchThreads; }
+template <class PL>
+__device__ __noinline__ void tile_zline(const BatchCaseDev& c, int kx, unsigned char* sm) {
+    zline_tile<PL, kZlStages, batch_lpt(PL::n), kBatchThreads>(c.zl, kx, sm);
 }
 
 __device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
@@ -149,11 +148,10 @@ __device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int t0, int cou
     }
 }
 
-template <int DIR>
-__device__ __forceinline__ void run_z(const BatchCaseDev& c, int tile, unsigned char* sm) {
+__device__ __forceinline__ void run_zline(const BatchCaseDev& c, int kx, unsigned char* sm) {
     switch (c.zplan) {
 #define PRJ_BZ(I, N, ...) \
-    case I: tile_z<DIR, PassList<__VA_ARGS__>>(c, tile, sm); break;
+    case I: tile_zline<PassList<__VA_ARGS__>>(c, kx, sm); break;
         PRJ_BATCH_PLANS(PRJ_BZ)
 #undef PRJ_BZ
     default: break;
@@ -208,19 +206,15 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
         }
         const BatchCaseDev& c = s_case;
         if (!s_skip) {
-            if (g.stage == kBFwdX) {
-                run_x_fwd(c, g.tile0, g.count, bsm);
-            } else if (g.stage == kBBwdX) {
-                run_x_bwd(c, g.tile0, g.count, bsm);
-            } else {
-                for (int tile = g.tile0; tile < g.tile0 + g.count; tile++) {
-                    switch (g.stage) {
-                    case kBZFwd: run_z<-1>(c, tile, bsm); break;
-                    case kBThomas: tile_thomas(c, tile, bsm); break;
-                    default: run_z<+1>(c, tile, bsm); break;
-                    }
+            switch (g.stage) {
+            case kBFwdX: run_x_fwd(c, g.tile0, g.count, bsm); break;
+            case kBBwdX: run_x_bwd(c, g.tile0, g.count, bsm); break;
+            default:
+                for (int kx = g.tile0; kx < g.tile0 + g.count; kx++) {
+                    run_zline(c, kx, bsm);
                     __syncthreads();  // bsm free for the next tile
                 }
+                break;
             }
         }
         __syncthreads();  // every thread's stores of the item
@@ -233,7 +227,9 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
 
 // shared memory of an x tile's staged input (the inverse's m+1 spectrum rows of tz)
 size_t x_stage_bytes(int m, int tz) { return (size_t)(m + 1) * tz * sizeof(double2); }
-constexpr size_t kXStagedBytes = 32 * 1024;
+// dynamic shared memory of a tile with its staged input: six CTAs of 128 threads per SM
+// (228 KB per SM, 1 KB reserved and ~2 KB static per CTA)
+constexpr size_t kStagedBytes = 34 * 1024 + 512;
 
 int batch_plan_index(int n, const DifDev& f) {
 #define PRJ_BI(I, N, ...) \
@@ -253,44 +249,50 @@ bool batchk_supported(const prj_plan* pl) {
 
 cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases, BatchKernel* out) {
     std::vector<BatchCaseDev> cs((size_t)ncases);
+    std::vector<std::array<long long, kBNumStages>> work((size_t)ncases);
     size_t smem = 0;
     for (int i = 0; i < ncases; i++) {
         const prj_plan* pl = plans[i];
         const Geometry& g = pl->g;
         BatchCaseDev& c = cs[i];
         c.x = batch_x_args(pl, d_P[i]);
-        c.z = batch_z_args(pl);
-        // tile shapes within the per-case kernels' default shared-memory budgets, the x
-        // tiles with their staged input within kXStagedBytes, so six CTAs fit per SM
-        // whatever the plans' own tuning; a tile's shape does not change its results
+        c.zl = zline_args(pl);
+        // x tile shapes within the per-case kernels' default shared-memory budgets and, with
+        // their staged input, within kStagedBytes, so six CTAs fit per SM whatever the
+        // plans' own tuning; a tile's shape does not change its results
         const int m = pl->fx64.m;
         c.x.tz = std::min(c.x.tz, choose_tz_xp(m));
-        while (c.x.tz > 1 && pass_x_smem(m, c.x.tz) + x_stage_bytes(m, c.x.tz) > kXStagedBytes) c.x.tz /= 2;
+        while (c.x.tz > 1 && pass_x_smem(m, c.x.tz) + x_stage_bytes(m, c.x.tz) > kStagedBytes) c.x.tz /= 2;
         c.soff = (int)pass_x_smem(m, c.x.tz);
-        c.z.rb = std::min(c.z.rb, batch_z_default_rows(g.nz));
-        c.t = thomas_args(pl, pl->spec, 0, g.nxh);
+        // planes per stage of the z solve's ring: up to 8 within kStagedBytes
+        c.zl.yb = std::min(8, g.ny);
+        while (c.zl.yb > 1 && zline_smem(g.nz, g.mzp, c.zl.yb, kZlStages) > kStagedBytes) c.zl.yb--;
         c.xplan = batch_plan_index(pl->fx64.m, pl->xd.f);
         c.zplan = batch_plan_index(g.nz, pl->zd.f);
         c.ntz = (g.nz + c.x.tz - 1) / c.x.tz;
         c.tiles[kBFwdX] = c.tiles[kBBwdX] = c.ntz * g.ny;
-        c.tiles[kBZFwd] = c.tiles[kBZInv] = (c.z.nrow_total + c.z.rb - 1) / c.z.rb;
-        c.tiles[kBThomas] = g.nxh * c.t.tiles;
+        c.tiles[kBZLine] = g.nxh;
+        // work of one tile of each stage (points), the order key within a stage
+        work[i][kBFwdX] = work[i][kBBwdX] = (long long)c.x.tz * g.nx;
+        work[i][kBZLine] = (long long)g.ny * g.nz;
         smem = std::max(smem, pass_x_smem(m, c.x.tz) + x_stage_bytes(m, c.x.tz));
-        smem = std::max(smem, (size_t)padded_len(c.z.rb * g.nz, true) * sizeof(double2));
-        smem = std::max(smem, thomas_async_smem<double2, kRingPlanes, kRingStages>());
+        smem = std::max(smem, zline_smem(g.nz, g.mzp, c.zl.yb, kZlStages));
     }
-    // stage-major order; within a stage the cases with the most tiles first; each stage of a
-    // case cut into items of up to 16 tiles (about 64 items per stage where it has that
-    // many tiles), so one counter increment and one load start several tiles
+    // stage-major order; within a stage the cases with the largest tiles first (the longest
+    // z solves start first, so the stage's tail is short); each x stage of a case cut into
+    // items of up to 16 tiles (about 64 items per stage where it has that many tiles), so
+    // one counter increment and one load start several tiles; a z item is one wavenumber
     std::vector<int> order((size_t)ncases);
     for (int i = 0; i < ncases; i++) order[i] = i;
     std::vector<BatchSeg> segs;
     long long tiles_total = 0;
     for (int s = 0; s < kBNumStages; s++) {
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cs[a].tiles[s] > cs[b].tiles[s]; });
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return work[a][s] != work[b][s] ? work[a][s] > work[b][s] : cs[a].tiles[s] > cs[b].tiles[s];
+        });
         for (int i : order) {
             const int T = cs[i].tiles[s];
-            const int chunk = std::max(1, std::min(16, T / 64));
+            const int chunk = s == kBZLine ? 1 : std::max(1, std::min(16, T / 64));
             for (int t0 = 0; t0 < T; t0 += chunk) segs.push_back(BatchSeg{i, s, t0, std::min(chunk, T - t0)});
             tiles_total += T;
         }

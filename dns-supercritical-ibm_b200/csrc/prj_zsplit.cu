@@ -285,7 +285,7 @@ cudaError_t launch_thomas_mixed(const prj_plan* pl, cudaStream_t st) {
     const int nblk64 = pl->kxs * a64.tiles;
     const unsigned grid = (unsigned)(nblk64 + rows32 * a32.tiles);
     // the mixed storage streams by default (measured 0.69 ms against 1.10 ms per solve at
-    // 768x384x384); PRJ_THOMAS_ASYNC=0 keeps the register-prefetch kernel
+    // 768x384x384); thomas_ring 0 keeps the register-prefetch kernel
     switch (pl->thomas_async) {
     case 0: break;
     case 2: return launch_thomas_mixed_async<8, 2>(a64, a32, nblk64, grid, st);

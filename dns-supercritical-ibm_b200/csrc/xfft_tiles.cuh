@@ -68,11 +68,6 @@ __device__ __forceinline__ double2 spec_load(const XArgs& a, int y, int kx, int 
 
 // element g of the tz x rows buffer lives at slot sidx<true>(g) (bank-conflict padding)
 
-// no action (the default hook of the tiles below)
-struct NoHook {
-    __device__ __forceinline__ void operator()() const {}
-};
-
 // Staged inputs of the persistent batch kernel, which runs several tiles of one stage in
 // a row: the next tile's input is copied into shared memory S by cp.async (one commit
 // group) while the current tile computes.  fwd_xp_stage: the tile's P rows z0 ..

@@ -37,8 +37,25 @@ __device__ __forceinline__ void from_d2(float2& o, double2 v) { o = make_float2(
 #define PRJ_ZPASS_MINB 5
 #endif
 
-template <int DIR, typename T, class PL, bool STAGE_INV = false>
-__device__ __forceinline__ void zfft_pass_tile(const ZfftArgs& a, double2* zp, int bx) {
+// staged input of a z tile (the persistent batch kernel, which copies the next tile's
+// input by cp.async while the current one computes): its nr FP64 rows, contiguous in X,
+// as S[r n + e]
+template <class PL>
+__device__ __forceinline__ void zfft_stage(const ZfftArgs& a, double2* S, int bx) {
+    constexpr int n = PL::n;
+    const size_t row0 = (size_t)bx * a.rb;
+    const int nr = (int)min((size_t)a.rb, (size_t)a.nrow_total - row0);
+    const double2* X = static_cast<const double2*>(a.X) + row0 * n;
+    for (int i = threadIdx.x; i < nr * n; i += blockDim.x) cp_async(S + i, X + i, 16);
+    cp_async_commit();
+}
+
+// STAGED: the rows come from S, where zfft_stage put them, and after_load() is called
+// once S is no longer read
+template <int DIR, typename T, class PL, bool STAGE_INV = false, bool STAGED = false, class Hook = NoHook>
+__device__ __forceinline__ void zfft_pass_tile(const ZfftArgs& a, double2* zp, int bx, const double2* S = nullptr,
+                                               Hook after_load = Hook{}) {
+    static_assert(!STAGED || (STAGE_INV || DIR < 0), "a staged inverse copies its rows in whole");
     constexpr int n = PL::n;
     const size_t row0 = (size_t)bx * a.rb;
     const int nr = (int)min((size_t)a.rb, (size_t)a.nrow_total - row0);
@@ -50,16 +67,26 @@ __device__ __forceinline__ void zfft_pass_tile(const ZfftArgs& a, double2* zp, i
     // (STAGE_INV) or reads them in its first pass
     const int tot = nr * n;
     if (DIR < 0) {
-        dif_first_pass<-1, PL>(zp, nr, n, tw, [&](int r, int e) { return to_d2(X[(size_t)r * n + e]); });
+        if constexpr (STAGED) {
+            dif_first_pass<-1, PL>(zp, nr, n, tw, [&](int r, int e) { return S[(size_t)r * n + e]; });
+        } else {
+            dif_first_pass<-1, PL>(zp, nr, n, tw, [&](int r, int e) { return to_d2(X[(size_t)r * n + e]); });
+        }
         __syncthreads();
+        after_load();
         dif_passes_shared<-1, PL, 1, PL::P>(zp, nr, n, tw);
         for (int i = threadIdx.x; i < tot; i += blockDim.x) from_d2(X[i], zp[sidx<true>(i)]);
     } else {
         if (STAGE_INV) {
             // slot-order rows copied in whole (coalesced), every pass in shared memory
+            if constexpr (STAGED) {
+                for (int i = threadIdx.x; i < tot; i += blockDim.x) zp[sidx<true>(i)] = S[i];
+            } else {
 #pragma unroll 4
-            for (int i = threadIdx.x; i < tot; i += blockDim.x) zp[sidx<true>(i)] = to_d2(X[i]);
+                for (int i = threadIdx.x; i < tot; i += blockDim.x) zp[sidx<true>(i)] = to_d2(X[i]);
+            }
             __syncthreads();
+            after_load();
             dit_passes_shared<+1, PL, PL::P - 1, 0>(zp, nr, n, tw);
         } else {
             dit_first_pass<+1, PL>(zp, nr, n, [&](int r, int q) { return to_d2(X[(size_t)r * n + q]); });

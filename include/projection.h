@@ -278,9 +278,10 @@ int prj_geom_read_base_params(const char* path, prj_case_params* out);
  *   FP64, every case with even nx, nx/2 and nz among the pass-plan lengths up to
  *   256 (16, 24, 32, 48, 64, 96, 128, 192, 256) and a 16-byte aligned array: one
  *   persistent kernel runs all
- *   cases from a work queue of (case, stage, tile) items in stage-major order,
- *   with bounded waits on per-case stage counters; prj_batch_launch issues a
- *   counter reset and that one kernel (both capturable in a CUDA graph).
+ *   cases from a work queue of (case, stage, tile) items in stage-major order
+ *   (forward x transform, the fused z solve of each x wavenumber, inverse x
+ *   transform), with bounded waits on per-case stage counters; prj_batch_launch
+ *   issues a counter reset and that one kernel (both capturable in a CUDA graph).
  *   Otherwise (FP32 + refinement, other lengths, or mode | PRJ_BATCH_GRAPH): one
  *   CUDA graph holding every case's kernels on parallel branches, replayed by one
  *   graph launch.
@@ -328,10 +329,8 @@ int prj_batch_destroy(prj_batch* batch);
  *               kernel family.  Changing an order rebuilds the transform's tables.
  * prj_plan_set_tuning rejects values out of range and shapes that do not fit
  * shared memory; it may free and later reallocate the mixed path's FP32 spectrum
- * (after a change of mixed_tau), so call it outside stream capture.
- * The environment variables PRJ_ZSOLVE (split|fused|basic|line),
- * PRJ_FFT_KERNELS=runtime and PRJ_THOMAS_ASYNC are read once, at plan creation,
- * as test hooks for the defaults.
+ * (after a change of mixed_tau), so call it outside stream capture.  The library
+ * reads no environment variable.
  */
 typedef struct prj_tuning {
     int x_rows;

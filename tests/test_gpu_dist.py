@@ -16,11 +16,11 @@ def test_emulated_ranks_equal_single_gpu(cuda_device, monkeypatch, world, shape)
     import prj
     import prj_dist
     import workloads
-    monkeypatch.setenv("PRJ_ZSOLVE", "split")
     nx, ny, nz = shape
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=31)
     bands = prj.bands(yu, "consistent")
     with prj.Plan(nx, nz, ny, dx, dz, bands) as plan:
+        plan.set_tuning(z_mode=0)  # the split z kernels, which the ranks run
         ref = to_dev(rhs)
         plan.poisson_fp64(ref)
         ref = from_dev(ref)
@@ -65,13 +65,13 @@ def test_emulated_projection_step_equals_single_gpu(cuda_device, monkeypatch, wo
     import prj_dist
     import workloads
     from test_gpu_projection import run_engine
-    monkeypatch.setenv("PRJ_ZSOLVE", "split")
     nx, ny, nz = shape
     Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=9)
     for F in (Uh, Vh, Wh):
         workloads.fill_halos(F)
     wall = (0.01, 0.0, -0.02, 0.03, 0.0, 0.04)
     with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        plan.set_tuning(z_mode=0)  # the split z kernels, which the ranks run
         ref = run_engine(plan, Uh, Vh, Wh, 0.6, wall)
     plans = [prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") for _ in range(world)]
     try:

@@ -174,8 +174,8 @@ def test_streamed_thomas_is_bitwise_register_thomas(cuda_device, monkeypatch, sh
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=12)
     out = {}
     for flag in ("0", "1"):
-        monkeypatch.setenv("PRJ_THOMAS_ASYNC", flag)
         with prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent")) as plan:
+            plan.set_tuning(thomas_ring=int(flag))
             t = to_dev(rhs)
             plan.poisson_fp64(t)
             t2 = to_dev(rhs)

@@ -150,13 +150,13 @@ def test_pipelined_host_steps_match_sync(cuda_device):
 
 @pytest.mark.parametrize("shape", [(64, 48, 32), (30, 17, 21)])
 def test_basic_z_kernel_matches_oracle(cuda_device, oracle, monkeypatch, shape):
-    """PRJ_ZSOLVE=basic selects the first, unpipelined per-wavenumber z kernel."""
+    """z_mode 2 selects the first, unpipelined per-wavenumber z kernel."""
     import prj
     import workloads
-    monkeypatch.setenv("PRJ_ZSOLVE", "basic")
     nx, ny, nz = shape
     Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=7)
     with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        plan.set_tuning(z_mode=2)
         assert plan.tuning["z_mode"] == 2
         U, V, W, P, st = run_engine(plan, Uh, Vh, Wh, 0.5)
     Uo, Vo, Wo, Po = oracle.projection(Uh, Vh, Wh, dx, dz, 0.5, yu, "consistent")

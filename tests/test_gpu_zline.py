@@ -1,4 +1,4 @@
-"""The per-wavenumber z kernel (PRJ_ZSOLVE=line: z FFT, Thomas and inverse z FFT of one
+"""The per-wavenumber z kernel (z_mode 3: z FFT, Thomas and inverse z FFT of one
 x wavenumber per CTA) against the split kernels.
 
 It runs the same pass-plan butterflies, twiddle tables and Thomas operation order as the
@@ -14,15 +14,17 @@ from gpu_util import from_dev, to_dev
 pytestmark = pytest.mark.gpu
 
 
-def _solve(monkeypatch, env, nx, ny, nz, seed, **tuning):
+SPLIT, LINE = {"z_mode": 0}, {"z_mode": 3}
+
+
+def _solve(monkeypatch, zsel, nx, ny, nz, seed, **tuning):
+    """FP64 solve with the z kernels zsel (SPLIT or LINE; LINE falls back to the split
+    kernels for a length without a pass plan)."""
     import prj
     import workloads
-    for k, v in env.items():
-        monkeypatch.setenv(k, v)
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=seed)
     with prj.Plan(nx, nz, ny, dx, dz, prj.bands(yu, "consistent")) as plan:
-        if tuning:
-            plan.set_tuning(**tuning)
+        plan.set_tuning(**zsel, **tuning)
         t = to_dev(rhs)
         plan.poisson_fp64(t)
         return from_dev(t)
@@ -32,16 +34,16 @@ def _solve(monkeypatch, env, nx, ny, nz, seed, **tuning):
                                    (40, 70, 768), (16, 33, 1536), (96, 130, 40)])
 def test_line_kernel_is_bitwise_split(cuda_device, monkeypatch, shape):
     nx, ny, nz = shape
-    split = _solve(monkeypatch, {"PRJ_ZSOLVE": "split"}, nx, ny, nz, seed=21)
-    line = _solve(monkeypatch, {"PRJ_ZSOLVE": "line"}, nx, ny, nz, seed=21)
+    split = _solve(monkeypatch, SPLIT, nx, ny, nz, seed=21)
+    line = _solve(monkeypatch, LINE, nx, ny, nz, seed=21)
     np.testing.assert_array_equal(split, line)
 
 
 @pytest.mark.parametrize("yb,ns", [(4, 2), (2, 3), (1, 4), (3, 2), (8, 3)])
 def test_line_kernel_ring_shapes(cuda_device, monkeypatch, yb, ns):
     nx, ny, nz = 64, 61, 384
-    split = _solve(monkeypatch, {"PRJ_ZSOLVE": "split"}, nx, ny, nz, seed=22)
-    line = _solve(monkeypatch, {"PRJ_ZSOLVE": "line"}, nx, ny, nz, seed=22, z_planes=yb, z_stages=ns)
+    split = _solve(monkeypatch, SPLIT, nx, ny, nz, seed=22)
+    line = _solve(monkeypatch, LINE, nx, ny, nz, seed=22, z_planes=yb, z_stages=ns)
     np.testing.assert_array_equal(split, line)
 
 
@@ -54,9 +56,9 @@ def test_line_kernel_projection_step(cuda_device, monkeypatch):
     nx, ny, nz = 96, 64, 48
     Uh, Vh, Wh, yu, dx, dz = workloads.projection_inputs(nx, ny, nz, seed=5)
     out = {}
-    for mode in ("split", "line"):
-        monkeypatch.setenv("PRJ_ZSOLVE", mode)
+    for mode, zsel in (("split", SPLIT), ("line", LINE)):
         with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+            plan.set_tuning(**zsel)
             out[mode] = run_engine(plan, Uh, Vh, Wh, 0.5)
     for a, b in zip(out["split"][:4], out["line"][:4]):
         np.testing.assert_array_equal(a, b)
@@ -69,7 +71,6 @@ def test_default_rule_and_tuning(cuda_device, monkeypatch):
     import torch
     import prj
     import workloads
-    monkeypatch.delenv("PRJ_ZSOLVE", raising=False)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     nx_big = 2 * (2 * sms)  # nx/2+1 > 2 x SMs
     rhs, yu, dx, dz = workloads.poisson_rhs(nx_big, 8, 16, seed=3)
@@ -101,9 +102,9 @@ def test_line_kernel_outside_the_fast_division_window(cuda_device, monkeypatch, 
     rhs = np.asfortranarray(rhs * scale)
     b6 = prj.bands(yu, "consistent")
     out = {}
-    for mode in ("split", "line"):
-        monkeypatch.setenv("PRJ_ZSOLVE", mode)
+    for mode, zsel in (("split", SPLIT), ("line", LINE)):
         with prj.Plan(nx, nz, ny, dx, dz, b6) as plan:
+            plan.set_tuning(**zsel)
             t = to_dev(rhs)
             plan.poisson_fp64(t)
             out[mode] = from_dev(t)
