@@ -1266,13 +1266,14 @@ int prj_batch_create(prj_plan* const* plans, double* const* d_P, int ncases, int
         b->persistent = true;
         cudaError_t e = prj::batchk_build(plans, d_P, ncases, &b->bk);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
-        if (e != cudaSuccess) {
-            batch_release(b);
-            delete b;
-            return cuda_fail(e, "persistent batch kernel set-up");
+        if (e == cudaSuccess) {
+            *out = b;
+            return PRJ_OK;
         }
-        *out = b;
-        return PRJ_OK;
+        batch_release(b);
+        delete b;
+        // a tensor map the driver refuses: the graph form instead
+        if (e != cudaErrorNotSupported) return cuda_fail(e, "persistent batch kernel set-up");
     }
     // eager pass: lazy buffers, kernel attributes, and a check that every case runs
     std::vector<cudaStream_t> streams((size_t)ncases, nullptr);

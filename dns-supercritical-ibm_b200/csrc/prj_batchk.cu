@@ -42,7 +42,8 @@ namespace prj {
 // stages of one solve
 enum BatchStage { kBFwdX = 0, kBZLine = 1, kBBwdX = 2, kBNumStages = 3 };
 
-struct __align__(16) BatchCaseDev {
+struct __align__(64) BatchCaseDev {
+    CUtensorMap zl_tmap;  // row copies of its z solves (read from global memory by the TMA unit)
     XArgs x;          // forward (source P) and inverse (P out) x transforms of the case
     ZLineArgs zl;     // its z solves (one tile per x wavenumber)
     int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in PRJ_BATCH_PLANS
@@ -124,8 +125,8 @@ __device__ __noinline__ void run_x_bwd_tiles(const BatchCaseDev& c, int t0, int 
 constexpr int kZlStages = 2;
 __host__ __device__ constexpr int batch_lpt(int n) { return (n + kBatchThreads - 1) / kBatchThreads; }
 template <class PL>
-__device__ __noinline__ void tile_zline(const BatchCaseDev& c, int kx, unsigned char* sm) {
-    zline_tile<PL, kZlStages, batch_lpt(PL::n), kBatchThreads>(c.zl, kx, sm);
+__device__ __noinline__ void tile_zline(const BatchCaseDev& c, const CUtensorMap* tmap, int kx, unsigned char* sm) {
+    zline_tile<PL, kZlStages, batch_lpt(PL::n), kBatchThreads>(c.zl, tmap, kx, sm);
 }
 
 __device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
@@ -148,10 +149,10 @@ __device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int t0, int cou
     }
 }
 
-__device__ __forceinline__ void run_zline(const BatchCaseDev& c, int kx, unsigned char* sm) {
+__device__ __forceinline__ void run_zline(const BatchCaseDev& c, const CUtensorMap* tmap, int kx, unsigned char* sm) {
     switch (c.zplan) {
 #define PRJ_BZ(I, N, ...) \
-    case I: tile_zline<PassList<__VA_ARGS__>>(c, kx, sm); break;
+    case I: tile_zline<PassList<__VA_ARGS__>>(c, tmap, kx, sm); break;
         PRJ_BATCH_PLANS(PRJ_BZ)
 #undef PRJ_BZ
     default: break;
@@ -161,12 +162,12 @@ __device__ __forceinline__ void run_zline(const BatchCaseDev& c, int kx, unsigne
 __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
     k_batch(const BatchCaseDev* __restrict__ cases, const BatchSeg* __restrict__ segs, int nseg,
             unsigned long long* counter, int* done, int* err) {
-    extern __shared__ __align__(16) unsigned char bsm[];
+    extern __shared__ __align__(128) unsigned char bsm[];
     __shared__ BatchSeg s_seg;
     __shared__ int s_skip;
     // the current case's arguments, copied once per change of case (the items of one case
     // and stage come in runs) so that the tile functions read them from shared memory
-    __shared__ __align__(16) BatchCaseDev s_case;
+    __shared__ __align__(64) BatchCaseDev s_case;
     int loaded = -1;
     for (;;) {
         if (threadIdx.x == 0) {
@@ -188,6 +189,7 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
                         __nanosleep(128);
                     }
                     __threadfence();  // acquire: the previous stage's results before this item's reads
+                    fence_proxy_async_global();  // ... and before the tensor-map copies this thread issues
                 }
             }
             s_seg = g;
@@ -211,12 +213,13 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
             case kBBwdX: run_x_bwd(c, g.tile0, g.count, bsm); break;
             default:
                 for (int kx = g.tile0; kx < g.tile0 + g.count; kx++) {
-                    run_zline(c, kx, bsm);
+                    run_zline(c, &cases[g.case_id].zl_tmap, kx, bsm);
                     __syncthreads();  // bsm free for the next tile
                 }
                 break;
             }
         }
+        fence_proxy_async_global();  // this thread's stores, for later tensor-map reads of other CTAs
         __syncthreads();  // every thread's stores of the item
         if (threadIdx.x == 0) {
             __threadfence();  // release: the item's stores before its count
@@ -267,6 +270,7 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
         // planes per stage of the z solve's ring: up to 8 within kStagedBytes
         c.zl.yb = std::min(8, g.ny);
         while (c.zl.yb > 1 && zline_smem(g.nz, g.mzp, c.zl.yb, kZlStages) > kStagedBytes) c.zl.yb--;
+        if (!zline_tmap(&c.zl_tmap, pl->spec, g.nz, g.nxh, g.ny, c.zl.yb)) return cudaErrorNotSupported;
         c.xplan = batch_plan_index(pl->fx64.m, pl->xd.f);
         c.zplan = batch_plan_index(g.nz, pl->zd.f);
         c.ntz = (g.nz + c.x.tz - 1) / c.x.tz;
@@ -318,6 +322,9 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
     if ((e = cudaMalloc(&out->d_segs, sb)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&out->d_work, wb)) != cudaSuccess) return e;
     out->work_bytes = wb - sizeof(int);  // the error word after the counters is cleared by its check
+    int* errw = reinterpret_cast<int*>(static_cast<unsigned char*>(out->d_work) + out->work_bytes);
+    for (BatchCaseDev& c : cs) c.zl.err = errw;  // a z tile's wait that gives up raises the batch's word
+    static_assert(sizeof(BatchCaseDev) % 64 == 0, "tensor maps 64-byte aligned in the case array");
     if ((e = cudaMemcpy(out->d_cases, cs.data(), cb, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     if ((e = cudaMemcpy(out->d_segs, segs.data(), sb, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     return cudaMemset(out->d_work, 0, wb);

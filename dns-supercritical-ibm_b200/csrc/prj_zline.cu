@@ -5,7 +5,12 @@
 // Thomas lines (kx, slot) that run through them (zline_tile, zline_tiles.cuh: z FFT,
 // both Thomas sweeps and the inverse z FFT, the spectrum crossing HBM four times).
 // Each thread owns LPT lines (slots tid + q NT) and carries their recurrence in
-// registers.
+// registers.  The rows of each chunk of planes arrive by one TMA copy through a 4-D
+// tensor map of the spectrum (zline_tmap, encoded on the host for every launch with the
+// driver's cuTensorMapEncodeTiled); a map the driver refuses sends the solve to the split
+// kernels.
+#include <cuda.h>
+
 #include "div_rn.cuh"
 #include "fft_pass.cuh"
 #include "prj_internal.h"
@@ -15,35 +20,40 @@ namespace prj {
 
 namespace {
 
+// `tmap` (zline_tmap) is a kernel parameter: the TMA unit reads it from parameter space
 template <class PL, int NS, int LPT>
-__global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL::n, LPT))) k_zline(const ZLineArgs a) {
-    extern __shared__ __align__(16) unsigned char zsm[];
-    zline_tile<PL, NS, LPT, zl_threads(PL::n, LPT)>(a, blockIdx.x, zsm);
+__global__ void __launch_bounds__(zl_threads(PL::n, LPT), zl_minb(zl_threads(PL::n, LPT)))
+    k_zline(const __grid_constant__ ZLineArgs a, const __grid_constant__ CUtensorMap tmap) {
+    extern __shared__ __align__(128) unsigned char zsm[];
+    zline_tile<PL, NS, LPT, zl_threads(PL::n, LPT)>(a, &tmap, blockIdx.x, zsm);
 }
 
 template <class PL, int NS, int LPT>
-cudaError_t launch_zline_pl(const ZLineArgs& a, size_t smem, cudaStream_t st) {
+cudaError_t launch_zline_pl(const ZLineArgs& a, const CUtensorMap& tm, size_t smem, cudaStream_t st) {
     cudaError_t e =
         cudaFuncSetAttribute(k_zline<PL, NS, LPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_zline<PL, NS, LPT><<<a.nh, zl_threads(PL::n, LPT), smem, st>>>(a);
+    k_zline<PL, NS, LPT><<<a.nh, zl_threads(PL::n, LPT), smem, st>>>(a, tm);
     return cudaGetLastError();
 }
 
 template <class PL>
-cudaError_t launch_zline_ns(const ZLineArgs& a, int ns, size_t smem, cudaStream_t st) {
+cudaError_t launch_zline_ns(const ZLineArgs& a, const CUtensorMap& tm, int ns, size_t smem, cudaStream_t st) {
     constexpr int L = zl_lpt(PL::n);
     switch (ns) {
-    case 2: return launch_zline_pl<PL, 2, L>(a, smem, st);
-    case 3: return launch_zline_pl<PL, 3, L>(a, smem, st);
-    default: return launch_zline_pl<PL, 4, L>(a, smem, st);
+    case 2: return launch_zline_pl<PL, 2, L>(a, tm, smem, st);
+    case 3: return launch_zline_pl<PL, 3, L>(a, tm, smem, st);
+    default: return launch_zline_pl<PL, 4, L>(a, tm, smem, st);
     }
 }
+
 
 }  // namespace
 
 bool zline_supported(const prj_plan* pl) {
-    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc) return false;
+    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc || !pl->spec) return false;
+    CUtensorMap tm{};
+    if (!zline_tmap(&tm, pl->spec, pl->g.nz, pl->g.nxh, pl->g.ny, 1)) return false;  // the driver's answer
 #define PRJ_ZL_HAS(N, ...)                                                          \
     if (pl->g.nz == N && same_radices<PassList<__VA_ARGS__>>(pl->zd.f))             \
         return zline_smem(N, pl->g.mzp, 1, 2) <= (size_t)200 * 1024;
@@ -59,7 +69,30 @@ ZLineArgs zline_args(const prj_plan* pl) {
     a.yb = pl->z_planes > 0 ? pl->z_planes : 4;
     a.tw = pl->zd.tw; a.bands = pl->t.bands; a.piv = pl->t.piv; a.pivc = pl->t.pivc;
     a.kz_of_slot = pl->kz_of_slot; a.X = pl->spec;
+    a.err = reinterpret_cast<int*>(pl->stat_buf + kStatErrSlot);
     return a;
+}
+
+bool zline_tmap(void* tmap128, const double2* X, int n, int nh, int ny, int yb) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static const Encode enc = []() -> Encode {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<Encode>(fn);
+    }();
+    if (!enc || n % 8 != 0 || n / 8 > 256 || yb < 1 || yb > 256 || ((uintptr_t)X & 15u) != 0) return false;
+    const cuuint64_t dims[4] = {16, (cuuint64_t)(n / 8), (cuuint64_t)nh, (cuuint64_t)ny};
+    const cuuint64_t strides[3] = {128, (cuuint64_t)n * 16, (cuuint64_t)nh * (cuuint64_t)n * 16};  // bytes
+    const cuuint32_t box[4] = {18, (cuuint32_t)(n / 8), 1, (cuuint32_t)yb};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(static_cast<CUtensorMap*>(tmap128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double2*>(X), dims,
+               strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // cudaErrorNotSupported when nz has no pass plan (the caller runs the split kernels)
@@ -80,9 +113,11 @@ cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st) {
     const size_t smem = zline_smem(g.nz, g.mzp, yb, ns);
     if (smem > (size_t)200 * 1024) return cudaErrorNotSupported;
     a.yb = yb;
+    CUtensorMap tm{};
+    if (!zline_tmap(&tm, pl->spec, g.nz, g.nxh, g.ny, yb)) return cudaErrorNotSupported;  // split kernels
 #define PRJ_ZL_CASE(N, ...)                                                  \
     if (g.nz == N && same_radices<PassList<__VA_ARGS__>>(pl->zd.f))          \
-        return launch_zline_ns<PassList<__VA_ARGS__>>(a, ns, smem, st);
+        return launch_zline_ns<PassList<__VA_ARGS__>>(a, tm, ns, smem, st);
     PRJ_PASS_ALL(PRJ_ZL_CASE)
 #undef PRJ_ZL_CASE
     return cudaErrorNotSupported;

@@ -1,7 +1,8 @@
 // tma_util.cuh -- bulk (TMA) copies and mbarriers for sm_100a, inline PTX.
 //
-// Only non-multicast, CTA-local forms are used: cp.async.bulk from global to
-// this CTA's shared memory with mbarrier completion.  Every wait is bounded by
+// Only non-multicast, CTA-local forms are used: cp.async.bulk and
+// cp.async.bulk.tensor from global to this CTA's shared memory with mbarrier
+// completion.  Every wait is bounded by
 // a clock budget; a caller that gives up reports an error instead of hanging.
 #pragma once
 #include <cuda_runtime.h>
@@ -62,6 +63,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
             smem_u32(dst)),
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// global -> shared copy of one box of a 4-D tensor map (cp.async.bulk.tensor, no
+// multicast): box coordinates c0..c3 (c0 in elements, a multiple of 16 bytes), completion
+// counted on `bar`; `tmap` is the generic address of the CUtensorMap in param, const or
+// global memory; `dst` 128-byte aligned
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
         : "memory");
 }
 

@@ -2,8 +2,8 @@
 // function: z FFT, Thomas sweeps and inverse z FFT of the ny spectral z-rows X[y][kx][:].
 //
 //   forward phase, y ascending, chunks of yb planes:
-//     rows (natural z order) and pivot rows copied into a shared-memory stage by
-//     cp.async, NS stages in flight;
+//     rows (natural z order) copied into a shared-memory stage by one tensor-map copy
+//     (TMA) and pivot rows by cp.async, NS stages in flight;
 //     forward z FFT of the chunk's rows in place, every pass in shared memory;
 //     d'_y = (d_y - a_y d'_{y-1}) / D_y for the chunk's planes, stored to the row
 //     (slot order);
@@ -18,13 +18,16 @@
 // in/out).  The butterflies, twiddle tables and the Thomas operation order
 // (poisson_solver_multigpu.f90:401-419, round-to-nearest intrinsics) are those of
 // k_zfft_pass and k_thomas, so the result is bitwise that of the split kernels.
-// cp.async copies complete on their own, so no wait here can hang.  k_zline
+// Every mbarrier wait is bounded (a clock budget).  k_zline
 // (prj_zline.cu) runs one wavenumber per CTA; the persistent batch kernel
 // (prj_batchk.cu) runs (case, wavenumber) tiles from its work queue.
 #pragma once
+#include <cuda.h>
+
 #include "cp_async.cuh"
 #include "div_rn.cuh"
 #include "fft_pass.cuh"
+#include "tma_util.cuh"
 
 struct prj_plan;
 
@@ -39,6 +42,7 @@ struct ZLineArgs {
     const double* pivc;   // c'[y][kx][kzs] = c_y / D_y
     const int* kz_of_slot;
     double2* X;           // [y][kx][z]
+    int* err;             // raised (5) when a bounded mbarrier wait gives up
 };
 
 // lines per thread (default) and threads per CTA of a length-n plan; resident CTAs per
@@ -76,17 +80,41 @@ constexpr bool zl_layout_ok(int n) {
 PRJ_PASS_PLANS(PRJ_ZL_LAYOUT_CHECK)
 #undef PRJ_ZL_LAYOUT_CHECK
 
+// Shared memory of a tile: 128 bytes of alignment slack, NS mbarriers (128 bytes),
+// NS row stages of zl_slot_bytes each (128-byte aligned), then the pivot ring.  A stage
+// holds yb rows in the padded layout of the FFT passes: each group of 8 complex values is
+// followed by one pad slot, which is what a tensor-map box of 9 complex values per group
+// (the 9th out of bounds, zero-filled) writes.
+__host__ __device__ inline size_t zl_slot_bytes(int n, int yb) { return ((size_t)yb * n * 18 + 127) / 128 * 128; }
+
 // The z solve of x wavenumber kx: NT threads (the CTA), LPT lines per thread (NT LPT >=
 // n; slots past n idle in the Thomas phase), NS stages of a.yb planes in `zsm`
-// (zline_smem bytes).
+// (zline_smem bytes).  Each stage's rows arrive by one tensor-map copy (`tmap`:
+// zline_tmap's 4-D view of the spectrum) issued by thread 0 and completed on an mbarrier;
+// the pivot rows are cp.async copies (their pieces are permuted).  Every mbarrier wait is
+// bounded: on a timeout the tile raises *a.err, waits (bounded) for its copies in flight
+// and returns.
 template <class PL, int NS, int LPT, int NT>
-__device__ __forceinline__ void zline_tile(const ZLineArgs& a, int kx, unsigned char* zsm) {
+__device__ __forceinline__ void zline_tile(const ZLineArgs& a, const void* tmap, int kx, unsigned char* zsm) {
     constexpr int n = PL::n;
     static_assert(NT * LPT >= n, "every line has a thread");
+    static_assert(n % 8 == 0, "the stage layout needs whole groups of 8");
     const int ny = a.ny, nh = a.nh, mzp = a.mzp, mzs = zl_mzs(mzp), yb = a.yb, tid = threadIdx.x;
-    double2* ring = reinterpret_cast<double2*>(zsm);  // NS * yb rows of n, padded as one array
-    double* dring = reinterpret_cast<double*>(zsm + (size_t)padded_len(NS * yb * n, true) * sizeof(double2));
     const int nch = (ny + yb - 1) / yb;
+    unsigned char* base = zsm + ((128u - (smem_u32(zsm) & 127u)) & 127u);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+    const size_t slot_bytes = zl_slot_bytes(n, yb);
+    unsigned char* rslots = base + 128;
+    double* dring = reinterpret_cast<double*>(rslots + NS * slot_bytes);
+    auto stage = [&](int s) { return reinterpret_cast<double2*>(rslots + s * slot_bytes); };
+    if (tid == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;    // bit s: parity of stage s's next completion
+    uint32_t pending = 0;  // bit s: stage s has a copy in flight (the same in every thread)
 
     // this thread's lines
     int slot[LPT], kzs[LPT];
@@ -103,16 +131,18 @@ __device__ __forceinline__ void zline_tile(const ZLineArgs& a, int kx, unsigned 
     const double* bA0 = a.bands + 3 * ny;
 
     // chunk c (planes c yb ..) into stage s with the rows of table tab (pivots on the way
-    // up, back-substitution factors on the way down); every thread copies a share; one
-    // group per call
+    // up, back-substitution factors on the way down): the rows by one tensor-map copy (a
+    // box of yb planes, those past ny zero-filled), the pivots by every thread's cp.async
+    // share; one cp.async group per call
     auto issue = [&](int c, int s, const double* tab) {
         if (c >= 0 && c < nch) {
             const int y0 = c * yb, nr = min(yb, ny - y0);
-            double2* buf = ring + sidx<true>(s * yb * n);
-            for (int i = tid; i < nr * n; i += NT) {
-                const int r = i / n, e = i - r * n;
-                cp_async(&buf[sidx<true>(r * n + e)], a.X + ((size_t)(y0 + r) * nh + kx) * n + e, 16);
+            if (tid == 0) {
+                fence_proxy_async_shared();  // the stage's earlier reads before the copy's writes
+                mbar_arrive_expect_tx(&bars[s], (uint32_t)(18 * n * yb));
+                tma_load_4d(stage(s), tmap, 0, 0, kx, y0, &bars[s]);
             }
+            pending |= 1u << s;
             const int hp = mzp / 2;  // 16-byte pieces of a pivot row
             double* dbuf = dring + (size_t)s * yb * mzs;
             for (int i = tid; i < nr * hp; i += NT) {
@@ -121,6 +151,28 @@ __device__ __forceinline__ void zline_tile(const ZLineArgs& a, int kx, unsigned 
             }
         }
         cp_async_commit();
+    };
+    // stage s's copies complete (pivots: this thread's groups but the NS-1 newest); false
+    // in every thread if any thread's wait gave up
+    auto acquire = [&](int s) -> bool {
+        cp_async_wait<NS - 1>();
+        const bool ok = mbar_wait_bounded(&bars[s], (phase >> s) & 1u);
+        phase ^= 1u << s;
+        pending &= ~(1u << s);
+        return !__syncthreads_or(!ok);
+    };
+    auto bail = [&]() {
+        if (tid == 0) {
+            atomicExch(a.err, 5);
+#pragma unroll
+            for (int s = 0; s < NS; s++)
+                if (pending & (1u << s)) mbar_wait_bounded(&bars[s], (phase >> s) & 1u);
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        if (tid == 0)
+#pragma unroll
+            for (int s = 0; s < NS; s++) mbar_inval(&bars[s]);
     };
 
     double2 prev[LPT];
@@ -132,10 +184,12 @@ __device__ __forceinline__ void zline_tile(const ZLineArgs& a, int kx, unsigned 
     for (int c = 0; c < NS - 1; c++) issue(c, c, a.piv);
     for (int c = 0; c < nch; c++) {
         issue(c + NS - 1, (c + NS - 1) % NS, a.piv);  // that stage was last read in iteration c - 1
-        cp_async_wait<NS - 1>();
-        __syncthreads();
         const int s = c % NS, y0 = c * yb, nr = min(yb, ny - y0);
-        double2* buf = ring + sidx<true>(s * yb * n);
+        if (!acquire(s)) {
+            bail();
+            return;
+        }
+        double2* buf = stage(s);
         const double* dbuf = dring + (size_t)s * yb * mzs;
         dif_passes_shared<-1, PL, 0, PL::P>(buf, nr, n, a.tw);  // barrier after every pass
         for (int r = 0; r < nr; r++) {
@@ -163,20 +217,25 @@ __device__ __forceinline__ void zline_tile(const ZLineArgs& a, int kx, unsigned 
         __syncthreads();
     }
     cp_async_wait<0>();
-    // the backward phase streams back rows other threads of this CTA stored
+    // the backward phase's tensor-map copies read back rows other threads of this CTA
+    // stored
     __threadfence();
+    fence_proxy_async_global();
     __syncthreads();
 
     // ----------------------------------------------------------- backward phase
-    // j-th chunk from the top (chunk nch-1-j) uses stage j % NS
+    // j-th chunk from the top (chunk nch-1-j) uses stage (nch + j) % NS, continuing the
+    // forward phase's rotation
 #pragma unroll
-    for (int j = 0; j < NS - 1; j++) issue(nch - 1 - j, j, a.pivc);
+    for (int j = 0; j < NS - 1; j++) issue(nch - 1 - j, (nch + j) % NS, a.pivc);
     for (int j = 0; j < nch; j++) {
-        issue(nch - 1 - (j + NS - 1), (j + NS - 1) % NS, a.pivc);
-        cp_async_wait<NS - 1>();
-        __syncthreads();
-        const int s = j % NS, c = nch - 1 - j, y0 = c * yb, nr = min(yb, ny - y0);
-        double2* buf = ring + sidx<true>(s * yb * n);
+        issue(nch - 1 - (j + NS - 1), (nch + j + NS - 1) % NS, a.pivc);
+        const int s = (nch + j) % NS, c = nch - 1 - j, y0 = c * yb, nr = min(yb, ny - y0);
+        if (!acquire(s)) {
+            bail();
+            return;
+        }
+        double2* buf = stage(s);
         const double* dbuf = dring + (size_t)s * yb * mzs;
         for (int r = nr - 1; r >= 0; r--) {
             const int y = y0 + r;
@@ -204,15 +263,25 @@ __device__ __forceinline__ void zline_tile(const ZLineArgs& a, int kx, unsigned 
         __syncthreads();
     }
     cp_async_wait<0>();
+    __syncthreads();
+    if (tid == 0)
+#pragma unroll
+        for (int s = 0; s < NS; s++) mbar_inval(&bars[s]);
 }
 
 // arguments of a plan's z solves (FP64 spectrum, pivots, z pass plan; yb from the plan's
 // z_planes tuning or 4; prj_zline.cu)
 ZLineArgs zline_args(const prj_plan* pl);
 
-// shared memory of a ring of ns stages of yb planes (rows and pivot rows)
+// shared memory of a tile (alignment slack, mbarriers, row stages, pivot ring)
 inline size_t zline_smem(int n, int mzp, int yb, int ns) {
-    return (size_t)padded_len(ns * yb * n, true) * sizeof(double2) + (size_t)ns * yb * zl_mzs(mzp) * sizeof(double);
+    return 256 + (size_t)ns * zl_slot_bytes(n, yb) + (size_t)ns * yb * zl_mzs(mzp) * sizeof(double);
 }
+
+// the 4-D tensor map of the row copies over the spectrum X (n-point z rows,
+// nh x wavenumbers, ny planes): dims {16 doubles (a group of 8 complex values), n/8
+// groups, nh, ny}, box {18, n/8, 1, yb}; false if the driver refuses it
+bool zline_tmap(void* tmap128, const double2* X, int n, int nh, int ny, int yb);
+
 
 }  // namespace prj

@@ -76,6 +76,8 @@ def test_default_rule_and_tuning(cuda_device, monkeypatch):
     rhs, yu, dx, dz = workloads.poisson_rhs(nx_big, 8, 16, seed=3)
     with prj.Plan(nx_big, 16, 8, dx, dz, prj.bands(yu, "consistent")) as plan:
         assert plan.tuning["z_mode"] == 3
+        # one z kernel per step: the driver accepted the tensor map of the row copies
+        assert plan.launches_per_step(prj.MODE_FP64) == 4
     nx, ny, nz = 64, 20, 48
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=4)
     out = {}
