@@ -44,11 +44,14 @@ enum BatchStage { kBFwdX = 0, kBZLine = 1, kBBwdX = 2, kBNumStages = 3 };
 
 struct __align__(64) BatchCaseDev {
     CUtensorMap zl_tmap;  // row copies of its z solves (read from global memory by the TMA unit)
+    CUtensorMap x_tmap;   // spectrum copies of its inverse x tiles: {2 nz doubles, nh, ny}, box {2 tz, xbox_k, 1}
     XArgs x;          // forward (source P) and inverse (P out) x transforms of the case
     ZLineArgs zl;     // its z solves (one tile per x wavenumber)
     int xplan, zplan; // index of the x (m = nx/2) and z (nz) pass plans in PRJ_BATCH_PLANS
     int ntz;          // x tiles per y plane
-    int soff;         // byte offset in shared memory of the x tiles' staged input
+    int soff;         // byte offset in shared memory of the x tiles' staged input (before 128-byte alignment)
+    int sbytes;       // its bytes (xboxes spectrum boxes of xbox_k x tz values; the forward's rows fit)
+    int xbox_k, xboxes;
     int tiles[kBNumStages];
 };
 
@@ -94,31 +97,75 @@ constexpr int kBatchMinBlocks = PRJ_BATCH_MINB;
 // The x and z stages run an item's tiles as a pipeline: the next tile's input is copied
 // into shared memory (cp.async) while the current tile computes, so a CTA keeps loads in
 // flight through its FFT passes and stores instead of one round trip per tile.
-template <class PL>
-__device__ __noinline__ void run_x_fwd_tiles(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
-    double2* S = reinterpret_cast<double2*>(sm + c.soff);
-    fwd_xp_stage<PL>(c.x, S, t0 % c.ntz, t0 / c.ntz);
-    for (int t = t0; t < t0 + count; t++) {
-        cp_async_wait<0>();
-        __syncthreads();  // S holds tile t for every thread; A is free
-        const int nt = t + 1;
-        fwd_xp_tile<2, PL>(c.x, sm, t % c.ntz, t / c.ntz, S, [&] {
-            if (nt < t0 + count) fwd_xp_stage<PL>(c.x, S, nt % c.ntz, nt / c.ntz);
-        });
+__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
+    return p + ((128u - (smem_u32(p) & 127u)) & 127u);
+}
+
+// The tiles t0 .. t0+count-1 of an x stage as a pipeline: the next tile's input is copied
+// into the staging buffer S (after the tile area) by the TMA unit -- the forward's P rows,
+// contiguous, by one bulk copy; the inverse's spectrum block X[y][k][z0 ..] by xboxes
+// tensor-map boxes -- while the current tile runs its FFT passes and stores, completion
+// counted on one mbarrier.  A wait that runs out raises *err (6) and ends the run.
+template <class PL, bool FWD>
+__device__ __forceinline__ void run_x_tiles(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
+                                            unsigned char* sm, int* err) {
+    constexpr int m = PL::n;
+    const int tid = threadIdx.x;
+    double2* S = reinterpret_cast<double2*>(align128(sm + c.soff));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(S) + c.sbytes);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
     }
+    __syncthreads();
+    uint32_t phase = 0;
+    auto stage = [&](int t) {  // thread 0
+        const int bx = t % c.ntz, by = t / c.ntz;
+        const int y = c.x.y0 + by, z0 = bx * c.x.tz;
+        fence_proxy_async_shared();  // S's earlier reads before the copy's writes
+        if constexpr (FWD) {
+            const int nr = min(c.x.tz, c.x.nz - z0);
+            const uint32_t bytes = (uint32_t)nr * m * (uint32_t)sizeof(double2);
+            mbar_arrive_expect_tx(bar, bytes);
+            bulk_g2s(S, reinterpret_cast<const double2*>(c.x.P) + ((size_t)y * c.x.nz + z0) * m, bytes, bar);
+        } else {
+            mbar_arrive_expect_tx(bar, (uint32_t)(c.xboxes * c.xbox_k * c.x.tz) * (uint32_t)sizeof(double2));
+            for (int b = 0; b < c.xboxes; b++)
+                tma_load_3d(S + (size_t)b * c.xbox_k * c.x.tz, xmap, 2 * z0, b * c.xbox_k, y, bar);
+        }
+    };
+    if (tid == 0) stage(t0);
+    for (int t = t0; t < t0 + count; t++) {
+        const bool ok = mbar_wait_bounded(bar, phase);
+        if (__syncthreads_or(!ok)) {  // S holds tile t for every thread (else: give up the run)
+            if (tid == 0) {
+                atomicExch(err, 6);
+                mbar_wait_bounded(bar, phase);
+            }
+            break;
+        }
+        phase ^= 1u;
+        const int nt = t + 1;
+        auto next = [&] {
+            if (tid == 0 && nt < t0 + count) stage(nt);
+        };
+        if constexpr (FWD) fwd_xp_tile<2, PL>(c.x, sm, t % c.ntz, t / c.ntz, S, next);
+        else bwd_xp_tile<PL, false, true>(c.x, sm, t % c.ntz, t / c.ntz, c.ntz, S, next);
+        // (the next iteration's barrier orders this tile's reads of its area before the
+        // next tile's writes)
+    }
+    __syncthreads();
+    if (tid == 0) mbar_inval(bar);
 }
 template <class PL>
-__device__ __noinline__ void run_x_bwd_tiles(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
-    double2* S = reinterpret_cast<double2*>(sm + c.soff);
-    bwd_xp_stage<PL>(c.x, S, t0 % c.ntz, t0 / c.ntz);
-    for (int t = t0; t < t0 + count; t++) {
-        cp_async_wait<0>();
-        __syncthreads();
-        const int nt = t + 1;
-        bwd_xp_tile<PL, false, true>(c.x, sm, t % c.ntz, t / c.ntz, c.ntz, S, [&] {
-            if (nt < t0 + count) bwd_xp_stage<PL>(c.x, S, nt % c.ntz, nt / c.ntz);
-        });
-    }
+__device__ __noinline__ void run_x_fwd_tiles(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
+                                             unsigned char* sm, int* err) {
+    run_x_tiles<PL, true>(c, xmap, t0, count, sm, err);
+}
+template <class PL>
+__device__ __noinline__ void run_x_bwd_tiles(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
+                                             unsigned char* sm, int* err) {
+    run_x_tiles<PL, false>(c, xmap, t0, count, sm, err);
 }
 // the z solve of one wavenumber: ring of kZlStages stages of c.zl.yb planes, lines
 // spread over the CTA's threads
@@ -129,20 +176,22 @@ __device__ __noinline__ void tile_zline(const BatchCaseDev& c, const CUtensorMap
     zline_tile<PL, kZlStages, batch_lpt(PL::n), kBatchThreads>(c.zl, tmap, kx, sm);
 }
 
-__device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
+__device__ __forceinline__ void run_x_fwd(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
+                                          unsigned char* sm, int* err) {
     switch (c.xplan) {
 #define PRJ_BX(I, N, ...) \
-    case I: run_x_fwd_tiles<PassList<__VA_ARGS__>>(c, t0, count, sm); break;
+    case I: run_x_fwd_tiles<PassList<__VA_ARGS__>>(c, xmap, t0, count, sm, err); break;
         PRJ_BATCH_PLANS(PRJ_BX)
 #undef PRJ_BX
     default: break;
     }
 }
 
-__device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, int t0, int count, unsigned char* sm) {
+__device__ __forceinline__ void run_x_bwd(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
+                                          unsigned char* sm, int* err) {
     switch (c.xplan) {
 #define PRJ_BX(I, N, ...) \
-    case I: run_x_bwd_tiles<PassList<__VA_ARGS__>>(c, t0, count, sm); break;
+    case I: run_x_bwd_tiles<PassList<__VA_ARGS__>>(c, xmap, t0, count, sm, err); break;
         PRJ_BATCH_PLANS(PRJ_BX)
 #undef PRJ_BX
     default: break;
@@ -209,8 +258,8 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
         const BatchCaseDev& c = s_case;
         if (!s_skip) {
             switch (g.stage) {
-            case kBFwdX: run_x_fwd(c, g.tile0, g.count, bsm); break;
-            case kBBwdX: run_x_bwd(c, g.tile0, g.count, bsm); break;
+            case kBFwdX: run_x_fwd(c, &cases[g.case_id].x_tmap, g.tile0, g.count, bsm, err); break;
+            case kBBwdX: run_x_bwd(c, &cases[g.case_id].x_tmap, g.tile0, g.count, bsm, err); break;
             default:
                 for (int kx = g.tile0; kx < g.tile0 + g.count; kx++) {
                     run_zline(c, &cases[g.case_id].zl_tmap, kx, bsm);
@@ -228,8 +277,17 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
     }
 }
 
-// shared memory of an x tile's staged input (the inverse's m+1 spectrum rows of tz)
-size_t x_stage_bytes(int m, int tz) { return (size_t)(m + 1) * tz * sizeof(double2); }
+// spectrum boxes of an inverse x tile: k = 0 .. m in boxes of at most 256 wavenumbers;
+// with more than one box, a multiple of 8 wavenumbers per box, so every box lands on a
+// 128-byte boundary of S (rows past m are zero-filled and unread)
+int x_boxes(int m) { return (m + 1 + 255) / 256; }
+int x_box_k(int m) {
+    const int b = x_boxes(m), k = (m + 1 + b - 1) / b;
+    return b == 1 ? k : (k + 7) / 8 * 8;
+}
+// shared memory of an x tile's staged input (the inverse's boxes of tz values; the forward's
+// tz rows of m fit) with 128 bytes of alignment slack and the mbarrier
+size_t x_stage_bytes(int m, int tz) { return 128 + (size_t)x_boxes(m) * x_box_k(m) * tz * sizeof(double2) + 16; }
 // dynamic shared memory of a tile with its staged input: six CTAs of 128 threads per SM
 // (228 KB per SM, 1 KB reserved and ~2 KB static per CTA)
 constexpr size_t kStagedBytes = 34 * 1024 + 512;
@@ -267,6 +325,15 @@ cudaError_t batchk_build(prj_plan* const* plans, double* const* d_P, int ncases,
         c.x.tz = std::min(c.x.tz, choose_tz_xp(m));
         while (c.x.tz > 1 && pass_x_smem(m, c.x.tz) + x_stage_bytes(m, c.x.tz) > kStagedBytes) c.x.tz /= 2;
         c.soff = (int)pass_x_smem(m, c.x.tz);
+        c.xboxes = x_boxes(m);
+        c.xbox_k = x_box_k(m);
+        c.sbytes = c.xboxes * c.xbox_k * c.x.tz * (int)sizeof(double2);
+        {
+            const uint64_t dims[3] = {2 * (uint64_t)g.nz, (uint64_t)g.nxh, (uint64_t)g.ny};
+            const uint64_t strides[2] = {(uint64_t)g.nz * 16, (uint64_t)g.nxh * (uint64_t)g.nz * 16};
+            const uint32_t box[3] = {2 * (uint32_t)c.x.tz, (uint32_t)c.xbox_k, 1};
+            if (2 * c.x.tz > 256 || !tmap_encode_f64(&c.x_tmap, pl->spec, 3, dims, strides, box)) return cudaErrorNotSupported;
+        }
         // planes per stage of the z solve's ring: up to 8 within kStagedBytes
         c.zl.yb = std::min(8, g.ny);
         while (c.zl.yb > 1 && zline_smem(g.nz, g.mzp, c.zl.yb, kZlStages) > kStagedBytes) c.zl.yb--;

@@ -73,7 +73,8 @@ ZLineArgs zline_args(const prj_plan* pl) {
     return a;
 }
 
-bool zline_tmap(void* tmap128, const double2* X, int n, int nh, int ny, int yb) {
+bool tmap_encode_f64(void* tmap128, const void* base, int rank, const uint64_t* dims, const uint64_t* strides,
+                     const uint32_t* box) {
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -85,14 +86,26 @@ bool zline_tmap(void* tmap128, const double2* X, int n, int nh, int ny, int yb) 
             return nullptr;
         return reinterpret_cast<Encode>(fn);
     }();
-    if (!enc || n % 8 != 0 || n / 8 > 256 || yb < 1 || yb > 256 || ((uintptr_t)X & 15u) != 0) return false;
-    const cuuint64_t dims[4] = {16, (cuuint64_t)(n / 8), (cuuint64_t)nh, (cuuint64_t)ny};
-    const cuuint64_t strides[3] = {128, (cuuint64_t)n * 16, (cuuint64_t)nh * (cuuint64_t)n * 16};  // bytes
-    const cuuint32_t box[4] = {18, (cuuint32_t)(n / 8), 1, (cuuint32_t)yb};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    return enc(static_cast<CUtensorMap*>(tmap128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double2*>(X), dims,
-               strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+    if (!enc || rank < 1 || rank > 5 || ((uintptr_t)base & 15u) != 0) return false;
+    cuuint64_t d[5], st[4];
+    cuuint32_t b[5], e[5];
+    for (int i = 0; i < rank; i++) {
+        d[i] = dims[i];
+        b[i] = box[i];
+        e[i] = 1;
+        if (i + 1 < rank) st[i] = strides[i];
+    }
+    return enc(static_cast<CUtensorMap*>(tmap128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank,
+               const_cast<void*>(base), d, st, b, e, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool zline_tmap(void* tmap128, const double2* X, int n, int nh, int ny, int yb) {
+    if (n % 8 != 0 || n / 8 > 256 || yb < 1 || yb > 256) return false;
+    const uint64_t dims[4] = {16, (uint64_t)(n / 8), (uint64_t)nh, (uint64_t)ny};
+    const uint64_t strides[3] = {128, (uint64_t)n * 16, (uint64_t)nh * (uint64_t)n * 16};  // bytes
+    const uint32_t box[4] = {18, (uint32_t)(n / 8), 1, (uint32_t)yb};
+    return tmap_encode_f64(tmap128, X, 4, dims, strides, box);
 }
 
 // cudaErrorNotSupported when nz has no pass plan (the caller runs the split kernels)

@@ -79,6 +79,22 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0,
         : "memory");
 }
 
+// global -> shared copy of one box of a 3-D tensor map (as tma_load_4d)
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Host: encode a tiled tensor map of FP64 elements (the driver's cuTensorMapEncodeTiled,
+// looked up once through the runtime): rank dims (innermost first), rank-1 byte strides,
+// the box; no interleave, swizzle or fill value (out-of-bounds elements read as zero).
+// False if the driver refuses it.
+bool tmap_encode_f64(void* tmap128, const void* base, int rank, const uint64_t* dims, const uint64_t* strides,
+                     const uint32_t* box);
+
 // order this thread's generic-proxy accesses before later async-proxy (bulk copy) accesses
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_shared() {

@@ -69,36 +69,15 @@ __device__ __forceinline__ double2 spec_load(const XArgs& a, int y, int kx, int 
 // element g of the tz x rows buffer lives at slot sidx<true>(g) (bank-conflict padding)
 
 // Staged inputs of the persistent batch kernel, which runs several tiles of one stage in
-// a row: the next tile's input is copied into shared memory S by cp.async (one commit
-// group) while the current tile computes.  fwd_xp_stage: the tile's P rows z0 ..
-// z0+nr-1 of plane y, contiguous in P, as S[r m + e].  bwd_xp_stage: its spectrum
-// X[y][k][z0 + r] (FP64 rows, kxs = nh) as S[k nr + r], k = 0 .. m.
-template <class PL>
-__device__ __forceinline__ void fwd_xp_stage(const XArgs& a, double2* S, int bx, int by) {
-    constexpr int m = PL::n;
-    const int y = a.y0 + by, z0 = bx * a.tz, nr = min(a.tz, a.nz - z0);
-    const double2* src = reinterpret_cast<const double2*>(a.P) + ((size_t)y * a.nz + z0) * m;
-    for (int i = threadIdx.x; i < nr * m; i += blockDim.x) cp_async(S + i, src + i, 16);
-    cp_async_commit();
-}
-
-template <class PL>
-__device__ __forceinline__ void bwd_xp_stage(const XArgs& a, double2* S, int bx, int by) {
-    constexpr int m = PL::n;
-    const int y = a.y0 + by, z0 = bx * a.tz, nr = min(a.tz, a.nz - z0);
-    const double2* src = a.X + (size_t)y * a.kxs * a.nz + z0;
-    for (int i = threadIdx.x; i < (m + 1) * nr; i += blockDim.x) {
-        const int k = i / nr, r = i - k * nr;
-        cp_async(S + i, src + (size_t)k * a.nz + r, 16);
-    }
-    cp_async_commit();
-}
+// a row and has the next tile's input copied into shared memory S (by the TMA unit) while
+// the current tile computes: the forward's P rows z0 .. z0+nr-1 of plane y, contiguous in
+// P, as S[r m + e]; the inverse's spectrum X[y][k][z0 + r] as S[k tz + r], k = 0 .. m.
 
 // fwd_xp_tile: source (P, or the divergence of u_hat) -> packed complex -> DIF
 // passes -> split X_k, X_{m-k} -> transposed store.  SRC 0 reads P in the first
-// pass; SRC 1 stages the divergence in shared memory first; SRC 2 reads P from S,
-// where fwd_xp_stage put it, and calls after_first() once S is no longer read (after
-// the first pass).  Tile (bx, by): rows z0 = bx tz .., plane y0 + by.
+// pass; SRC 1 stages the divergence in shared memory first; SRC 2 reads P from S
+// (staged as above) and calls after_first() once S is no longer read (after the first
+// pass).  Tile (bx, by): rows z0 = bx tz .., plane y0 + by.
 template <int SRC, class PL, class Hook = NoHook>
 __device__ __forceinline__ void fwd_xp_tile(const XArgs& a, unsigned char* sm, int bx, int by,
                                             const double2* S = nullptr, Hook after_first = Hook{}) {
@@ -231,8 +210,8 @@ __device__ __forceinline__ void fwd_xp_tile(const XArgs& a, unsigned char* sm, i
 // order -> DIT passes -> P rows (x pairs as double2), optionally accumulated; the
 // tile's partial sum of P goes to psum[y][bx] (tiles_per_plane entries per plane).
 // EXTRAS = false: plain P = result (no accumulation, partial sums or norms), the form of
-// the persistent batch kernel.  STAGED: the spectrum comes from S, where bwd_xp_stage put
-// it, and after_split() is called once S is no longer read.
+// the persistent batch kernel.  STAGED: the spectrum comes from S (staged as above), and
+// after_split() is called once S is no longer read.
 template <class PL, bool EXTRAS = true, bool STAGED = false, class Hook = NoHook>
 __device__ __forceinline__ void bwd_xp_tile(const XArgs& a, unsigned char* sm, int bx, int by, int tiles_per_plane,
                                             const double2* S = nullptr, Hook after_split = Hook{}) {
@@ -252,8 +231,8 @@ __device__ __forceinline__ void bwd_xp_tile(const XArgs& a, unsigned char* sm, i
             if (idx < total) {
                 const int k = idx / nr, r = idx - k * nr;
                 if constexpr (STAGED) {
-                    xa[u] = S[k * nr + r];
-                    xb[u] = S[(m - k) * nr + r];
+                    xa[u] = S[k * a.tz + r];
+                    xb[u] = S[(m - k) * a.tz + r];
                 } else {
                     xa[u] = spec_load(a, y, k, z0 + r);
                     xb[u] = spec_load(a, y, m - k, z0 + r);
