@@ -97,65 +97,12 @@ constexpr int kBatchMinBlocks = PRJ_BATCH_MINB;
 // The x and z stages run an item's tiles as a pipeline: the next tile's input is copied
 // into shared memory (cp.async) while the current tile computes, so a CTA keeps loads in
 // flight through its FFT passes and stores instead of one round trip per tile.
-__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
-    return p + ((128u - (smem_u32(p) & 127u)) & 127u);
-}
-
-// The tiles t0 .. t0+count-1 of an x stage as a pipeline: the next tile's input is copied
-// into the staging buffer S (after the tile area) by the TMA unit -- the forward's P rows,
-// contiguous, by one bulk copy; the inverse's spectrum block X[y][k][z0 ..] by xboxes
-// tensor-map boxes -- while the current tile runs its FFT passes and stores, completion
-// counted on one mbarrier.  A wait that runs out raises *err (6) and ends the run.
+// The tiles t0 .. t0+count-1 of an x stage through x_tiles_tma (xfft_tiles.cuh): the next
+// tile's input staged by the TMA unit while the current tile computes.
 template <class PL, bool FWD>
 __device__ __forceinline__ void run_x_tiles(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
                                             unsigned char* sm, int* err) {
-    constexpr int m = PL::n;
-    const int tid = threadIdx.x;
-    double2* S = reinterpret_cast<double2*>(align128(sm + c.soff));
-    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(S) + c.sbytes);
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    uint32_t phase = 0;
-    auto stage = [&](int t) {  // thread 0
-        const int bx = t % c.ntz, by = t / c.ntz;
-        const int y = c.x.y0 + by, z0 = bx * c.x.tz;
-        fence_proxy_async_shared();  // S's earlier reads before the copy's writes
-        if constexpr (FWD) {
-            const int nr = min(c.x.tz, c.x.nz - z0);
-            const uint32_t bytes = (uint32_t)nr * m * (uint32_t)sizeof(double2);
-            mbar_arrive_expect_tx(bar, bytes);
-            bulk_g2s(S, reinterpret_cast<const double2*>(c.x.P) + ((size_t)y * c.x.nz + z0) * m, bytes, bar);
-        } else {
-            mbar_arrive_expect_tx(bar, (uint32_t)(c.xboxes * c.xbox_k * c.x.tz) * (uint32_t)sizeof(double2));
-            for (int b = 0; b < c.xboxes; b++)
-                tma_load_3d(S + (size_t)b * c.xbox_k * c.x.tz, xmap, 2 * z0, b * c.xbox_k, y, bar);
-        }
-    };
-    if (tid == 0) stage(t0);
-    for (int t = t0; t < t0 + count; t++) {
-        const bool ok = mbar_wait_bounded(bar, phase);
-        if (__syncthreads_or(!ok)) {  // S holds tile t for every thread (else: give up the run)
-            if (tid == 0) {
-                atomicExch(err, 6);
-                mbar_wait_bounded(bar, phase);
-            }
-            break;
-        }
-        phase ^= 1u;
-        const int nt = t + 1;
-        auto next = [&] {
-            if (tid == 0 && nt < t0 + count) stage(nt);
-        };
-        if constexpr (FWD) fwd_xp_tile<2, PL>(c.x, sm, t % c.ntz, t / c.ntz, S, next);
-        else bwd_xp_tile<PL, false, true>(c.x, sm, t % c.ntz, t / c.ntz, c.ntz, S, next);
-        // (the next iteration's barrier orders this tile's reads of its area before the
-        // next tile's writes)
-    }
-    __syncthreads();
-    if (tid == 0) mbar_inval(bar);
+    x_tiles_tma<PL, FWD, false>(c.x, xmap, c.ntz, c.xboxes, c.xbox_k, sm, c.soff, c.sbytes, t0, 1, t0 + count, err);
 }
 template <class PL>
 __device__ __noinline__ void run_x_fwd_tiles(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
@@ -277,14 +224,6 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks)
     }
 }
 
-// spectrum boxes of an inverse x tile: k = 0 .. m in boxes of at most 256 wavenumbers;
-// with more than one box, a multiple of 8 wavenumbers per box, so every box lands on a
-// 128-byte boundary of S (rows past m are zero-filled and unread)
-int x_boxes(int m) { return (m + 1 + 255) / 256; }
-int x_box_k(int m) {
-    const int b = x_boxes(m), k = (m + 1 + b - 1) / b;
-    return b == 1 ? k : (k + 7) / 8 * 8;
-}
 // shared memory of an x tile's staged input (the inverse's boxes of tz values; the forward's
 // tz rows of m fit) with 128 bytes of alignment slack and the mbarrier
 size_t x_stage_bytes(int m, int tz) { return 128 + (size_t)x_boxes(m) * x_box_k(m) * tz * sizeof(double2) + 16; }

@@ -47,6 +47,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
+// the first 128-byte boundary at or after p (a shared-memory address)
+__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
+    return p + ((128u - (smem_u32(p) & 127u)) & 127u);
+}
+
 // Wait for completion of the phase with parity `phase`; false after `budget` cycles.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase,
                                                   long long budget = kWaitBudgetCycles) {

@@ -12,6 +12,7 @@
 #include "cp_async.cuh"
 #include "fft_dif.cuh"
 #include "fft_pass.cuh"
+#include "tma_util.cuh"
 
 struct prj_plan;
 
@@ -307,6 +308,76 @@ __device__ __forceinline__ void bwd_xp_tile(const XArgs& a, unsigned char* sm, i
             atomicAdd(a.sq + 1, sq1);
         }
     }
+}
+
+// spectrum boxes of an inverse x tile: k = 0 .. m in boxes of at most 256 wavenumbers;
+// with more than one box, a multiple of 8 wavenumbers per box, so every box lands on a
+// 128-byte boundary of S (rows past m are zero-filled and unread)
+inline int x_boxes(int m) { return (m + 1 + 255) / 256; }
+inline int x_box_k(int m) {
+    const int b = x_boxes(m), k = (m + 1 + b - 1) / b;
+    return b == 1 ? k : (k + 7) / 8 * 8;
+}
+
+// Tiles t = first, first + stride, ... < end of an x transform (tile (t % tpp, t / tpp)) as a
+// pipeline: the next tile's input is copied into the staging buffer S (128-byte aligned at or
+// after sm + soff, sbytes long, followed by an mbarrier) by the TMA unit -- FWD: the tile's P
+// rows, contiguous, by one bulk copy; inverse: its spectrum block X[y][k][z0 ..] by `boxes`
+// boxes of box_k wavenumbers of the 3-D tensor map `xmap` ({2 nz doubles, nh, ny}, box
+// {2 tz, box_k, 1}; FP64 rows only) -- while the current tile runs its FFT passes and stores.
+// The tiles compute as fwd_xp_tile<2> / bwd_xp_tile<STAGED>, so the results are those of the
+// one-tile kernels.  A wait that runs out raises *err (6) and ends the run.
+template <class PL, bool FWD, bool EXTRAS>
+__device__ __forceinline__ void x_tiles_tma(const XArgs& a, const void* xmap, int tpp, int boxes, int box_k,
+                                            unsigned char* sm, int soff, int sbytes, int first, int stride, int end,
+                                            int* err) {
+    constexpr int m = PL::n;
+    const int tid = threadIdx.x;
+    if (first >= end) return;
+    double2* S = reinterpret_cast<double2*>(align128(sm + soff));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(S) + sbytes);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    auto stage = [&](int t) {  // thread 0
+        const int bx = t % tpp, by = t / tpp;
+        const int y = a.y0 + by, z0 = bx * a.tz;
+        fence_proxy_async_shared();  // S's earlier reads before the copy's writes
+        if constexpr (FWD) {
+            const int nr = min(a.tz, a.nz - z0);
+            const uint32_t bytes = (uint32_t)nr * m * (uint32_t)sizeof(double2);
+            mbar_arrive_expect_tx(bar, bytes);
+            bulk_g2s(S, reinterpret_cast<const double2*>(a.P) + ((size_t)y * a.nz + z0) * m, bytes, bar);
+        } else {
+            mbar_arrive_expect_tx(bar, (uint32_t)(boxes * box_k * a.tz) * (uint32_t)sizeof(double2));
+            for (int b = 0; b < boxes; b++) tma_load_3d(S + (size_t)b * box_k * a.tz, xmap, 2 * z0, b * box_k, y, bar);
+        }
+    };
+    if (tid == 0) stage(first);
+    for (int t = first; t < end; t += stride) {
+        const bool ok = mbar_wait_bounded(bar, phase);
+        if (__syncthreads_or(!ok)) {  // S holds tile t for every thread (else: give up the run)
+            if (tid == 0) {
+                atomicExch(err, 6);
+                mbar_wait_bounded(bar, phase);
+            }
+            break;
+        }
+        phase ^= 1u;
+        const int nt = t + stride;
+        auto next = [&] {
+            if (tid == 0 && nt < end) stage(nt);
+        };
+        // (the next iteration's barrier orders this tile's reads of its area before the next
+        // tile's writes)
+        if constexpr (FWD) fwd_xp_tile<2, PL>(a, sm, t % tpp, t / tpp, S, next);
+        else bwd_xp_tile<PL, EXTRAS, true>(a, sm, t % tpp, t / tpp, tpp, S, next);
+    }
+    __syncthreads();
+    if (tid == 0) mbar_inval(bar);
 }
 
 }  // namespace prj
