@@ -19,7 +19,8 @@ it) or copied into host arrays the request brings (``want="host"``: the
 device-to-host copies are part of the request's work and latency).
 
 The server keeps, per grid size, a pool of resident *slots*: a solver plan, the
-device fields of one request and a CUDA stream.  A queued request is admitted as
+device fields of one request and a CUDA stream (of higher priority for smaller grids,
+so a short request's kernels do not queue behind a long one's).  A queued request is admitted as
 soon as a slot of its size is idle; if none exists, a new slot is created when it
 fits the HBM budget, evicting idle slots of other sizes (least recently used)
 when needed.  Admitted requests run asynchronously on their slot's stream (input,
@@ -99,7 +100,7 @@ def device_predictor(Uh, Vh, Wh, yp, seed, stream=None):
 
 class ProjectionServer:
     def __init__(self, device: int = 0, hbm_budget: float = 150e9, max_slots: int = 64, slots_per_size: int = 4,
-                 mode: int = prj.MODE_FP64, band_mode: str = "consistent", dt: float = 1.0):
+                 mode: int = prj.MODE_FP64, band_mode: str = "consistent", dt: float = 1.0, priority: str = "small"):
         import torch
         self.torch = torch
         self.device = device
@@ -109,6 +110,15 @@ class ProjectionServer:
         self.mode = mode
         self.band_mode = band_mode
         self.dt = dt
+        # stream priority of a slot: "small" (smaller grids first, the default), "large" or
+        # "none" (all equal); the GPU's block scheduler prefers the CTAs of higher-priority
+        # streams when both have work ready.  Measured at 1000 requests/s of the served mix:
+        # "small" p50 0.9 ms / p99 36 ms, "none" 5.3 / 92 ms (small requests' kernels queued
+        # behind the 768^3 ones: 133 ms p99 at 128x96x64), "large" 5.3 / 131 ms
+        if priority not in ("none", "large", "small"):
+            raise ValueError(f"priority {priority!r}")
+        self.priority = priority
+        self.known_points = {sz[0] * sz[1] * sz[2] for sz in SERVED_SIZES}
         self.slots: list[Slot] = []
         self.used = 0
         self.peak_used = 0
@@ -148,7 +158,7 @@ class ProjectionServer:
         U, V, W = (torch.empty_like(Uh) for _ in range(3))
         P = torch.empty((ny, nz, nx), dtype=torch.float64, device=dev)
         yp = torch.tensor((yu[:-1] + yu[1:]) / 2, dtype=torch.float64, device=dev)
-        s = torch.cuda.Stream(device=dev)
+        s = torch.cuda.Stream(device=dev, priority=self._stream_priority(size))
         torch.cuda.synchronize(dev)
         nbytes = plan.device_bytes + 8 * (6 * Uh.numel() + P.numel())
         slot = Slot(size, plan, (Uh, Vh, Wh, U, V, W, P), s, None, nbytes, yp)
@@ -159,6 +169,17 @@ class ProjectionServer:
         self.used += nbytes
         self.peak_used = max(self.peak_used, self.used)
         return slot
+
+    def _stream_priority(self, size):
+        if self.priority == "none":
+            return 0
+        least, greatest = self.torch.cuda.Stream.priority_range()  # e.g. (0, -5): lower is higher
+        # rank among the sizes the server knows (the served mix, the run's requests, resident
+        # slots): the most preferred gets the greatest priority
+        pts = lambda sz: sz[0] * sz[1] * sz[2]
+        known = self.known_points | {pts(s.size) for s in self.slots} | {pts(size)}
+        order = sorted(known, reverse=(self.priority == "large"))
+        return max(greatest, least - (len(order) - 1 - order.index(pts(size))))
 
     def _drop(self, s):
         s.jobs.put(None)
@@ -221,6 +242,7 @@ class ProjectionServer:
         if requests is None:
             requests = [Request(i, size, t, seed=1000 + i) for i, (t, size) in enumerate(arrivals)]
         sizes = sorted({r.size for r in requests})
+        self.known_points |= {sz[0] * sz[1] * sz[2] for sz in sizes}
         if warm:  # the per-size slots that fit the budget, created before the clock starts
             for k in range(self.slots_per_size):
                 for size in sizes:
@@ -299,6 +321,11 @@ class ProjectionServer:
 
 def summarize(done, duration_s):
     lat = np.array([r.done - r.arrival for r in done]) * 1e3
+    by_size = {}
+    for size in sorted({r.size for r in done}):
+        ls = np.array([r.done - r.arrival for r in done if r.size == size]) * 1e3
+        by_size["x".join(map(str, size))] = {"requests": int(len(ls)), "p50_ms": float(np.percentile(ls, 50)),
+                                             "p99_ms": float(np.percentile(ls, 99))}
     pts = sum(s[0] * s[1] * s[2] for s in (r.size for r in done))
     span = max(r.done for r in done) if done else 0.0
     return {
@@ -310,4 +337,5 @@ def summarize(done, duration_s):
         "gpts_per_s": pts / span / 1e9 if span else None,
         "offered_window_s": duration_s,
         "drain_s": span - duration_s,
+        "by_size": by_size,
     }

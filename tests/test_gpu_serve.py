@@ -139,3 +139,25 @@ def test_budget_limits_resident_memory(cuda_device):
     s = serve.summarize(done, 0.02)
     assert s["p99_ms"] >= s["p50_ms"] > 0
     srv.close()
+
+
+def test_slot_streams_prefer_smaller_grids(cuda_device):
+    """Each slot's stream gets a priority by its grid size's rank among the sizes the server
+    knows: under the default policy the smaller grid's stream has the higher priority (a lower
+    number), "large" reverses it, "none" is flat; an unknown policy is refused."""
+    import torch
+    import serve
+    least, greatest = torch.cuda.Stream.priority_range()
+    small, big = serve.SERVED_SIZES[0], serve.SERVED_SIZES[1]
+    pr = {}
+    for pol in ("small", "large", "none"):
+        srv = serve.ProjectionServer(hbm_budget=8e9, priority=pol)
+        try:
+            pr[pol] = [srv._acquire(size, 0.0).stream.priority for size in (small, big)]
+        finally:
+            srv.close()
+    assert pr["small"][0] < pr["small"][1] and pr["large"][0] > pr["large"][1]
+    assert pr["none"] == [0, 0]
+    assert all(greatest <= p <= least for v in pr.values() for p in v)
+    with pytest.raises(ValueError):
+        serve.ProjectionServer(priority="fifo")
