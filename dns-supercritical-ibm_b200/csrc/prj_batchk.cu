@@ -26,7 +26,9 @@
 // equals its own prj_poisson_fp64 bit for bit (the z solve of k_zline is bitwise that of
 // the split z kernels).  One launch replaces ncases x 3 to 5 small kernels, their launch
 // gaps and their tails, and the fused z solve moves the spectrum through HBM four times
-// where the split kernels move it eight.  Counters are reset by a memset issued
+// where the split kernels move it eight.  Every staged copy (x tiles' inputs, z tiles'
+// rows) is a TMA copy completed on an mbarrier; the tensor maps live in the case array
+// (global memory), where the TMA unit reads them.  Counters are reset by a memset issued
 // with the launch, so the pair can be captured in a CUDA graph.
 #include <algorithm>
 #include <array>
@@ -94,11 +96,10 @@ constexpr int kBatchMinBlocks = PRJ_BATCH_MINB;
 // stack per thread); as calls, each tile function is allocated on its own, as in its
 // per-case kernel.
 //
-// The x and z stages run an item's tiles as a pipeline: the next tile's input is copied
-// into shared memory (cp.async) while the current tile computes, so a CTA keeps loads in
-// flight through its FFT passes and stores instead of one round trip per tile.
-// The tiles t0 .. t0+count-1 of an x stage through x_tiles_tma (xfft_tiles.cuh): the next
-// tile's input staged by the TMA unit while the current tile computes.
+// The x stages run an item's tiles as a pipeline (x_tiles_tma, xfft_tiles.cuh): the next
+// tile's input is copied into shared memory by the TMA unit while the current tile
+// computes, so a CTA keeps loads in flight through its FFT passes and stores instead of
+// one round trip per tile; the z tiles stream their planes through zline_tile's ring.
 template <class PL, bool FWD>
 __device__ __forceinline__ void run_x_tiles(const BatchCaseDev& c, const CUtensorMap* xmap, int t0, int count,
                                             unsigned char* sm, int* err) {
