@@ -19,7 +19,8 @@ SPLIT, LINE = {"z_mode": 0}, {"z_mode": 3}
 
 def _solve(monkeypatch, zsel, nx, ny, nz, seed, **tuning):
     """FP64 solve with the z kernels zsel (SPLIT or LINE; LINE falls back to the split
-    kernels for a length without a pass plan)."""
+    kernels for a length without a pass plan); no bounded wait of the line kernel's
+    tensor-map copies may have given up (the plan's error word stays clear)."""
     import prj
     import workloads
     rhs, yu, dx, dz = workloads.poisson_rhs(nx, ny, nz, seed=seed)
@@ -27,6 +28,7 @@ def _solve(monkeypatch, zsel, nx, ny, nz, seed, **tuning):
         plan.set_tuning(**zsel, **tuning)
         t = to_dev(rhs)
         plan.poisson_fp64(t)
+        plan.check_error()
         return from_dev(t)
 
 
