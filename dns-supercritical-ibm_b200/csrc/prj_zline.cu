@@ -86,7 +86,7 @@ bool tmap_encode_f64(void* tmap128, const void* base, int rank, const uint64_t* 
             return nullptr;
         return reinterpret_cast<Encode>(fn);
     }();
-    if (!enc || rank < 1 || rank > 5 || ((uintptr_t)base & 15u) != 0) return false;
+    if (!enc || !base || rank < 1 || rank > 5 || ((uintptr_t)base & 15u) != 0) return false;
     cuuint64_t d[5], st[4];
     cuuint32_t b[5], e[5];
     for (int i = 0; i < rank; i++) {
@@ -110,7 +110,7 @@ bool zline_tmap(void* tmap128, const double2* X, int n, int nh, int ny, int yb) 
 
 // cudaErrorNotSupported when nz has no pass plan (the caller runs the split kernels)
 cudaError_t launch_zline(const prj_plan* pl, cudaStream_t st) {
-    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc) return cudaErrorNotSupported;
+    if (!pl->use_pass || !pl->zd.ok || !pl->kz_of_slot || !pl->t.pivc || !pl->spec) return cudaErrorNotSupported;
     const Geometry& g = pl->g;
     ZLineArgs a = zline_args(pl);
     // planes per stage and stage count: the plan's z_planes / z_stages tuning, else 4 x 2;
