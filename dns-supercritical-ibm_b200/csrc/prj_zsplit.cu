@@ -256,7 +256,7 @@ cudaError_t launch_thomas_t(const prj_plan* pl, void* X, int kx0, int rows_per_p
 cudaError_t launch_zfft(const prj_plan* pl, int dir, cudaStream_t st, YRange yr) {
     yr = yr.resolved(pl->g.ny);
     if (yr.y0 == 0 && yr.y1 == pl->g.ny) return launch_zfft_t<double2>(pl, dir, pl->spec, pl->g.nxh, st);
-    // a y range: the pass-plan kernel only (the overlapped schedule requires it)
+    // a y range (one rank's planes of the distributed solve): the pass-plan kernel only
     double2* X = pl->spec + (size_t)yr.y0 * pl->g.nxh * pl->g.nz;
     return launch_zfft_pass<double2>(pl, dir, X, pl->g.nxh, st, yr.y1 - yr.y0);
 }
