@@ -37,19 +37,36 @@ __device__ __forceinline__ double of_ord(unsigned long long o) {
 // one read of rho: ih = 0.5 / rho on the whole halo'd box (the quotient both stencils form
 // for every neighbour, computed once: the same correctly rounded values), and rho_min, the
 // minimum over the interior (mod_cfd_subroutines.f90:476-486), reduced by fmin and an
-// atomicMin on the order-preserving integer image, both exact and order-free
-__global__ void k_rho_prep(int nx, int nz, int ny, const double* __restrict__ rho, double* __restrict__ ih,
-                           unsigned long long* out) {
-    const size_t hx = (size_t)nx + 2, hz = (size_t)nz + 2, n = hx * hz * ((size_t)ny + 2);
+// atomicMin on the order-preserving integer image, both exact and order-free.  One warp per
+// halo'd x-row (the row's plane and z index from one division per row, not per element).
+__global__ void __launch_bounds__(256) k_rho_prep(int nx, int nz, int ny, const double* __restrict__ rho,
+                                                  double* __restrict__ ih, unsigned long long* out) {
+    const int hx = nx + 2, hz = nz + 2, rows = hz * (ny + 2), lane = threadIdx.x & 31;
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
     double m = 1e20;  // mod_cfd_subroutines.f90:476
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double r = rho[i];
-        ih[i] = __ddiv_rn(0.5, r);
-        const size_t x = i % hx, zr = i / hx, z = zr % hz, y = zr / hz;
-        if (x >= 1 && x <= (size_t)nx && z >= 1 && z <= (size_t)nz && y >= 1 && y <= (size_t)ny) m = fmin(m, r);
+    for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < rows; r += nw) {
+        const int z = r % hz, y = r / hz;
+        const bool inner = z >= 1 && z <= nz && y >= 1 && y <= ny;
+        const double* src = rho + (size_t)r * hx;
+        double* dst = ih + (size_t)r * hx;
+        // eight loads in flight per lane before the quotients
+        constexpr int U = 8;
+        for (int x0 = lane; x0 < hx; x0 += 32 * U) {
+            double v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) v[u] = x0 + 32 * u < hx ? src[x0 + 32 * u] : 1.0;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int x = x0 + 32 * u;
+                if (x < hx) {
+                    dst[x] = __ddiv_rn(0.5, v[u]);
+                    if (inner && x >= 1 && x <= nx) m = fmin(m, v[u]);
+                }
+            }
+        }
     }
     for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMin(out, ord_of(m));
+    if (lane == 0) atomicMin(out, ord_of(m));
 }
 
 struct VdArgs {
@@ -195,8 +212,13 @@ cudaError_t launch_vd_prep(const prj_plan* pl, const double* rho, double* ih, un
     cudaError_t e = cudaMemsetAsync(slot, 0xff, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const Geometry& g = pl->g;
-    const size_t n = (size_t)(g.nx + 2) * (g.nz + 2) * (g.ny + 2);
-    const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+    // eight warps per CTA, one halo'd row per warp at a time, one wave of resident CTAs
+    int dev = 0, sms = 0, per = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rho_prep, 256, 0)) != cudaSuccess) return e;
+    const long long rows = (long long)(g.nz + 2) * (g.ny + 2);
+    const unsigned blocks = (unsigned)std::max(1LL, std::min<long long>((rows + 7) / 8, (long long)std::max(per, 1) * sms));
     k_rho_prep<<<blocks, 256, 0, st>>>(g.nx, g.nz, g.ny, rho, ih, slot);
     return cudaGetLastError();
 }
