@@ -47,6 +47,32 @@ def test_vd_matches_oracle(cuda_device, oracle, band_mode, shape):
     np.testing.assert_array_equal(Pnext, workloads.fill_halos(np.pad(P, 1)))
 
 
+@pytest.mark.parametrize("where", ["x", "z", "y"])
+def test_vd_rho_min_ignores_halos(cuda_device, oracle, where):
+    """rho_min is the minimum over the interior (mod_cfd_subroutines.f90:476-486): a smaller
+    density planted in the x halo columns, the z halo rows or the wall ghost planes changes
+    neither rho_min nor the agreement with the oracle (both read the same halo'd arrays)."""
+    import prj
+    import workloads
+    nx, ny, nz = 30, 17, 21
+    Uh, Vh, Wh, rho, Pn, Po, div, yu, dx, dz = workloads.vd_inputs(nx, ny, nz)
+    rho = np.array(rho, order="F")
+    inner_min = rho[1:-1, 1:-1, 1:-1].min()
+    tiny = 0.5 * inner_min
+    cells = {"x": [(0, 5, 7), (nx + 1, 3, 2)], "z": [(4, 0, 6), (9, nz + 1, 3)],
+             "y": [(6, 7, 0), (2, 3, ny + 1)]}[where]
+    for c in cells:
+        rho[c] = tiny
+    with prj.Plan.from_yu(nx, nz, dx, dz, yu, "consistent") as plan:
+        U, V, W, P, Pnext, st = run_vd(plan, (Uh, Vh, Wh, rho, Pn, Po, div), 0.45)
+    Uo, Vo, Wo, Po_, Pno, rmin = oracle.projection_vd(Uh, Vh, Wh, rho, Pn, Po, div, dx, dz, 0.45, yu,
+                                                      "consistent", (0.0,) * 6)
+    assert st["rho_min"] == rmin == inner_min
+    assert rel_l2(P, Po_) <= 1e-12
+    for a, b in ((U, Uo), (V, Vo), (W, Wo)):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
 def test_vd_constant_density_equals_incompressible(cuda_device):
     """rho = 2, div_now = 0: the variable-density step is the incompressible step bit for bit
     (P scaled by rho_min = 2 exactly)."""
