@@ -374,11 +374,19 @@ int run_mixed_core(prj_plan* pl, const double* Uh, const double* Vh, const doubl
                    "plane means");
             else
                 CK(prj::launch_plane_mean(pl, P, pl->pbar, st), "plane means");
-            CK(prj::launch_residual(pl, b, P, pl->pbar, r, st), "residual");
         }
         {
+            // the residual formed inside the forward x transform (no round trip of r through
+            // HBM), or as its own kernel where the x length has no pass plan
             StageTimer tm(pl, prj::kStFwdX, st);
-            CK(prj::launch_fwd_xd(pl, prj::FwdSource::Pressure, r, nullptr, nullptr, nullptr, nullptr, st), "forward x");
+            const cudaError_t e = prj::launch_fwd_residual(pl, b, P, pl->pbar, st);
+            if (e == cudaErrorNotSupported) {
+                CK(prj::launch_residual(pl, b, P, pl->pbar, r, st), "residual");
+                CK(prj::launch_fwd_xd(pl, prj::FwdSource::Pressure, r, nullptr, nullptr, nullptr, nullptr, st),
+                   "forward x");
+            } else {
+                CK(e, "residual + forward x");
+            }
         }
         if ((rc = run_zsolve_mixed(pl, st))) return rc;
         if (last) CK(cudaMemsetAsync(pl->stat_buf + 4, 0, 2 * sizeof(double), st), "norm slots");
@@ -1130,10 +1138,11 @@ int prj_plan_schedule(const prj_plan* plan, int mode, int* launches) {
         *launches = one_z ? 4 : 6;
     } else {
         // forward x, z transforms of the FP64 and FP32 rows, one Thomas launch, inverse z of both,
-        // inverse x; per refinement pass also the plane means, the residual and a norm reset;
+        // inverse x; per refinement pass also the plane means and a norm reset, and the
+        // residual where the forward x transform does not form it (no pass plan for nx/2);
         // then the correction
         const int solve = 1 + 2 + 1 + 2 + 1;
-        *launches = solve + plan->mixed_iters * (solve + 3) + 1;
+        *launches = solve + plan->mixed_iters * (solve + (x_pass_active(plan) ? 2 : 3)) + 1;
     }
     return PRJ_OK;
 }

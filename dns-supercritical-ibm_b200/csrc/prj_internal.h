@@ -137,7 +137,7 @@ struct prj_plan {
 namespace prj {
 
 // Kernel launchers (prj_kernels.cu).  All are asynchronous on `st`.
-enum class FwdSource { Pressure, Divergence };
+enum class FwdSource { Pressure, Divergence, Residual };
 
 // a range of y planes [y0, y1) of one launch; y1 < 0 means up to ny
 struct YRange {
@@ -205,6 +205,11 @@ cudaError_t launch_plane_mean(const prj_plan* pl, const double* P, double* pbar,
 // plane means from the inverse x kernel's partial sums ([ny][tiles])
 cudaError_t launch_plane_mean_partials(const prj_plan* pl, const double* psum, int tiles, double* pbar,
                                        cudaStream_t st);
+// forward x transform of the residual B - A P formed on the fly (the pass-plan kernel);
+// cudaErrorNotSupported when the x length has no pass plan or an array is not 16-byte
+// aligned (the caller then runs launch_residual and the forward x of its result)
+cudaError_t launch_fwd_residual(const prj_plan* pl, const double* B, const double* P, const double* pbar,
+                                cudaStream_t st);
 cudaError_t launch_residual(const prj_plan* pl, const double* B, const double* P, const double* pbar, double* R,
                             cudaStream_t st);
 

@@ -9,8 +9,11 @@
 // where pm(k) is the (x, z) mean of plane k: the kx = kz = 0 mode uses the
 // pinned bands (poisson_solver_multigpu.f90:167-175), i.e. the Neumann problem
 // with the gauge of the reference.  The x/z stencils are the ones whose
-// eigenvalues are a_x, a_z (PSM:147-148).  k_residual forms r = b - A p in FP64.
+// eigenvalues are a_x, a_z (PSM:147-148).  k_residual forms r = b - A p in FP64 (the
+// refinement's forward x transform forms it on the fly instead where the x length has a
+// pass plan: fwd_xp_tile's residual source, xfft_tiles.cuh).
 #include "prj_internal.h"
+#include "residual.cuh"
 
 namespace prj {
 
@@ -65,18 +68,11 @@ __global__ void __launch_bounds__(128) k_residual(const ResArgs a) {
     const double* pkp = k < ny - 1 ? a.P + ((size_t)(k + 1) * nz + j) * nx : p0;
     const double* bd = a.bands;
     const double ak = bd[k], bk = bd[ny + k], ck = bd[2 * ny + k];
-    const double a0 = bd[3 * ny + k], b0 = bd[4 * ny + k], c0 = bd[5 * ny + k];
-    // pinned-mode correction, the same for the whole plane
-    double pin = (b0 - bk) * a.pm[k];
-    if (k > 0) pin += (a0 - ak) * a.pm[k - 1];
-    if (k < ny - 1) pin += (c0 - ck) * a.pm[k + 1];
+    const double pin = residual_pin(bd, a.pm, ny, k);  // pinned-mode correction of the plane
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         const int ip = i + 1 == nx ? 0 : i + 1, im = i == 0 ? nx - 1 : i - 1;
-        const double pc = p0[i];
-        double ap = (p0[ip] - 2.0 * pc + p0[im]) * a.idx2 + (pjp[i] - 2.0 * pc + pjm[i]) * a.idz2 + bk * pc;
-        if (k > 0) ap += ak * pkm[i];
-        if (k < ny - 1) ap += ck * pkp[i];
-        a.R[row + i] = a.B[row + i] - (ap + pin);
+        a.R[row + i] = residual_at(a.B[row + i], p0[i], p0[ip], p0[im], pjp[i], pjm[i], pkm[i], pkp[i], k > 0,
+                                   k < ny - 1, a.idx2, a.idz2, ak, bk, ck, pin);
     }
 }
 

@@ -314,6 +314,9 @@ cudaError_t launch_fwd_xp_pl(const XArgs& a, FwdSource src, const dim3& grid, cu
     if (src == FwdSource::Pressure) {
         if ((e = allow_smem(k_fwd_xp<0, PL>, smem)) != cudaSuccess) return e;
         k_fwd_xp<0, PL><<<grid, kPassThreads, smem, st>>>(a);
+    } else if (src == FwdSource::Residual) {
+        if ((e = allow_smem(k_fwd_xp<3, PL>, smem)) != cudaSuccess) return e;
+        k_fwd_xp<3, PL><<<grid, kPassThreads, smem, st>>>(a);
     } else {
         if ((e = allow_smem(k_fwd_xp<1, PL>, smem)) != cudaSuccess) return e;
         k_fwd_xp<1, PL><<<grid, kPassThreads, smem, st>>>(a);
@@ -371,6 +374,20 @@ cudaError_t launch_fwd_xd(const prj_plan* pl, FwdSource src, const double* P, co
         k_fwd_xd<1><<<grid, 256, smem, st>>>(a);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_fwd_residual(const prj_plan* pl, const double* B, const double* P, const double* pbar,
+                                cudaStream_t st) {
+    if (!aligned16(B) || !aligned16(P)) return cudaErrorNotSupported;
+    XArgs a = make_args(pl);
+    a.y0 = 0;
+    a.P = P;
+    a.B = B;
+    a.pm = pbar;
+    a.bands = pl->t.bands;
+    a.idx2 = 1.0 / (pl->g.dx * pl->g.dx);
+    a.idz2 = 1.0 / (pl->g.dz * pl->g.dz);
+    return launch_xpass(pl, true, FwdSource::Residual, a, pl->g.ny, st);
 }
 
 cudaError_t launch_bwd_xd(const prj_plan* pl, double* P, cudaStream_t st, int accum, double* sq, YRange yr,

@@ -12,6 +12,7 @@
 #include "cp_async.cuh"
 #include "fft_dif.cuh"
 #include "fft_pass.cuh"
+#include "residual.cuh"
 #include "tma_util.cuh"
 
 struct prj_plan;
@@ -48,6 +49,11 @@ struct XArgs {
     double* psum;    // bwd_xp_tile: per-tile sums of the written P values, [y][z tile], or null
     double* Pout;
     double* Bout;    // k_fwd_xd: copy of the source field (P layout), or null
+    // fwd_xp_tile's residual source (SRC 3): r = B - A P of the pinned operator (residual.cuh)
+    const double* B;       // right-hand side (P layout)
+    const double* pm;      // plane means of P (ny)
+    const double* bands;   // a, b, c, a00, b00, c00 (6 ny)
+    double idx2, idz2;     // 1/dx^2, 1/dz^2
     int accum;       // k_bwd_xd: Pout += result instead of Pout = result
     double* sq;      // k_bwd_xd with accum: sq[0] += sum(update^2), sq[1] += sum(result^2), or null
 };
@@ -78,7 +84,8 @@ __device__ __forceinline__ double2 spec_load(const XArgs& a, int y, int kx, int 
 // passes -> split X_k, X_{m-k} -> transposed store.  SRC 0 reads P in the first
 // pass; SRC 1 stages the divergence in shared memory first; SRC 2 reads P from S
 // (staged as above) and calls after_first() once S is no longer read (after the first
-// pass).  Tile (bx, by): rows z0 = bx tz .., plane y0 + by.
+// pass); SRC 3 stages the residual B - A P (residual.cuh) in shared memory first.
+// Tile (bx, by): rows z0 = bx tz .., plane y0 + by.
 template <int SRC, class PL, class Hook = NoHook>
 __device__ __forceinline__ void fwd_xp_tile(const XArgs& a, unsigned char* sm, int bx, int by,
                                             const double2* S = nullptr, Hook after_first = Hook{}) {
@@ -165,6 +172,38 @@ __device__ __forceinline__ void fwd_xp_tile(const XArgs& a, unsigned char* sm, i
                 }
                 A[sidx<true>(r * rs + e)] = vv;
             }
+        }
+        __syncthreads();
+        dif_passes_shared<-1, PL, 0, PL::P>(A, nr, rs, tw);
+    } else if (SRC == 3) {
+        // the residual at the x pair (2e, 2e+1) of row z0 + r, as packed complex element e:
+        // P, B and the z and wall-normal neighbour rows read as aligned pairs, the x
+        // neighbours 2e-1 and 2e+2 (periodic) as scalars
+        const int ny = a.ny, nz = a.nz;
+        const double ak = a.bands[y], bk = a.bands[ny + y], ck = a.bands[2 * ny + y];
+        const double pin = residual_pin(a.bands, a.pm, ny, y);
+        const bool hkm = y > 0, hkp = y + 1 < ny;
+        const size_t plane = (size_t)nz * nx;
+        const int total = nr * m;
+        for (int idx = tid; idx < total; idx += nthr) {
+            const int r = idx / m, e = idx - r * m;
+            const int z = z0 + r, zp = (z + 1 == nz) ? 0 : z + 1, zm = (z == 0) ? nz - 1 : z - 1;
+            const size_t row = (size_t)y * plane + (size_t)z * nx;
+            const double* p0 = a.P + row;
+            const double2 pc = *reinterpret_cast<const double2*>(p0 + 2 * e);
+            const double pxm = p0[e == 0 ? nx - 1 : 2 * e - 1];
+            const double pxp = p0[e == m - 1 ? 0 : 2 * e + 2];
+            const double2 pjp = *reinterpret_cast<const double2*>(a.P + (size_t)y * plane + (size_t)zp * nx + 2 * e);
+            const double2 pjm = *reinterpret_cast<const double2*>(a.P + (size_t)y * plane + (size_t)zm * nx + 2 * e);
+            double2 pkm = make_double2(0.0, 0.0), pkp = make_double2(0.0, 0.0);
+            if (hkm) pkm = *reinterpret_cast<const double2*>(p0 - plane + 2 * e);
+            if (hkp) pkp = *reinterpret_cast<const double2*>(p0 + plane + 2 * e);
+            const double2 b = *reinterpret_cast<const double2*>(a.B + row + 2 * e);
+            const double r0 = residual_at(b.x, pc.x, pc.y, pxm, pjp.x, pjm.x, pkm.x, pkp.x, hkm, hkp, a.idx2, a.idz2,
+                                          ak, bk, ck, pin);
+            const double r1 = residual_at(b.y, pc.y, pxp, pc.x, pjp.y, pjm.y, pkm.y, pkp.y, hkm, hkp, a.idx2, a.idz2,
+                                          ak, bk, ck, pin);
+            A[sidx<true>(r * rs + e)] = make_double2(r0, r1);
         }
         __syncthreads();
         dif_passes_shared<-1, PL, 0, PL::P>(A, nr, rs, tw);
