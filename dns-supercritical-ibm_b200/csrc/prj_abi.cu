@@ -813,6 +813,7 @@ const char* prj_stage_name(int stage) {
     case prj::kStZfftInv: return "k_zfft_inv";
     case prj::kStResidual: return "k_residual";
     case prj::kStVdRhs: return "k_vd_rhs";
+    case prj::kStVdPrep: return "k_rho_prep";
     default: return "";
     }
 }
@@ -969,8 +970,11 @@ int prj_projection_step_vd(prj_plan* plan, const double* d_Uh, const double* d_V
         plan->device_bytes += nh * sizeof(double);
     }
     {
-        StageTimer tm(plan, prj::kStVdRhs, st);
+        StageTimer tm(plan, prj::kStVdPrep, st);
         CK(prj::launch_vd_prep(plan, vd->rho, plan->vd_ih, slot, st), "rho_min and 0.5 / rho");
+    }
+    {
+        StageTimer tm(plan, prj::kStVdRhs, st);
         CK(prj::launch_vd_rhs(plan, d_Uh, d_Vh, d_Wh, f, sc, slot, d_P, st), "variable-density right-hand side");
     }
     if (mode == PRJ_MODE_FP32_REFINE) {

@@ -71,7 +71,7 @@ namespace prj {
 // stage ids of the per-kernel timing record
 enum Stage {
     kStFwdX = 0, kStZSolve = 1, kStBwdX = 2, kStCorrect = 3, kStStats = 4,
-    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kStResidual = 8, kStVdRhs = 9, kNumStages = 12
+    kStZfftFwd = 5, kStThomas = 6, kStZfftInv = 7, kStResidual = 8, kStVdRhs = 9, kStVdPrep = 10, kNumStages = 12
 };
 
 struct StageRecord {
